@@ -1,0 +1,380 @@
+"""Benchmark: site-updates/s of the leapfrog evolution on B200 (headline: SM 256^3, mixed form).
+
+Contract: ``python bench.py --gpus N --steps K --warmup W`` (torchrun for N > 1)
+prints ONE JSON line on rank 0.  A "step" is one leapfrog time step of the
+whole lattice (the body of GFTEvolver's Lattice::evolve time loop), with the
+Energy and GaugeCondition analysers logging every 10 steps as in the
+reference's shipped analyser configuration.
+
+  value      site-updates/s of the mixed form over all ranks, fields resident
+             in HBM (device-timed with CUDA events on the library's stream,
+             max over ranks).  Lattice (1.3 GB) >> L2 (126 MB): no L2 flush needed.
+  e2e        the same metric through the C ABI with host buffers: upload of the
+             initial fields from pinned host memory, K steps, download of the
+             final fields and the observable rows, all inside the timed region.
+  roofline   step kernel: algorithmic bytes per site-update (228 B for SM in
+             FP32 storage: both time levels read once, one level written)
+             x sites / average step-kernel duration, vs measured HBM copy
+             bandwidth.
+  cpu_baseline  the reference itself (oracle/_ref/ref32, compiled from its own
+             sources) on the host cores, a bounded sample.
+
+``--impl reference`` times the reference CPU evolver on the host cores
+instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG = {  # algorithmic bytes per site-update: 2 levels read once + 1 level written
+    ("sm", 4): 57 * 4, ("sm", 8): 57 * 8,
+    ("2hdm", 4): 69 * 4, ("2hdm", 8): 69 * 8,
+}
+LOG_EVERY = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--model", choices=["sm", "2hdm"], default="sm")
+    ap.add_argument("--form", choices=["mixed", "fp64", "ref32", "ref64"], default="mixed")
+    ap.add_argument("--fp64-steps", type=int, default=None, help="steps for the FP64 comparison run")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_params(model: str, n: int):
+    from gftevolver_b200 import GFT_MODEL_2HDM, GFT_MODEL_SM, InitialData, LatticeParams
+    if model == "sm":
+        p = LatticeParams(model=GFT_MODEL_SM, nx=n, ny=n, nz=n, dt=0.05, g=0.65, gp=0.35, lam=0.13, eta_sqr=1.0,
+                          energy_every=LOG_EVERY, gauss_every=LOG_EVERY)
+        ic = InitialData(seed=20240101, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    else:
+        p = LatticeParams(model=GFT_MODEL_2HDM, nx=n, ny=n, nz=n, dt=0.05, g=0.65, gp=0.35,
+                          m1=0.5, m2=0.5, l1=0.065, l2=0.065, l3=0.2, m12r=0.2, l4p5=-0.1,
+                          energy_every=LOG_EVERY, gauss_every=LOG_EVERY)
+        ic = InitialData(seed=20240102, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    return p, ic
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="gft_clocks_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 9:
+                    rows.append(t)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """Per-launch DRAM bytes from the committed ncu summary, if any (profiles/*.json)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(kernel)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference binary (or the oracle port) on the host cores
+# ---------------------------------------------------------------------------
+def cpu_reference_throughput(model: str, n: int, steps: int, procs: int):
+    """Run `procs` independent reference processes, each n^3 for `steps` steps; aggregate site-updates/s."""
+    import numpy as np
+    from oracle import oracle as orc
+    from oracle import refrun
+
+    op = orc.Params(model=orc.MODEL_SM if model == "sm" else orc.MODEL_2HDM, nx=n, ny=n, nz=n,
+                    energy_every=LOG_EVERY, gauss_every=LOG_EVERY)
+    ic = orc.ICSpec(seed=7, mean=[1.0 if model == "sm" else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
+                    eps_sigma=0.1)
+    sc, ve = orc.init_fields(op, ic, np.float32)
+    if refrun.available(False):
+        results = [None] * procs
+
+        def one(k):
+            results[k] = refrun.run(op, sc, ve, steps, fp64=False)[3]
+
+        ths = [threading.Thread(target=one, args=(k,)) for k in range(procs)]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        wall = time.perf_counter() - t0
+        per = [op.nsite * steps / s for s in results]
+        agg = procs * op.nsite * steps / max(results)
+        return {"value": agg, "unit": "site-updates/s", "cores": procs, "kind": "reference",
+                "per_process": statistics.median(per), "wall_s": wall,
+                "sample": f"{procs} independent processes of the reference (oracle/_ref/ref32, -O3) "
+                          f"each {n}^3 x {steps} steps, analysers every {LOG_EVERY}"}
+    # oracle port (single thread per process)
+    t0 = time.perf_counter()
+    orc.evolve(op, sc, ve, steps)
+    secs = time.perf_counter() - t0
+    return {"value": op.nsite * steps / secs, "unit": "site-updates/s", "cores": 1, "kind": "port",
+            "sample": f"C oracle, 1 thread, {n}^3 x {steps} steps"}
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank, world):
+    """--impl reference: the reference CPU evolver on the host cores (rank 0 only).
+
+    One reference process per host core, each evolving its own n^3 lattice for
+    W + K steps (the reference is single-threaded and not reentrant, so the
+    cores run independent lattices); n is chosen so the run takes about a
+    minute.  Site-updates/s of this per-site loop does not depend on n.
+    """
+    if rank != 0:
+        return
+    procs = host_cores()
+    total = args.warmup + args.steps
+    n = int(round((60.0 * 1.9e5 / max(total, 1)) ** (1.0 / 3.0)))
+    n = max(8, min(n, 64))
+    r = cpu_reference_throughput(args.model, n, total, procs)
+    value = r["value"]
+    line = {
+        "impl": "reference", "metric": "site-updates/s", "value": value, "unit": "site-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage, f64 arithmetic", "data": "synthetic",
+        "config": {"workload": f"{args.model.upper()} periodic leapfrog, {n}^3 per process (bounded sample of the "
+                               f"{args.size}^3 workload; site-updates/s is size-independent for this per-site loop), "
+                               f"analysers every {LOG_EVERY}",
+                   "lattice": [n, n, n], "log_every": LOG_EVERY, "processes": procs},
+        "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"]},
+        "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+
+    from gftevolver_b200 import Evolver
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p, ic = workload_params(args.model, args.size)
+    form = args.form
+    sbytes = 8 if form in ("fp64", "ref64") else 4
+    balg = B_ALG[(args.model, sbytes)]
+
+    def timed_run(form_, steps, warmup, sampler=None):
+        ev = Evolver(p, form=form_, device=local)
+        ev.init_fields(ic)
+        if warmup:
+            ev.evolve(warmup)
+        ev.step_kernel_ms()  # reset
+        stream = torch.cuda.ExternalStream(ev.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier()
+        if sampler:
+            sampler.start()
+        e0.record(stream)
+        rows = ev.evolve(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        ms = e0.elapsed_time(e1)
+        kms, nk = ev.step_kernel_ms()
+        return ev, ms, kms, nk, rows, clocks
+
+    sampler = ClockSampler(local)
+    ev, ms, kms, nk, rows, clocks = timed_run(form, args.steps, args.warmup, sampler)
+    ms_max = max_over_ranks(ms)
+    value = world * p.nsite * args.steps / (ms_max / 1e3)
+    nlog = sum(1 for t in range(args.warmup, args.warmup + args.steps) if t % LOG_EVERY == 0)
+    launches = args.steps + nlog * 3  # step kernels + (energy finalize, gauss kernel, gauss finalize) per log step
+
+    # FP64 plain form for the mixed-vs-FP64 ratio
+    fp64 = None
+    if form == "mixed":
+        ev.close()
+        fsteps = args.fp64_steps or max(args.steps // 4, 10)
+        ev64, ms64, kms64, nk64, _, _ = timed_run("fp64", fsteps, min(args.warmup, 3))
+        ms64 = max_over_ranks(ms64)
+        v64 = world * p.nsite * fsteps / (ms64 / 1e3)
+        fp64 = {"value": v64, "steps": fsteps, "step_kernel_ms": kms64,
+                "roofline_frac": (B_ALG[(args.model, 8)] * p.nsite / (kms64 / 1e3)) / 1e9 / measured_peaks()[0],
+                "mixed_over_fp64": value / v64}
+        ev64.close()
+    else:
+        ev.close()
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        dt = torch.float32 if sbytes == 4 else torch.float64
+        sc_h = torch.empty((2, p.nx, p.ny, p.nz, p.nsc), dtype=dt).pin_memory()
+        ve_h = torch.empty((2, p.nx, p.ny, p.nz, 15), dtype=dt).pin_memory()
+        ev = Evolver(p, form=form, device=local)
+        ev.init_fields(ic)
+        ev.download_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8)
+        ev.upload_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8, 0)  # warm the staging buffer
+        ev.evolve(min(args.warmup, 3))
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ev.upload_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8, 0)
+        rows_e2e = ev.evolve(args.steps)
+        ev.download_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8)
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        barrier()
+        secs = max_over_ranks(secs)
+        ev.close()
+        nbytes = (sc_h.numel() + ve_h.numel()) * sc_h.element_size()
+        e2e = {"value": world * p.nsite * args.steps / secs, "unit": "site-updates/s",
+               "h2d_bytes_per_step": nbytes / args.steps,
+               "d2h_bytes_per_step": (nbytes + len(rows_e2e) * 160) / args.steps,
+               "note": "upload of both levels from pinned host memory + K steps (analysers every 10) + download "
+                       "of both levels and the observable rows, per rank; bytes per step = per-run bytes / K"}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = measured_peaks()
+    achieved = balg * p.nsite / (kms / 1e3) / 1e9
+    traffic = committed_traffic(f"fast_step_kernel_{args.model}_{form}")
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_throughput(args.model, 40, 10, host_cores())
+        except Exception as ex:  # the baseline is reported, not required
+            cpu = {"value": None, "error": str(ex)}
+    line = {
+        "metric": "site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if sbytes == 4 else "f64", "data": "synthetic",
+        "config": {"workload": f"{args.model.upper()} {args.size}^3 periodic leapfrog, form={form}, random SU(2) "
+                               f"links eps~N(0,0.1^2), theta_Y~N(0,0.1^2), Higgs N(1,0.1^2), dt=0.05, "
+                               f"energy+Gauss analysers every {LOG_EVERY} steps",
+                   "lattice": [p.nx, p.ny, p.nz], "form": form, "log_every": LOG_EVERY,
+                   "l2": "inputs larger than L2 (state %.2f GB per level pair)" % (2 * p.nsite * (15 + p.nsc) * sbytes / 1e9),
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "step kernel",
+                     "bytes_per_site_update": balg, "avg_kernel_ms": kms, "kernel_launches_timed": nk},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "forms": {"fp64": fp64} if fp64 else None,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "analyser_rows": len(rows),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,615 @@
+// gft_abi.cu -- the C ABI (include/gft.h): handle, device memory, step loop.
+//
+// The handle plays the role of the reference's Lattice + Model objects
+// (Core/Header/Lattice.hpp:22-212, Core/Header/Model.hpp:23-266): it owns both
+// time levels of the fields on the device, the model parameters, the step
+// counter and the analysers' logging cadence.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gft.h"
+#include "gft_launch.h"
+
+using namespace gft;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;
+
+void set_global_error(const std::string& s)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = s;
+}
+
+// Slots of one device row: kObsCount energy slots, then kGaussSlots.
+constexpr int kRowSlots = kObsCount + kGaussSlots;
+constexpr int kMaxProfiled = 8192;
+
+}  // namespace
+
+struct gft_handle {
+    gft_config cfg{};
+    int nsc = 4;
+    int nsite = 0;
+    int sbytes = 4;         // storage bytes per word (4 or 8)
+    void* level_mem[2] = {nullptr, nullptr};
+    LevelPtrs<float> lf[2]{};
+    LevelPtrs<double> ld[2]{};
+    unsigned* d_status = nullptr;
+    double* d_part_e = nullptr;
+    double* d_part_g = nullptr;
+    double* d_scale = nullptr;  // kRowSlots scale factors
+    double* d_rows = nullptr;
+    int rows_cap = 0;
+    void* d_stage = nullptr;
+    size_t stage_bytes = 0;
+    cudaStream_t stream = nullptr;
+    int time_iter = 0;
+    bool has_data = false;
+    bool profile = true;
+    std::vector<cudaEvent_t> ev;
+    int ev_used = 0;
+    std::string err;
+    size_t dev_bytes = 0;
+
+    int fail(int code, const std::string& msg)
+    {
+        err = msg;
+        set_global_error(msg);
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what)
+    {
+        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+        return fail(GFT_E_CUDA, m);
+    }
+};
+
+namespace {
+
+bool is_f64_storage(const gft_handle* h) { return h->sbytes == 8; }
+
+// Parameters of one launch.  For the reference-arithmetic form with float
+// storage, the couplings and the damping factor take the values the shipped
+// reference sees: getSqrCouplings returns float (WilsonLoops/Source/StandardModel.cpp:224-230)
+// and currentDamping is a float member (Core/Header/Model.hpp:38-40).
+StepParams make_params(const gft_handle* h, int time_iter, bool energy)
+{
+    const gft_config& c = h->cfg;
+    const bool f32ref = (c.form == GFT_FORM_REF) && h->sbytes == 4;
+    StepParams P{};
+    P.nx = c.nx;
+    P.ny = c.ny;
+    P.nz = c.nz;
+    P.nsite = h->nsite;
+    P.dt = c.dt;
+    P.dt2 = c.dt * c.dt;
+    const double sp[3] = {c.dx, c.dy, c.dz};
+    for (int a = 0; a < 3; a++) {
+        P.lap[a] = 1.0 / (sp[a] * sp[a]);
+        P.inv_dx[a] = 1.0 / sp[a];
+    }
+    P.inv_sqr_dt = 1.0 / (c.dt * c.dt);
+    const double g2 = c.g * c.g, gp2 = c.gp * c.gp;
+    P.gsq[0] = f32ref ? (double)(float)gp2 : gp2;
+    for (int k = 1; k < 4; k++) P.gsq[k] = f32ref ? (double)(float)g2 : g2;
+    P.inv_g_sqr = (g2 > c.div_tol) ? 1.0 / g2 : 0.0;
+    P.inv_gp_sqr = (gp2 > c.div_tol) ? 1.0 / gp2 : 0.0;
+    double damp = (time_iter < c.nt_damped) ? c.damping : 0.0;
+    if (f32ref) damp = (double)(float)damp;
+    P.damping_step = 0.5 * damp * c.dt;
+    P.lambda = c.lambda;
+    P.eta_sqr = c.eta_sqr;
+    P.m1 = c.m1;
+    P.m2 = c.m2;
+    P.l1 = c.l1;
+    P.l2 = c.l2;
+    P.l3 = c.l3;
+    P.m12r = c.m12r;
+    P.l4p5 = c.l4p5;
+    P.l6r = c.l6r;
+    P.l7r = c.l7r;
+    P.m12i = c.m12i;
+    P.l4m5 = c.l4m5;
+    P.l5i = c.l5i;
+    P.l6i = c.l6i;
+    P.l7i = c.l7i;
+    P.break_son = c.break_son;
+    P.break_uhalfn = c.break_uhalfn;
+    P.apply_norm = c.apply_norm;
+    P.energy_offset = c.energy_offset;
+    P.store_energy = energy ? 1 : 0;
+    return P;
+}
+
+template <class S>
+void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
+{
+    S* p = static_cast<S*>(mem);
+    for (int d = 0; d < 3; d++) {
+        L.q[d] = p;
+        p += 4 * (size_t)nsite;
+    }
+    for (int d = 0; d < 3; d++) {
+        L.th[d] = p;
+        p += (size_t)nsite;
+    }
+    L.ph[0] = p;
+    p += 4 * (size_t)nsite;
+    L.ph[1] = (nsc == 8) ? p : nullptr;
+}
+
+size_t level_words(int nsite, int nsc) { return (size_t)nsite * (15 + (size_t)nsc); }
+
+int step_blocks(const gft_handle* h, const StepParams& P)
+{
+    return (h->cfg.form == GFT_FORM_REF) ? ref_launch_blocks(P) : fast_launch_blocks(P, 0);
+}
+
+template <class S>
+cudaError_t launch_step(gft_handle* h, const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past,
+                        bool energy)
+{
+    const int model = h->cfg.model;
+    if (h->cfg.form == GFT_FORM_REF) {
+        if (model == GFT_MODEL_SM) return launch_ref_step<S, kModelSM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
+        return launch_ref_step<S, kModel2HDM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
+    }
+    if (model == GFT_MODEL_SM)
+        return launch_fast_step<S, kModelSM>(P, now, past, h->d_status, h->d_part_e, energy, 0, h->stream);
+    return launch_fast_step<S, kModel2HDM>(P, now, past, h->d_status, h->d_part_e, energy, 0, h->stream);
+}
+
+template <class S>
+cudaError_t launch_gauss(gft_handle* h, const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut)
+{
+    const int model = h->cfg.model;
+    if (h->cfg.form == GFT_FORM_REF) {
+        if (model == GFT_MODEL_SM) return launch_ref_gauss<S, kModelSM>(P, now, fut, h->d_part_g, h->stream);
+        return launch_ref_gauss<S, kModel2HDM>(P, now, fut, h->d_part_g, h->stream);
+    }
+    if (model == GFT_MODEL_SM) return launch_fast_gauss<S, kModelSM>(P, now, fut, h->d_part_g, h->stream);
+    return launch_fast_gauss<S, kModel2HDM>(P, now, fut, h->d_part_g, h->stream);
+}
+
+int validate(const gft_config* c, std::string& why)
+{
+    if (!c) {
+        why = "gft_create: null config";
+        return GFT_E_INVALID;
+    }
+    if (c->model != GFT_MODEL_SM && c->model != GFT_MODEL_2HDM) {
+        why = "gft_create: unsupported model " + std::to_string(c->model);
+        return GFT_E_UNSUPPORTED;
+    }
+    if (c->form != GFT_FORM_REF && c->form != GFT_FORM_FP64 && c->form != GFT_FORM_MIXED) {
+        why = "gft_create: unknown form " + std::to_string(c->form);
+        return GFT_E_INVALID;
+    }
+    if (c->form == GFT_FORM_REF && c->storage_bytes != 4 && c->storage_bytes != 8) {
+        why = "gft_create: storage_bytes must be 4 or 8 for the reference-arithmetic form";
+        return GFT_E_INVALID;
+    }
+    if (c->nx < 1 || c->ny < 1 || c->nz < 1) {
+        why = "gft_create: lattice dimensions must be >= 1";
+        return GFT_E_INVALID;
+    }
+    if (c->nx > 65535) {
+        why = "gft_create: nx > 65535 is not supported (one grid row per x plane)";
+        return GFT_E_UNSUPPORTED;
+    }
+    const long long n = (long long)c->nx * c->ny * c->nz;
+    if (n > (long long)0x7fffffff / 4) {
+        why = "gft_create: lattice too large for 32-bit site indices";
+        return GFT_E_UNSUPPORTED;
+    }
+    if (!(c->dx > 0 && c->dy > 0 && c->dz > 0 && c->dt > 0)) {
+        why = "gft_create: spacings and time step must be positive";
+        return GFT_E_INVALID;
+    }
+    if (c->energy_every < 0 || c->gauss_every < 0) {
+        why = "gft_create: analyser frequencies must be >= 0";
+        return GFT_E_INVALID;
+    }
+    return GFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gft_version(void) { return "gft_b200 1.0 (sm_100a)"; }
+
+const char* gft_last_error(const gft_handle* h)
+{
+    if (h) return h->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    static thread_local std::string copy;
+    copy = g_err;
+    return copy.c_str();
+}
+
+int gft_create(const gft_config* cfg, gft_handle** out)
+{
+    if (!out) return GFT_E_INVALID;
+    *out = nullptr;
+    std::string why;
+    int rc = validate(cfg, why);
+    if (rc != GFT_OK) {
+        set_global_error(why);
+        return rc;
+    }
+    gft_handle* h = new gft_handle();
+    h->cfg = *cfg;
+    h->nsc = (cfg->model == GFT_MODEL_SM) ? 4 : 8;
+    h->nsite = cfg->nx * cfg->ny * cfg->nz;
+    h->sbytes = (cfg->form == GFT_FORM_REF) ? cfg->storage_bytes : (cfg->form == GFT_FORM_FP64 ? 8 : 4);
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) {
+        int r = h->cuda_fail(e, "cudaSetDevice");
+        delete h;
+        return r;
+    }
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        int r = h->cuda_fail(e, "cudaStreamCreate");
+        delete h;
+        return r;
+    }
+    const size_t lbytes = level_words(h->nsite, h->nsc) * (size_t)h->sbytes;
+    for (int t = 0; t < 2; t++) {
+        e = cudaMalloc(&h->level_mem[t], lbytes);
+        if (e != cudaSuccess) {
+            h->fail(GFT_E_NOMEM, std::string("cudaMalloc(level): ") + cudaGetErrorString(e));
+            gft_destroy(h);
+            return GFT_E_NOMEM;
+        }
+        h->dev_bytes += lbytes;
+        if (h->sbytes == 4)
+            carve<float>(h->level_mem[t], h->nsite, h->nsc, h->lf[t]);
+        else
+            carve<double>(h->level_mem[t], h->nsite, h->nsc, h->ld[t]);
+    }
+    const StepParams P = make_params(h, 0, false);
+    const int nb = std::max(step_blocks(h, P), fast_gauss_blocks(P));
+    const size_t pe = (size_t)nb * kObsCount * sizeof(double), pg = (size_t)nb * kGaussSlots * sizeof(double);
+    h->rows_cap = 64;
+    if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_part_e, pe)) != cudaSuccess || (e = cudaMalloc(&h->d_part_g, pg)) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_scale, kRowSlots * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_rows, (size_t)h->rows_cap * kRowSlots * sizeof(double))) != cudaSuccess) {
+        h->fail(GFT_E_NOMEM, std::string("cudaMalloc(scratch): ") + cudaGetErrorString(e));
+        gft_destroy(h);
+        return GFT_E_NOMEM;
+    }
+    h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap);
+    double scale[kRowSlots];
+    const double dv = cfg->dx * cfg->dy * cfg->dz;
+    for (int k = 0; k < kRowSlots; k++) scale[k] = 1.0;
+    for (int k = kObsEnergy; k <= kObsElectric; k++) scale[k] = dv;
+    scale[kObsPlaqSU2] = 1.0 / (3.0 * h->nsite);
+    scale[kObsPlaqU1] = 1.0 / (3.0 * h->nsite);
+    scale[kObsPhiSq] = 1.0 / (double)h->nsite;
+    for (int k = 0; k < 4; k++) scale[kObsCount + k] = dv;
+    cudaMemcpy(h->d_scale, scale, sizeof(scale), cudaMemcpyHostToDevice);
+    cudaMemset(h->d_status, 0, sizeof(unsigned));
+    h->ev.resize(2 * (size_t)kMaxProfiled);
+    for (auto& x : h->ev) {
+        if ((e = cudaEventCreate(&x)) != cudaSuccess) {
+            x = nullptr;
+            h->cuda_fail(e, "cudaEventCreate");
+            gft_destroy(h);
+            return GFT_E_CUDA;
+        }
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        int r = h->cuda_fail(e, "gft_create");
+        gft_destroy(h);
+        return r;
+    }
+    *out = h;
+    return GFT_OK;
+}
+
+void gft_destroy(gft_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& x : h->ev)
+        if (x) cudaEventDestroy(x);
+    for (int t = 0; t < 2; t++)
+        if (h->level_mem[t]) cudaFree(h->level_mem[t]);
+    cudaFree(h->d_status);
+    cudaFree(h->d_part_e);
+    cudaFree(h->d_part_g);
+    cudaFree(h->d_scale);
+    cudaFree(h->d_rows);
+    cudaFree(h->d_stage);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int gft_time_iter(const gft_handle* h) { return h ? h->time_iter : -1; }
+void* gft_stream(gft_handle* h) { return h ? (void*)h->stream : nullptr; }
+size_t gft_device_bytes(const gft_handle* h) { return h ? h->dev_bytes : 0; }
+
+}  // extern "C"
+
+namespace {
+
+int ensure_stage(gft_handle* h, size_t bytes)
+{
+    if (h->stage_bytes >= bytes) return GFT_OK;
+    if (h->d_stage) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->d_stage);
+        h->dev_bytes -= h->stage_bytes;
+        h->d_stage = nullptr;
+        h->stage_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&h->d_stage, bytes);
+    if (e != cudaSuccess) return h->fail(GFT_E_NOMEM, std::string("cudaMalloc(stage): ") + cudaGetErrorString(e));
+    h->stage_bytes = bytes;
+    h->dev_bytes += bytes;
+    return GFT_OK;
+}
+
+template <class H>
+int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter)
+{
+    if (!h || !sc || !ve) return GFT_E_INVALID;
+    if (time_iter < 0) return h->fail(GFT_E_INVALID, "gft_upload: time_iter must be >= 0");
+    cudaSetDevice(h->cfg.device);
+    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
+    int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
+    if (rc != GFT_OK) return rc;
+    H* dsc = static_cast<H*>(h->d_stage);
+    H* dve = dsc + nsc_w;
+    cudaError_t e = cudaMemcpyAsync(dsc, sc, nsc_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dve, ve, nve_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
+    for (int t = 0; t < 2 && e == cudaSuccess; t++) {
+        const H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
+        const H* v_t = dve + (size_t)t * h->nsite * 15;
+        e = is_f64_storage(h) ? launch_aos_to_soa<double, H>(s_t, v_t, h->nsite, h->nsc, h->ld[t], h->stream)
+                              : launch_aos_to_soa<float, H>(s_t, v_t, h->nsite, h->nsc, h->lf[t], h->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_upload");
+    h->time_iter = time_iter;
+    h->has_data = true;
+    return GFT_OK;
+}
+
+template <class H>
+int download_impl(gft_handle* h, H* sc, H* ve)
+{
+    if (!h || !sc || !ve) return GFT_E_INVALID;
+    if (!h->has_data) return h->fail(GFT_E_STATE, "gft_download: no field data on the device");
+    cudaSetDevice(h->cfg.device);
+    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
+    int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
+    if (rc != GFT_OK) return rc;
+    H* dsc = static_cast<H*>(h->d_stage);
+    H* dve = dsc + nsc_w;
+    cudaError_t e = cudaSuccess;
+    for (int t = 0; t < 2 && e == cudaSuccess; t++) {
+        H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
+        H* v_t = dve + (size_t)t * h->nsite * 15;
+        e = is_f64_storage(h) ? launch_soa_to_aos<double, H>(h->ld[t], h->nsite, h->nsc, s_t, v_t, h->stream)
+                              : launch_soa_to_aos<float, H>(h->lf[t], h->nsite, h->nsc, s_t, v_t, h->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sc, dsc, nsc_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ve, dve, nve_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_download");
+    return GFT_OK;
+}
+
+int ensure_rows(gft_handle* h, int n)
+{
+    if (n <= h->rows_cap) return GFT_OK;
+    cudaStreamSynchronize(h->stream);
+    double* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (size_t)n * kRowSlots * sizeof(double));
+    if (e != cudaSuccess) return h->fail(GFT_E_NOMEM, std::string("cudaMalloc(rows): ") + cudaGetErrorString(e));
+    h->dev_bytes += (size_t)(n - h->rows_cap) * kRowSlots * sizeof(double);
+    cudaFree(h->d_rows);
+    h->d_rows = p;
+    h->rows_cap = n;
+    return GFT_OK;
+}
+
+void fill_row(gft_observables* r, int time_iter, bool e, bool g, const double* v)
+{
+    std::memset(r, 0, sizeof(*r));
+    r->time_iter = time_iter;
+    r->has_energy = e;
+    r->has_gauss = g;
+    if (e) {
+        r->energy = v[kObsEnergy];
+        r->potential = v[kObsPotential];
+        r->gradient = v[kObsGradient];
+        r->kinetic = v[kObsKinetic];
+        r->magnetic = v[kObsMagnetic];
+        r->electric = v[kObsElectric];
+        r->plaq_su2 = v[kObsPlaqSU2];
+        r->plaq_u1 = v[kObsPlaqU1];
+        r->phi_sq = v[kObsPhiSq];
+    }
+    if (g) {
+        for (int k = 0; k < 4; k++) {
+            r->gauss_int[k] = v[kObsCount + k];
+            r->gauss_max[k] = v[kObsCount + 4 + k];
+        }
+    }
+}
+
+template <class S>
+int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observables* rows, int max_rows, int* n_rows)
+{
+    const gft_config& c = h->cfg;
+    struct Meta {
+        int ti;
+        bool e, g;
+    };
+    std::vector<Meta> meta;
+    int nlog = 0;
+    for (int s = 0; s < n_steps; s++) {
+        const int ti = h->time_iter + s;
+        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;
+        const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
+        if (e || g) nlog++;
+    }
+    int rc = ensure_rows(h, std::max(nlog, 1));
+    if (rc != GFT_OK) return rc;
+    cudaError_t err = cudaSuccess;
+    int row = 0;
+    for (int s = 0; s < n_steps && err == cudaSuccess; s++) {
+        const int ti = h->time_iter;
+        const int tn = (ti + 1) % 2, tp = 1 - tn;
+        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;
+        const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
+        const StepParams P = make_params(h, ti, e);
+        const bool prof = h->profile && h->ev_used < kMaxProfiled;
+        if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
+        err = launch_step<S>(h, P, lv[tn], lv[tp], e);
+        if (prof) {
+            cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
+            h->ev_used++;
+        }
+        if (err != cudaSuccess) break;
+        double* out = h->d_rows + (size_t)row * kRowSlots;
+        if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->stream);
+        if (g && err == cudaSuccess) {
+            err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
+            if (err == cudaSuccess)
+                err = launch_finalize(h->d_part_g, fast_gauss_blocks(P), kGaussSlots, 4, h->d_scale + kObsCount,
+                                      out + kObsCount, h->stream);
+        }
+        if (e || g) {
+            meta.push_back({ti, e, g});
+            row++;
+        }
+        h->time_iter++;
+    }
+    if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve(launch)");
+    std::vector<double> host((size_t)std::max(row, 1) * kRowSlots);
+    unsigned status = 0;
+    if (row > 0) err = cudaMemcpyAsync(host.data(), h->d_rows, (size_t)row * kRowSlots * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->stream);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&status, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+    if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve");
+    const int nw = rows ? std::min(row, std::max(max_rows, 0)) : 0;
+    for (int r = 0; r < nw; r++) fill_row(&rows[r], meta[r].ti, meta[r].e, meta[r].g, host.data() + (size_t)r * kRowSlots);
+    if (n_rows) *n_rows = nw;
+    return (int)(status & (GFT_W_ASIN_DOMAIN | GFT_W_SQRT_DOMAIN | GFT_W_NONFINITE));
+}
+
+}  // namespace
+
+extern "C" {
+
+int gft_upload_f32(gft_handle* h, const float* sc, const float* ve, int time_iter) { return upload_impl(h, sc, ve, time_iter); }
+int gft_upload_f64(gft_handle* h, const double* sc, const double* ve, int time_iter) { return upload_impl(h, sc, ve, time_iter); }
+int gft_download_f32(gft_handle* h, float* sc, float* ve) { return download_impl(h, sc, ve); }
+int gft_download_f64(gft_handle* h, double* sc, double* ve) { return download_impl(h, sc, ve); }
+
+int gft_init_fields(gft_handle* h, const gft_ic* ic)
+{
+    if (!h || !ic) return GFT_E_INVALID;
+    cudaSetDevice(h->cfg.device);
+    ICParams p{};
+    p.seed = ic->seed;
+    for (int k = 0; k < 8; k++) {
+        p.mean[k] = ic->mean[k];
+        p.sigma[k] = ic->sigma[k];
+    }
+    p.theta_sigma = ic->theta_sigma;
+    p.eps_sigma = ic->eps_sigma;
+    p.wall_width = ic->wall_width;
+    p.wall_value = ic->wall_value;
+    const StepParams P = make_params(h, 0, false);
+    cudaError_t e = is_f64_storage(h) ? launch_init_fields<double>(P, h->nsc, p, h->ld[0], h->ld[1], h->stream)
+                                      : launch_init_fields<float>(P, h->nsc, p, h->lf[0], h->lf[1], h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_init_fields");
+    h->time_iter = 0;
+    h->has_data = true;
+    return GFT_OK;
+}
+
+int gft_evolve(gft_handle* h, int n_steps, gft_observables* rows, int max_rows, int* n_rows)
+{
+    if (n_rows) *n_rows = 0;
+    if (!h) return GFT_E_INVALID;
+    if (n_steps < 0) return h->fail(GFT_E_INVALID, "gft_evolve: n_steps must be >= 0");
+    if (!h->has_data) return h->fail(GFT_E_STATE, "gft_evolve: upload or initialise the fields first");
+    cudaSetDevice(h->cfg.device);
+    if (is_f64_storage(h)) return evolve_impl<double>(h, h->ld, n_steps, rows, max_rows, n_rows);
+    return evolve_impl<float>(h, h->lf, n_steps, rows, max_rows, n_rows);
+}
+
+int gft_observe(gft_handle* h, gft_observables* row)
+{
+    if (!h || !row) return GFT_E_INVALID;
+    if (!h->has_data) return h->fail(GFT_E_STATE, "gft_observe: no field data on the device");
+    // Observe = one energy-logging step computed into scratch levels is not
+    // side-effect free; instead evaluate with a copy of the past level.
+    cudaSetDevice(h->cfg.device);
+    const int ti = h->time_iter;
+    const int tn = (ti + 1) % 2, tp = 1 - tn;
+    const size_t lbytes = level_words(h->nsite, h->nsc) * (size_t)h->sbytes;
+    int rc = ensure_stage(h, lbytes);
+    if (rc != GFT_OK) return rc;
+    cudaError_t e = cudaMemcpyAsync(h->d_stage, h->level_mem[tp], lbytes, cudaMemcpyDeviceToDevice, h->stream);
+    const StepParams P = make_params(h, ti, true);
+    if (e == cudaSuccess) {
+        if (is_f64_storage(h)) {
+            LevelPtrs<double> tmp;
+            carve<double>(h->d_stage, h->nsite, h->nsc, tmp);
+            e = launch_step<double>(h, P, h->ld[tn], tmp, true);
+        } else {
+            LevelPtrs<float> tmp;
+            carve<float>(h->d_stage, h->nsite, h->nsc, tmp);
+            e = launch_step<float>(h, P, h->lf[tn], tmp, true);
+        }
+    }
+    // the step wrote into the copy; restore nothing (the levels are untouched)
+    if (e == cudaSuccess) e = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, h->d_rows, h->stream);
+    std::vector<double> host(kRowSlots, 0.0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), h->d_rows, kObsCount * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_observe");
+    fill_row(row, ti, true, false, host.data());
+    return GFT_OK;
+}
+
+double gft_step_kernel_ms(gft_handle* h, int* launches)
+{
+    if (launches) *launches = 0;
+    if (!h || h->ev_used == 0) return 0.0;
+    cudaEventSynchronize(h->ev[2 * (size_t)h->ev_used - 1]);
+    double total = 0.0;
+    for (int i = 0; i < h->ev_used; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[2 * (size_t)i], h->ev[2 * (size_t)i + 1]);
+        total += ms;
+    }
+    const int n = h->ev_used;
+    h->ev_used = 0;
+    if (launches) *launches = n;
+    return total / n;
+}
+
+}  // extern "C"

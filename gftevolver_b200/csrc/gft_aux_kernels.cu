@@ -1,0 +1,207 @@
+// gft_aux_kernels.cu -- layout conversion, initial data and reduction finalisation.
+#include "gft_device.cuh"
+#include "gft_launch.h"
+
+namespace gft {
+namespace {
+
+// Reference AoS record -> structure-of-arrays level (one thread per site).
+template <class S, class H>
+__global__ void aos_to_soa_kernel(const H* __restrict__ sc, const H* __restrict__ ve, int nsite, int nsc,
+                                  LevelPtrs<S> lv)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsite) return;
+    const H* v = ve + (size_t)s * 15;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        lv.th[d][s] = (S)v[5 * d];
+        st4(lv.q[d], s, (S)v[5 * d + 1], (S)v[5 * d + 2], (S)v[5 * d + 3], (S)v[5 * d + 4]);
+    }
+    const H* f = sc + (size_t)s * nsc;
+    for (int db = 0; db < nsc / 4; db++)
+        st4(lv.ph[db], s, (S)f[4 * db], (S)f[4 * db + 1], (S)f[4 * db + 2], (S)f[4 * db + 3]);
+}
+
+template <class S, class H>
+__global__ void soa_to_aos_kernel(LevelPtrs<S> lv, int nsite, int nsc, H* __restrict__ sc, H* __restrict__ ve)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsite) return;
+    H* v = ve + (size_t)s * 15;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        v[5 * d] = (H)lv.th[d][s];
+        const S* q = lv.q[d] + 4 * (size_t)s;
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[5 * d + 1 + k] = (H)q[k];
+    }
+    H* f = sc + (size_t)s * nsc;
+    for (int db = 0; db < nsc / 4; db++) {
+        const S* p = lv.ph[db] + 4 * (size_t)s;
+#pragma unroll
+        for (int k = 0; k < 4; k++) f[4 * db + k] = (H)p[k];
+    }
+}
+
+// Counter-based generator: SplitMix64 finaliser (Steele, Lea, Flood 2014) keyed by
+// (seed, stream, index); uniforms from the top 53 bits; normals by the cosine
+// branch of Box-Muller.  Stream ids: scalar component c -> c, theta_Y of
+// direction d -> 16 + d, SU(2) angle -> 32 + d, axis cos(polar) -> 48 + d,
+// axis azimuth -> 64 + d.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double uniform01(unsigned long long seed, unsigned long long stream, unsigned long long i)
+{
+    const unsigned long long h = mix64(mix64(seed ^ (stream * 0xD1B54A32D192ED03ULL)) + i);
+    return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ double gaussian(unsigned long long seed, unsigned long long stream, unsigned long long i)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    const double u1 = uniform01(seed, stream, 2 * i), u2 = uniform01(seed, stream, 2 * i + 1);
+    return sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
+}
+
+template <class S>
+__global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs<S> a, LevelPtrs<S> b)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.nsite) return;
+    const double two_pi = 6.283185307179586476925286766559;
+    const int zc = s % P.nz;
+    double f[8];
+    for (int c = 0; c < nsc; c++) {
+        double v = ic.mean[c] + ic.sigma[c] * gaussian(ic.seed, (unsigned long long)c, (unsigned long long)s);
+        if (c == 0 && ic.wall_width > 0.0) {
+            const double zz = (double)zc;
+            v += ic.wall_value * 0.5 *
+                 (tanh((zz - 0.25 * P.nz) / ic.wall_width) - tanh((zz - 0.75 * P.nz) / ic.wall_width));
+        }
+        f[c] = v;
+    }
+    for (int db = 0; db < nsc / 4; db++) {
+        st4(a.ph[db], s, (S)f[4 * db], (S)f[4 * db + 1], (S)f[4 * db + 2], (S)f[4 * db + 3]);
+        st4(b.ph[db], s, (S)f[4 * db], (S)f[4 * db + 1], (S)f[4 * db + 2], (S)f[4 * db + 3]);
+    }
+    for (int d = 0; d < 3; d++) {
+        const double th = ic.theta_sigma * gaussian(ic.seed, 16ULL + d, (unsigned long long)s);
+        double q0 = 1.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        if (ic.eps_sigma > 0.0) {
+            const double eps = ic.eps_sigma * gaussian(ic.seed, 32ULL + d, (unsigned long long)s);
+            const double ct = 2.0 * uniform01(ic.seed, 48ULL + d, (unsigned long long)s) - 1.0;
+            const double st = sqrt(1.0 - ct * ct);
+            const double ph = two_pi * uniform01(ic.seed, 64ULL + d, (unsigned long long)s);
+            const double se = sin(eps);
+            q0 = cos(eps);
+            q1 = se * st * cos(ph);
+            q2 = se * st * sin(ph);
+            q3 = se * ct;
+        }
+        a.th[d][s] = (S)th;
+        b.th[d][s] = (S)th;
+        st4(a.q[d], s, (S)q0, (S)q1, (S)q2, (S)q3);
+        st4(b.q[d], s, (S)q0, (S)q1, (S)q2, (S)q3);
+    }
+}
+
+// One block: slot k summed over blocks with Neumaier compensation (k < max_from)
+// or maximised (k >= max_from), in a fixed order (deterministic).
+constexpr int kFinThreads = 256;
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __restrict__ partials, int nblocks,
+                                                               int nslots, int max_from, const double* scale,
+                                                               double* out)
+{
+    __shared__ double s_sum[kFinThreads];
+    __shared__ double s_cmp[kFinThreads];
+    for (int k = 0; k < nslots; k++) {
+        const bool is_max = k >= max_from;
+        double sum = 0.0, comp = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+            const double v = partials[(size_t)b * nslots + k];
+            if (is_max) {
+                sum = fmax(sum, v);
+            } else {
+                const double t = sum + v;
+                comp += (fabs(sum) >= fabs(v)) ? (sum - t) + v : (v - t) + sum;
+                sum = t;
+            }
+        }
+        s_sum[threadIdx.x] = sum;
+        s_cmp[threadIdx.x] = comp;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tsum = 0.0, tcomp = 0.0;
+            for (int t = 0; t < (int)blockDim.x; t++) {
+                if (is_max) {
+                    tsum = fmax(tsum, s_sum[t]);
+                } else {
+                    const double v = s_sum[t];
+                    const double u = tsum + v;
+                    tcomp += (fabs(tsum) >= fabs(v)) ? (tsum - u) + v : (v - u) + tsum;
+                    tsum = u;
+                    tcomp += s_cmp[t];
+                }
+            }
+            out[k] = (is_max ? tsum : tsum + tcomp) * scale[k];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+template <class S, class H>
+cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s)
+{
+    aos_to_soa_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(aos_sc, aos_ve, nsite, nsc, lv);
+    return cudaGetLastError();
+}
+
+template <class S, class H>
+cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s)
+{
+    soa_to_aos_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(lv, nsite, nsc, aos_sc, aos_ve);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic, LevelPtrs<S> a, LevelPtrs<S> b,
+                               cudaStream_t s)
+{
+    init_fields_kernel<S><<<(P.nsite + 255) / 256, 256, 0, s>>>(P, nsc, ic, a, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_dev,
+                            double* out, cudaStream_t s)
+{
+    finalize_kernel<<<1, kFinThreads, 0, s>>>(partials, nblocks, nslots, max_from, scale_dev, out);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_aos_to_soa<float, float>(const float*, const float*, int, int, LevelPtrs<float>,
+                                                     cudaStream_t);
+template cudaError_t launch_aos_to_soa<float, double>(const double*, const double*, int, int, LevelPtrs<float>,
+                                                      cudaStream_t);
+template cudaError_t launch_aos_to_soa<double, float>(const float*, const float*, int, int, LevelPtrs<double>,
+                                                      cudaStream_t);
+template cudaError_t launch_aos_to_soa<double, double>(const double*, const double*, int, int, LevelPtrs<double>,
+                                                       cudaStream_t);
+template cudaError_t launch_soa_to_aos<float, float>(LevelPtrs<float>, int, int, float*, float*, cudaStream_t);
+template cudaError_t launch_soa_to_aos<float, double>(LevelPtrs<float>, int, int, double*, double*, cudaStream_t);
+template cudaError_t launch_soa_to_aos<double, float>(LevelPtrs<double>, int, int, float*, float*, cudaStream_t);
+template cudaError_t launch_soa_to_aos<double, double>(LevelPtrs<double>, int, int, double*, double*, cudaStream_t);
+template cudaError_t launch_init_fields<float>(const StepParams&, int, const ICParams&, LevelPtrs<float>,
+                                               LevelPtrs<float>, cudaStream_t);
+template cudaError_t launch_init_fields<double>(const StepParams&, int, const ICParams&, LevelPtrs<double>,
+                                                LevelPtrs<double>, cudaStream_t);
+
+}  // namespace gft

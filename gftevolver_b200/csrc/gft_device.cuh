@@ -1,0 +1,240 @@
+// gft_device.cuh -- device-side layout, parameters and algebra shared by the
+// step kernels.
+//
+// HBM layout (structure of arrays, one block per time level):
+//   q[d]  : [N][4] storage words, SU(2) quaternion (c0, c1, c2, c3) of the link in direction d
+//   th[d] : [N]    storage words, U(1) hypercharge phase theta_Y of the link in direction d
+//   ph[k] : [N][4] storage words, Higgs doublet k (k = 0 for SM, 0..1 for 2HDM)
+// Site index s = (x*ny + y)*nz + z as in the reference (Core/Source/Lattice.cpp:658-671).
+// The reference's AoS record per site ([theta, c0..c3] x 3 directions, then the
+// scalar components) is split so that a warp reads 16- or 32-byte vectors of
+// consecutive sites.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gft {
+
+constexpr int kModelSM = 1;
+constexpr int kModel2HDM = 2;
+
+// Observable slots reduced per block on logging steps.
+enum ObsSlot : int {
+    kObsEnergy = 0,
+    kObsPotential,
+    kObsGradient,
+    kObsKinetic,
+    kObsMagnetic,
+    kObsElectric,
+    kObsPlaqSU2,
+    kObsPlaqU1,
+    kObsPhiSq,
+    kObsCount
+};
+constexpr int kGaussSlots = 8;  // integrated |viol| (4) then max |viol| (4)
+
+template <class S>
+struct LevelPtrs {
+    S* q[3];
+    S* th[3];
+    S* ph[2];
+};
+
+// Per-launch parameters (POD, passed by value).
+struct StepParams {
+    int nx, ny, nz;
+    int nsite;
+    double dt, dt2;
+    double lap[3];          // 1/dx_a^2 (covariant Laplacian and Wilson-loop weights)
+    double inv_dx[3];       // 1/dx_a (forward-difference gradient energy)
+    double inv_sqr_dt;      // 1/dt^2
+    double gsq[4];          // coupling^2 per equation k % 4 (as the reference's getSqrCouplings returns it)
+    double inv_g_sqr, inv_gp_sqr;
+    double damping_step;    // 0.5 * damping * dt for this step
+    // SO_N
+    double lambda, eta_sqr;
+    // Double_SO_N
+    double m1, m2, l1, l2, l3, m12r, l4p5, l6r, l7r, m12i, l4m5, l5i, l6i, l7i;
+    int break_son, break_uhalfn, apply_norm;
+    double energy_offset;
+    int store_energy;       // logging step: renormalise as the reference does and accumulate energies
+};
+
+// ---------------------------------------------------------------------------
+// Quaternions: U = c0 + i c.sigma, product (a0 b0 - a.b, a0 b + b0 a - a x b)
+// (the convention of WilsonLoops/Source/StandardModel.cpp:160-191).
+// ---------------------------------------------------------------------------
+template <class C>
+struct Q {
+    C w, x, y, z;
+};
+
+template <class C>
+__device__ __forceinline__ Q<C> qconj(Q<C> a) { return {a.w, -a.x, -a.y, -a.z}; }
+
+template <class C>
+__device__ __forceinline__ Q<C> qmul(Q<C> a, Q<C> b)
+{
+    Q<C> r;
+    r.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+    r.x = a.w * b.x + a.x * b.w - a.y * b.z + a.z * b.y;
+    r.y = a.w * b.y + a.y * b.w - a.z * b.x + a.x * b.z;
+    r.z = a.w * b.z + a.z * b.w - a.x * b.y + a.y * b.x;
+    return r;
+}
+
+// vector part of a * b only
+template <class C>
+__device__ __forceinline__ void qmul_vec(Q<C> a, Q<C> b, C& rx, C& ry, C& rz)
+{
+    rx = a.w * b.x + a.x * b.w - a.y * b.z + a.z * b.y;
+    ry = a.w * b.y + a.y * b.w - a.z * b.x + a.x * b.z;
+    rz = a.w * b.z + a.z * b.w - a.x * b.y + a.y * b.x;
+}
+
+// scalar part of a * b only
+template <class C>
+__device__ __forceinline__ C qmul_w(Q<C> a, Q<C> b)
+{
+    return a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+}
+
+template <class C>
+__device__ __forceinline__ Q<C> qadd_scaled(Q<C> acc, C s, Q<C> a)
+{
+    acc.w += s * a.w;
+    acc.x += s * a.x;
+    acc.y += s * a.y;
+    acc.z += s * a.z;
+    return acc;
+}
+
+template <class To, class From>
+__device__ __forceinline__ Q<To> qcast(Q<From> a)
+{
+    return {(To)a.w, (To)a.x, (To)a.y, (To)a.z};
+}
+
+// ---------------------------------------------------------------------------
+// Vector loads / stores of 4-word records.
+// ---------------------------------------------------------------------------
+template <class C>
+__device__ __forceinline__ Q<C> ld4(const float* p, int s)
+{
+    float4 v = __ldg(reinterpret_cast<const float4*>(p) + s);
+    return {(C)v.x, (C)v.y, (C)v.z, (C)v.w};
+}
+
+template <class C>
+__device__ __forceinline__ Q<C> ld4(const double* p, int s)
+{
+    const double2* b = reinterpret_cast<const double2*>(p) + 2 * (size_t)s;
+    double2 a0 = __ldg(b), a1 = __ldg(b + 1);
+    return {(C)a0.x, (C)a0.y, (C)a1.x, (C)a1.y};
+}
+
+template <class C>
+__device__ __forceinline__ C ld1(const float* p, int s) { return (C)__ldg(p + s); }
+template <class C>
+__device__ __forceinline__ C ld1(const double* p, int s) { return (C)__ldg(p + s); }
+
+__device__ __forceinline__ void st4(float* p, int s, float a, float b, float c, float d)
+{
+    reinterpret_cast<float4*>(p)[s] = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void st4(double* p, int s, double a, double b, double c, double d)
+{
+    double2* o = reinterpret_cast<double2*>(p) + 2 * (size_t)s;
+    o[0] = make_double2(a, b);
+    o[1] = make_double2(c, d);
+}
+
+// ---------------------------------------------------------------------------
+// Neighbourhood of a site with periodic wrap (BoundaryConditions/Source/Periodic.cpp:18-57, 125-170):
+//   c = x, m[a] = x - e_a, p[a] = x + e_a, dg[a][j] = x + e_a - e_j.
+// ---------------------------------------------------------------------------
+struct Nbr {
+    int c;
+    int m[3];
+    int p[3];
+    int dg[3][3];
+};
+
+__device__ __forceinline__ int site_of(const StepParams& P, int x, int y, int z)
+{
+    return (x * P.ny + y) * P.nz + z;
+}
+
+__device__ __forceinline__ Nbr neighbours(const StepParams& P, int x, int y, int z)
+{
+    const int xm = (x == 0) ? P.nx - 1 : x - 1, xp = (x + 1 == P.nx) ? 0 : x + 1;
+    const int ym = (y == 0) ? P.ny - 1 : y - 1, yp = (y + 1 == P.ny) ? 0 : y + 1;
+    const int zm = (z == 0) ? P.nz - 1 : z - 1, zp = (z + 1 == P.nz) ? 0 : z + 1;
+    Nbr n;
+    n.c = site_of(P, x, y, z);
+    n.m[0] = site_of(P, xm, y, z);
+    n.m[1] = site_of(P, x, ym, z);
+    n.m[2] = site_of(P, x, y, zm);
+    n.p[0] = site_of(P, xp, y, z);
+    n.p[1] = site_of(P, x, yp, z);
+    n.p[2] = site_of(P, x, y, zp);
+    n.dg[0][0] = n.dg[1][1] = n.dg[2][2] = n.c;
+    n.dg[0][1] = site_of(P, xp, ym, z);
+    n.dg[0][2] = site_of(P, xp, y, zm);
+    n.dg[1][0] = site_of(P, xm, yp, z);
+    n.dg[1][2] = site_of(P, x, yp, zm);
+    n.dg[2][0] = site_of(P, xm, y, zp);
+    n.dg[2][1] = site_of(P, x, ym, zp);
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions (double) into a per-block partials array.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Reduce NV values per thread over the block; thread 0 writes them to out[0..NV).
+// `is_max` selects max for slots >= max_from.  Requires blockDim.x*y multiple of 32, <= 1024.
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out, int max_from)
+{
+    __shared__ double red[32][NV];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = (k >= max_from) ? warp_max(v[k]) : warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) red[warp][k] = v[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = (lane < nwarps) ? red[lane][k] : 0.0;
+            t = (k >= max_from) ? warp_max(t) : warp_sum(t);
+            if (lane == 0) out[k] = t;
+        }
+    }
+}
+
+// Device status word bits (mirror GFT_W_*).
+constexpr unsigned kWarnAsin = 1u;
+constexpr unsigned kWarnSqrt = 2u;
+constexpr unsigned kWarnNonFinite = 4u;
+
+}  // namespace gft

@@ -1,0 +1,442 @@
+// gft_fast_kernels.cu -- throughput forms of the leapfrog step.
+//
+//   GFT_FORM_FP64  : S = double, every operation in FP64.
+//   GFT_FORM_MIXED : S = float storage; forces (staples, sines, covariant
+//                    transports, currents, potential) in FP32; the link
+//                    momentum vec(U_now U_past^dag), the update sums, the
+//                    quaternion renormalisation and all reductions in FP64.
+//
+// Same physics as the reference's per-site update (Core/Source/Model.cpp:339-373,
+// WilsonLoops/Source/StandardModel.cpp:324-514, Gradients/Source/StandardModel.cpp:72-100,
+// 272-363, Potentials/Source/SO_N.cpp:57-75, Double_SO_N.cpp:244-341), reassociated:
+//   * the reference builds, for every link i and plane j, the loops
+//       P1 = U_j(x+i)^dag U_i(x+j) U_j(x) U_i(x)^dag,
+//       P2 = U_i(x) U_j(x-j) U_i(x-j)^dag U_j(x+i-j)^dag,
+//     renormalising intermediate products.  Here the staples are summed first,
+//       SA_i = sum_j w_j U_j(x+i)^dag U_i(x+j) U_j(x),   SB_i = sum_j w_j U_j(x-j) U_i(x-j)^dag U_j(x+i-j)^dag,
+//     and vec(P1) - vec(P2) summed over j becomes vec(SA_i U_i^dag) - vec(U_i SB_i)
+//     (the vector part is linear).  C_ij = U_j(x+i)^dag U_i(x+j) is shared by
+//     the staples of links i and j.  Intermediate renormalisation is dropped:
+//     it changes products of unit quaternions only at the rounding level.
+//   * the U(1) plaquette angle of plane (i,j) is computed once for both links.
+// One thread per site (x, y, z); the grid covers (z, y) tiles of 32 x 4 and
+// one x plane per grid row; neighbour reads hit L1/L2.
+#include "gft_device.cuh"
+#include "gft_launch.h"
+
+namespace gft {
+namespace {
+
+__device__ __forceinline__ void sc_(float x, float& s, float& c) { sincosf(x, &s, &c); }
+__device__ __forceinline__ void sc_(double x, double& s, double& c) { sincos(x, &s, &c); }
+__device__ __forceinline__ float sin_(float x) { return sinf(x); }
+__device__ __forceinline__ double sin_(double x) { return sin(x); }
+__device__ __forceinline__ float asin_(float x) { return asinf(x); }
+__device__ __forceinline__ double asin_(double x) { return asin(x); }
+__device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+
+// Doublet phi rotated by the hypercharge phase (cos, sin) then acted on by the
+// SU(2) quaternion u as the real 4x4 of Gradients/Source/StandardModel.cpp:94-97.
+template <class C>
+__device__ __forceinline__ Q<C> transport(Q<C> u, C cs, C sn, Q<C> f)
+{
+    const C h0 = cs * f.w - sn * f.x;
+    const C h1 = cs * f.x + sn * f.w;
+    const C h2 = cs * f.y - sn * f.z;
+    const C h3 = cs * f.z + sn * f.y;
+    Q<C> t;
+    t.w = u.w * h0 - u.z * h1 + u.y * h2 - u.x * h3;
+    t.x = u.z * h0 + u.w * h1 + u.x * h2 + u.y * h3;
+    t.y = -u.y * h0 - u.x * h1 + u.w * h2 + u.z * h3;
+    t.z = u.x * h0 - u.y * h1 - u.z * h2 + u.w * h3;
+    return t;
+}
+
+// 1 - a0/|a| computed without cancellation: |vec a|^2 / (|a| (|a| + a0)).
+template <class C>
+__device__ __forceinline__ double one_minus_trace(Q<C> a)
+{
+    const double v2 = (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z;
+    const double nrm = sqrt((double)a.w * a.w + v2);
+    return v2 / (nrm * (nrm + (double)a.w));
+}
+
+template <class S, int MODEL, bool ENERGY>
+__global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> past,
+                                                        unsigned* status, double* partials)
+{
+    using C = S;  // force arithmetic: FP64 form -> double, mixed form -> float
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x = blockIdx.z;
+    const bool active = (z < P.nz) && (y < P.ny);
+    double obs[kObsCount];
+#pragma unroll
+    for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
+    unsigned warn = 0;
+
+    if (active) {
+        const Nbr n = neighbours(P, x, y, z);
+        const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
+
+        Q<C> U[3];
+        C th[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            U[a] = ld4<C>(now.q[a], n.c);
+            th[a] = ld1<C>(now.th[a], n.c);
+        }
+
+        // ---- magnetic term: U(1) sines and SU(2) staple sums ----
+        C MgY[3] = {(C)0, (C)0, (C)0};
+        Q<C> SA[3], SB[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            SA[a] = {(C)0, (C)0, (C)0, (C)0};
+            SB[a] = {(C)0, (C)0, (C)0, (C)0};
+        }
+        double mag_e = 0.0, plaq2 = 0.0, plaq1 = 0.0;
+#pragma unroll
+        for (int pl = 0; pl < 3; pl++) {
+            const int i = (pl == 2) ? 1 : 0;
+            const int j = (pl == 0) ? 1 : 2;
+            const Q<C> Uj_pi = ld4<C>(now.q[j], n.p[i]);
+            const Q<C> Ui_pj = ld4<C>(now.q[i], n.p[j]);
+            const C thj_pi = ld1<C>(now.th[j], n.p[i]);
+            const C thi_pj = ld1<C>(now.th[i], n.p[j]);
+            // F_ij(x) = theta_i(x) + theta_j(x+i) - theta_i(x+j) - theta_j(x); the reference's
+            // local angle is -F for link i and +F for link j (StandardModel.cpp:348-353).
+            const C F = th[i] + thj_pi - thi_pj - th[j];
+            const C sF = sin_(F);
+            MgY[i] -= sF * lap[j];
+            MgY[j] += sF * lap[i];
+            const Q<C> Cij = qmul(qconj(Uj_pi), Ui_pj);
+            const Q<C> Aij = qmul(Cij, U[j]);
+            const Q<C> Aji = qmul(qconj(Cij), U[i]);
+            SA[i] = qadd_scaled(SA[i], lap[j], Aij);
+            SA[j] = qadd_scaled(SA[j], lap[i], Aji);
+            if (ENERGY) {
+                // plaquette P1 = Aij U_i^dag: both orientations have the same trace
+                const Q<C> P1 = qmul(Aij, qconj(U[i]));
+                const double omt = one_minus_trace(P1);
+                const double wF = (double)F;
+                const double omc = 2.0 * sin(0.5 * wF) * sin(0.5 * wF);
+                mag_e += 4.0 * P.lap[i] * P.lap[j] * (P.inv_g_sqr * omt + P.inv_gp_sqr * omc);
+                plaq2 += 1.0 - omt;
+                plaq1 += cos(wF);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if (j == i) continue;
+                const int mj = n.m[j];
+                const int dg = n.dg[i][j];
+                const Q<C> Uj_mj = ld4<C>(now.q[j], mj);
+                const Q<C> Ui_mj = ld4<C>(now.q[i], mj);
+                const Q<C> Uj_dg = ld4<C>(now.q[j], dg);
+                const C neigh = -ld1<C>(now.th[j], dg) - ld1<C>(now.th[i], mj) + ld1<C>(now.th[j], mj) + th[i];
+                MgY[i] -= sin_(neigh) * lap[j];
+                const Q<C> B = qmul(qmul(Uj_mj, qconj(Ui_mj)), qconj(Uj_dg));
+                SB[i] = qadd_scaled(SB[i], lap[j], B);
+            }
+        }
+        C Mg[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            C a1, a2, a3, b1, b2, b3;
+            qmul_vec(SA[i], qconj(U[i]), a1, a2, a3);
+            qmul_vec(U[i], SB[i], b1, b2, b3);
+            Mg[i][0] = a1 - b1;
+            Mg[i][1] = a2 - b2;
+            Mg[i][2] = a3 - b3;
+        }
+
+        // ---- scalar sector: covariant Laplacian D and currents J ----
+        Q<C> fc[ND];
+#pragma unroll
+        for (int db = 0; db < ND; db++) fc[db] = ld4<C>(now.ph[db], n.c);
+        Q<C> D[ND];
+#pragma unroll
+        for (int db = 0; db < ND; db++) {
+            const C w = (C)(-2.0 * (P.lap[0] + P.lap[1] + P.lap[2]));
+            D[db] = {w * fc[db].w, w * fc[db].x, w * fc[db].y, w * fc[db].z};
+        }
+        C J[3][4];
+        double grad_e = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            C sn, cs;
+            sc_(th[a], sn, cs);
+            C sm, cm;
+            const C thm = ld1<C>(now.th[a], n.m[a]);
+            sc_(thm, sm, cm);
+            const Q<C> Um = ld4<C>(now.q[a], n.m[a]);
+            const Q<C> Uc = qconj(U[a]);
+            C j0 = 0, j1 = 0, j2 = 0, j3 = 0;
+#pragma unroll
+            for (int db = 0; db < ND; db++) {
+                const Q<C> fp = ld4<C>(now.ph[db], n.p[a]);
+                const Q<C> fm = ld4<C>(now.ph[db], n.m[a]);
+                // D: U_a(x-a) phi(x-a) + U_a(x)^dag phi(x+a)
+                const Q<C> tm = transport(Um, cm, sm, fm);
+                const Q<C> tp = transport(Uc, cs, -sn, fp);
+                D[db] = qadd_scaled(D[db], lap[a], tm);
+                D[db] = qadd_scaled(D[db], lap[a], tp);
+                // J: Im of (U_a(x) phi(x))^dag sigma phi(x+a)
+                const Q<C> t = transport(U[a], cs, sn, fc[db]);
+                j0 += t.w * fp.x - t.x * fp.w + t.y * fp.z - t.z * fp.y;
+                j1 += t.w * fp.z - t.x * fp.y + t.y * fp.x - t.z * fp.w;
+                j2 += -t.w * fp.y - t.x * fp.z + t.y * fp.w + t.z * fp.x;
+                j3 += t.w * fp.x - t.x * fp.w - t.y * fp.z + t.z * fp.y;
+                if (ENERGY) {
+                    const double e0 = (double)fp.w - t.w, e1 = (double)fp.x - t.x;
+                    const double e2 = (double)fp.y - t.y, e3 = (double)fp.z - t.z;
+                    grad_e += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                }
+            }
+            J[a][0] = (C)0.25 * j0;
+            J[a][1] = (C)0.25 * j1;
+            J[a][2] = (C)0.25 * j2;
+            J[a][3] = (C)0.25 * j3;
+        }
+
+        // ---- potential dV/dphi ----
+        C Pot[ND][4];
+        double pot_e = 0.0;
+        if (MODEL == kModelSM) {
+            const C fsq = fc[0].w * fc[0].w + fc[0].x * fc[0].x + fc[0].y * fc[0].y + fc[0].z * fc[0].z;
+            const C k = (C)P.lambda * (fsq - (C)P.eta_sqr);
+            Pot[0][0] = k * fc[0].w;
+            Pot[0][1] = k * fc[0].x;
+            Pot[0][2] = k * fc[0].y;
+            Pot[0][3] = k * fc[0].z;
+            if (ENERGY) {
+                const double t = (double)fsq - P.eta_sqr;
+                pot_e = 0.25 * P.lambda * t * t;
+            }
+        } else {
+            const Q<C> f1 = fc[0], f2 = fc[ND - 1];
+            const C s1 = f1.w * f1.w + f1.x * f1.x + f1.y * f1.y + f1.z * f1.z;
+            const C s2 = f2.w * f2.w + f2.x * f2.x + f2.y * f2.y + f2.z * f2.z;
+            const C dot = P.break_son ? f1.w * f2.w + f1.x * f2.x + f1.y * f2.y + f1.z * f2.z : (C)0;
+            const C anti = (P.break_son && P.break_uhalfn) ? f1.w * f2.x - f1.x * f2.w + f1.y * f2.z - f1.z * f2.y : (C)0;
+            const C a1 = (C)(-2.0 * P.m1) + (C)(4.0 * P.l1) * s1 + (C)(2.0 * P.l3) * s2;
+            const C a2 = (C)(-2.0 * P.m2) + (C)(4.0 * P.l2) * s2 + (C)(2.0 * P.l3) * s1;
+            // single SO(N): (-m12r + 2 l4p5 dot + l6r s1 + l7r s2) f_other + 2 l6r|l7r dot f_self
+            const C bs = (C)(-P.m12r) + (C)(2.0 * P.l4p5) * dot + (C)P.l6r * s1 + (C)P.l7r * s2;
+            const C b1 = (C)(2.0 * P.l6r) * dot, b2 = (C)(2.0 * P.l7r) * dot;
+            // U(N/2): (m12i + 2 l4m5 anti - 2 l5i dot - l6i s1 - l7i s2) J f_other - 2 l5i anti f_other - 2 l6i|l7i anti f_self
+            const C cu = (C)P.m12i + (C)(2.0 * P.l4m5) * anti - (C)(2.0 * P.l5i) * dot - (C)P.l6i * s1 - (C)P.l7i * s2;
+            const C c5 = (C)(2.0 * P.l5i) * anti;
+            const C c1 = (C)(2.0 * P.l6i) * anti, c2 = (C)(2.0 * P.l7i) * anti;
+            const C f1v[4] = {f1.w, f1.x, f1.y, f1.z};
+            const C f2v[4] = {f2.w, f2.x, f2.y, f2.z};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int alt = 1 - 2 * (k % 2);
+                C v1 = a1 * f1v[k];
+                C v2 = a2 * f2v[k];
+                if (P.break_son) {
+                    v1 += bs * f2v[k] + b1 * f1v[k];
+                    v2 += bs * f1v[k] + b2 * f2v[k];
+                    if (P.break_uhalfn) {
+                        v1 += cu * (C)alt * f2v[k + alt] - c5 * f2v[k] - c1 * f1v[k];
+                        v2 += -cu * (C)alt * f1v[k + alt] - c5 * f1v[k] - c2 * f2v[k];
+                    }
+                }
+                Pot[0][k] = v1;
+                Pot[ND - 1][k] = v2;
+            }
+            if (ENERGY) {
+                const double d1 = s1, d2 = s2, dd = dot, da = anti;
+                double v = -P.m1 * d1 - P.m2 * d2 + P.l1 * d1 * d1 + P.l2 * d2 * d2 + P.l3 * d1 * d2;
+                if (P.break_son) {
+                    v += -P.m12r * dd + P.l4p5 * dd * dd + P.l6r * d1 * dd + P.l7r * d2 * dd;
+                    if (P.break_uhalfn)
+                        v += P.m12i * da + P.l4m5 * da * da - 2.0 * P.l5i * dd * da - P.l6i * d1 * da - P.l7i * d2 * da;
+                }
+                if (P.apply_norm) v += P.energy_offset;
+                pot_e = v;
+            }
+        }
+
+        // ---- scalar leapfrog (Model.cpp:347-356), summed in FP64 ----
+        double kin_e = 0.0, phisq = 0.0;
+        bool finite = true;
+#pragma unroll
+        for (int db = 0; db < ND; db++) {
+            const Q<C> fpast = ld4<C>(past.ph[db], n.c);
+            const C fn[4] = {fc[db].w, fc[db].x, fc[db].y, fc[db].z};
+            const C fo[4] = {fpast.w, fpast.x, fpast.y, fpast.z};
+            const C dd[4] = {D[db].w, D[db].x, D[db].y, D[db].z};
+            double out[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const C vel = fn[k] - fo[k];
+                const C acc = (C)P.dt2 * (dd[k] - Pot[db][k]);
+                out[k] = (double)fn[k] + ((double)vel + (double)acc - P.damping_step * (double)vel);
+                finite = finite && isfinite(out[k]);
+                if (ENERGY) {
+                    const double v = (double)vel / P.dt;
+                    kin_e += 0.5 * v * v;
+                    phisq += (double)fn[k] * (double)fn[k];
+                }
+            }
+            st4(past.ph[db], n.c, (S)out[0], (S)out[1], (S)out[2], (S)out[3]);
+        }
+
+        // ---- link update (WilsonLoops/Source/StandardModel.cpp:456-514) ----
+        double elec_e = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const Q<double> Un = qcast<double>(U[d]);
+            const Q<double> Up = ld4<double>(past.q[d], n.c);
+            const C thp = ld1<C>(past.th[d], n.c);
+            // link momentum: vec(U_now U_past^dag) and sin(theta_now - theta_past), FP64 products
+            const Q<double> E = qmul(Un, qconj(Up));
+            const C dth = th[d] - thp;
+            const double elY = (double)sin_(dth);
+            const double gY = P.gsq[0], gI = P.gsq[1];
+            const double keep = 1.0 - P.damping_step;
+            const double R0 = keep * elY + P.dt2 * ((double)MgY[d] + gY * (double)J[d][0]);
+            const double R1 = keep * E.x + P.dt2 * ((double)Mg[d][0] + gI * (double)J[d][1]);
+            const double R2 = keep * E.y + P.dt2 * ((double)Mg[d][1] + gI * (double)J[d][2]);
+            const double R3 = keep * E.z + P.dt2 * ((double)Mg[d][2] + gI * (double)J[d][3]);
+            if (ENERGY) {
+                const double dthd = (double)dth;
+                elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt
+                          * (P.inv_g_sqr * one_minus_trace(E) + P.inv_gp_sqr * 2.0 * sin(0.5 * dthd) * sin(0.5 * dthd));
+            }
+            if (R0 * R0 > 1.0) warn |= kWarnAsin;
+            // theta(t+dt) = theta(t) + asin(RHS_Y)
+            const double thn = (double)th[d] + (double)asin_((C)R0);
+            // u = (sqrt(1-|c|^2), c); U(t+dt) = normalise(u U(t)).  u - 1 = (-|c|^2/(1+sqrt(1-|c|^2)), c)
+            const double cm = R1 * R1 + R2 * R2 + R3 * R3;
+            if (cm > 1.0) warn |= kWarnSqrt;
+            const C cmC = (C)cm;
+            const C u0m1 = -cmC / ((C)1 + sqrt_((C)1 - cmC));
+            const Q<C> du = {u0m1, (C)R1, (C)R2, (C)R3};
+            const Q<C> dU = qmul(du, U[d]);  // (u - 1) U(t): small, FP32 suffices in the mixed form
+            Q<double> Unew = {Un.w + (double)dU.w, Un.x + (double)dU.x, Un.y + (double)dU.y, Un.z + (double)dU.z};
+            const double n2 = Unew.w * Unew.w + Unew.x * Unew.x + Unew.y * Unew.y + Unew.z * Unew.z;
+            const double sc = rsqrt(n2);
+            Unew = {Unew.w * sc, Unew.x * sc, Unew.y * sc, Unew.z * sc};
+            finite = finite && isfinite(thn) && isfinite(Unew.w) && isfinite(Unew.x) && isfinite(Unew.y) &&
+                     isfinite(Unew.z);
+            past.th[d][n.c] = (S)thn;
+            st4(past.q[d], n.c, (S)Unew.w, (S)Unew.x, (S)Unew.y, (S)Unew.z);
+        }
+        if (!finite) warn |= kWarnNonFinite;
+
+        if (ENERGY) {
+            obs[kObsPotential] = pot_e;
+            obs[kObsGradient] = grad_e;
+            obs[kObsKinetic] = kin_e;
+            obs[kObsMagnetic] = mag_e;
+            obs[kObsElectric] = elec_e;
+            obs[kObsEnergy] = pot_e + grad_e + kin_e + mag_e + elec_e;
+            obs[kObsPlaqSU2] = plaq2;
+            obs[kObsPlaqU1] = plaq1;
+            obs[kObsPhiSq] = phisq;
+        }
+    }
+
+    if (ENERGY) {
+        const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        block_reduce_store<kObsCount>(obs, partials + (size_t)b * kObsCount, kObsCount);
+    }
+    if (warn) atomicOr(status, warn);
+}
+
+// Gauss-law residual after a step, FP64 for both forms (GaugeCondition.cpp:117-165 semantics).
+template <class S, int MODEL>
+__global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
+                                                         double* partials)
+{
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x = blockIdx.z;
+    double v[kGaussSlots];
+#pragma unroll
+    for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
+    if (z < P.nz && y < P.ny) {
+        const Nbr n = neighbours(P, x, y, z);
+        double el[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double la = ld1<double>(fut.th[d], n.c) - ld1<double>(now.th[d], n.c);
+            const double na = ld1<double>(fut.th[d], n.m[d]) - ld1<double>(now.th[d], n.m[d]);
+            el[0] += (sin(la) - sin(na)) * P.lap[d];
+            // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
+            double a1, a2, a3, b1, b2, b3;
+            qmul_vec(qconj(ld4<double>(now.q[d], n.c)), ld4<double>(fut.q[d], n.c), a1, a2, a3);
+            qmul_vec(ld4<double>(fut.q[d], n.m[d]), qconj(ld4<double>(now.q[d], n.m[d])), b1, b2, b3);
+            el[1] += (a1 - b1) * P.lap[d];
+            el[2] += (a2 - b2) * P.lap[d];
+            el[3] += (a3 - b3) * P.lap[d];
+        }
+        double gr[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int db = 0; db < ND; db++) {
+            const Q<double> p = ld4<double>(now.ph[db], n.c);
+            const Q<double> q = ld4<double>(fut.ph[db], n.c);
+            gr[0] += 0.25 * (p.w * q.x - p.x * q.w + p.y * q.z - p.z * q.y);
+            gr[1] += 0.25 * (p.w * q.z - p.x * q.y + p.y * q.x - p.z * q.w);
+            gr[2] += 0.25 * (-p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x);
+            gr[3] += 0.25 * (p.w * q.x - p.x * q.w - p.y * q.z + p.z * q.y);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const double av = fabs(el[k] - P.gsq[k] * gr[k]);
+            v[k] = av;
+            v[4 + k] = av;
+        }
+    }
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    block_reduce_store<kGaussSlots>(v, partials + (size_t)blk * kGaussSlots, 4);
+}
+
+}  // namespace
+
+int fast_launch_blocks(const StepParams& P, int /*variant*/) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
+int fast_gauss_blocks(const StepParams& P) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
+
+template <class S, int MODEL>
+cudaError_t launch_fast_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                             double* partials, bool energy, int /*variant*/, cudaStream_t stream)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    if (energy)
+        fast_step_kernel<S, MODEL, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+    else
+        fast_step_kernel<S, MODEL, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+    return cudaGetLastError();
+}
+
+template <class S, int MODEL>
+cudaError_t launch_fast_gauss(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
+                              cudaStream_t stream)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    fast_gauss_kernel<S, MODEL><<<grid, block, 0, stream>>>(P, now, fut, partials);
+    return cudaGetLastError();
+}
+
+#define GFT_INSTANTIATE_FAST(S, M)                                                                                   \
+    template cudaError_t launch_fast_step<S, M>(const StepParams&, const LevelPtrs<S>&, const LevelPtrs<S>&,         \
+                                                unsigned*, double*, bool, int, cudaStream_t);                         \
+    template cudaError_t launch_fast_gauss<S, M>(const StepParams&, const LevelPtrs<S>&, const LevelPtrs<S>&,        \
+                                                 double*, cudaStream_t);
+GFT_INSTANTIATE_FAST(float, kModelSM)
+GFT_INSTANTIATE_FAST(float, kModel2HDM)
+GFT_INSTANTIATE_FAST(double, kModelSM)
+GFT_INSTANTIATE_FAST(double, kModel2HDM)
+
+}  // namespace gft

@@ -1,0 +1,50 @@
+// gft_launch.h -- host-side launchers of the device kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gft_device.cuh"
+
+namespace gft {
+
+// Reference-arithmetic form (gft_ref_kernels.cu, compiled with -fmad=false).
+template <class S, int MODEL>
+cudaError_t launch_ref_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                            double* partials, bool energy, cudaStream_t stream);
+template <class S, int MODEL>
+cudaError_t launch_ref_gauss(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
+                             cudaStream_t stream);
+int ref_launch_blocks(const StepParams& P);
+
+// Throughput forms (gft_fast_kernels.cu): FP64 plain form (S = double) and
+// mixed form (S = float).
+template <class S, int MODEL>
+cudaError_t launch_fast_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                             double* partials, bool energy, int variant, cudaStream_t stream);
+template <class S, int MODEL>
+cudaError_t launch_fast_gauss(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
+                              cudaStream_t stream);
+int fast_launch_blocks(const StepParams& P, int variant);
+int fast_gauss_blocks(const StepParams& P);
+
+// Auxiliary kernels (gft_aux_kernels.cu).
+template <class S, class H>
+cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s);
+template <class S, class H>
+cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s);
+
+struct ICParams {
+    unsigned long long seed;
+    double mean[8], sigma[8];
+    double theta_sigma, eps_sigma, wall_width, wall_value;
+};
+template <class S>
+cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic, LevelPtrs<S> a, LevelPtrs<S> b,
+                               cudaStream_t s);
+
+// Sum (slots < max_from, compensated) or max (slots >= max_from) the per-block
+// partials [nblocks][nslots] into out[nslots], scaled by scale[slot].
+cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_host,
+                            double* out, cudaStream_t s);
+
+}  // namespace gft

@@ -1,0 +1,237 @@
+"""Python front end of the B200 evolver (over the C ABI in include/gft.h).
+
+``Evolver`` owns one device handle: both time levels of the fields, the model
+parameters, the step counter and the analysers' logging cadence -- the state
+the reference keeps in ``Lattice`` and ``Model`` (Core/Header/Lattice.hpp:22-212,
+Core/Header/Model.hpp:23-266).  Host arrays use the reference layout
+``scalars[2, nx, ny, nz, nsc]``, ``vectors[2, nx, ny, nz, 15]``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import asdict, dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+FORMS = {
+    "ref32": (_lib.GFT_FORM_REF, 4),
+    "ref64": (_lib.GFT_FORM_REF, 8),
+    "fp64": (_lib.GFT_FORM_FP64, 8),
+    "mixed": (_lib.GFT_FORM_MIXED, 4),
+}
+STORAGE_DTYPE = {"ref32": np.float32, "ref64": np.float64, "fp64": np.float64, "mixed": np.float32}
+
+
+@dataclass
+class LatticeParams:
+    """Model and lattice parameters (the values of the reference's .cfg files)."""
+
+    model: int = _lib.GFT_MODEL_SM
+    nx: int = 32
+    ny: int = 32
+    nz: int = 32
+    dx: float = 1.0
+    dy: float = 1.0
+    dz: float = 1.0
+    dt: float = 0.05
+    g: float = 0.65
+    gp: float = 0.35
+    div_tol: float = 1e-9
+    damping: float = 0.0
+    nt_damped: int = 0
+    lam: float = 0.13
+    eta_sqr: float = 1.0
+    m1: float = 0.5
+    m2: float = 0.5
+    l1: float = 0.065
+    l2: float = 0.065
+    l3: float = 0.2
+    m12r: float = 0.2
+    l4p5: float = -0.1
+    l6r: float = 0.0
+    l7r: float = 0.0
+    m12i: float = 0.0
+    l4m5: float = 0.0
+    l5i: float = 0.0
+    l6i: float = 0.0
+    l7i: float = 0.0
+    break_son: int = 1
+    break_uhalfn: int = 1
+    apply_norm: int = 0
+    energy_offset: float = 0.0
+    energy_every: int = 0
+    gauss_every: int = 0
+
+    @property
+    def nsc(self) -> int:
+        return 4 if self.model == _lib.GFT_MODEL_SM else 8
+
+    @property
+    def nsite(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def as_dict(self) -> dict:
+        return asdict(self)
+
+
+@dataclass
+class InitialData:
+    """Device-generated initial data (both levels equal: E = 0, pi = 0)."""
+
+    seed: int = 1
+    mean: list = field(default_factory=lambda: [0.0] * 8)
+    sigma: list = field(default_factory=lambda: [0.1] * 8)
+    theta_sigma: float = 0.0
+    eps_sigma: float = 0.0
+    wall_width: float = 0.0
+    wall_value: float = 1.0
+
+
+ROW_KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric")
+
+
+def _row_dict(r: _lib.GftObservables) -> dict:
+    d = {"time_iter": r.time_iter, "has_energy": bool(r.has_energy), "has_gauss": bool(r.has_gauss)}
+    for k in ROW_KEYS:
+        d[k] = r.__getattribute__(k)
+    d["gauss_int"] = list(r.gauss_int)
+    d["gauss_max"] = list(r.gauss_max)
+    d["plaq_su2"], d["plaq_u1"], d["phi_sq"] = r.plaq_su2, r.plaq_u1, r.phi_sq
+    return d
+
+
+class Evolver:
+    """One lattice on one GPU, evolved by the CUDA kernels of libgft_b200.so."""
+
+    def __init__(self, params: LatticeParams, form: str = "mixed", device: int = 0):
+        if form not in FORMS:
+            raise ValueError(f"unknown form {form!r}; choose one of {sorted(FORMS)}")
+        self.lib = _lib.load()
+        self.params = params
+        self.form = form
+        self.dtype = STORAGE_DTYPE[form]
+        cfg = _lib.GftConfig()
+        for name, _ in _lib.GftConfig._fields_:
+            if name in ("form", "storage_bytes", "device"):
+                continue
+            setattr(cfg, name, getattr(params, name))
+        cfg.form, cfg.storage_bytes = FORMS[form]
+        cfg.device = device
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.last_warnings = 0
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gft_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- fields --------------------------------------------------------------
+    def _shapes(self):
+        p = self.params
+        return (2, p.nx, p.ny, p.nz, p.nsc), (2, p.nx, p.ny, p.nz, 15)
+
+    def upload(self, scalars: np.ndarray, vectors: np.ndarray, time_iter: int = 0) -> None:
+        ss, vs = self._shapes()
+        if scalars.shape != ss or vectors.shape != vs:
+            raise ValueError(f"expected shapes {ss} and {vs}, got {scalars.shape} and {vectors.shape}")
+        if scalars.dtype == np.float64:
+            sc = np.ascontiguousarray(scalars)
+            ve = np.ascontiguousarray(vectors, dtype=np.float64)
+            fn, ptr = self.lib.gft_upload_f64, ctypes.POINTER(ctypes.c_double)
+        else:
+            sc = np.ascontiguousarray(scalars, dtype=np.float32)
+            ve = np.ascontiguousarray(vectors, dtype=np.float32)
+            fn, ptr = self.lib.gft_upload_f32, ctypes.POINTER(ctypes.c_float)
+        _lib.check(fn(self.h, sc.ctypes.data_as(ptr), ve.ctypes.data_as(ptr), int(time_iter)), self.h)
+
+    def upload_ptr(self, scalars_ptr: int, vectors_ptr: int, f64: bool, time_iter: int = 0) -> None:
+        """Upload from raw host pointers (e.g. pinned torch tensors)."""
+        if f64:
+            P = ctypes.POINTER(ctypes.c_double)
+            fn = self.lib.gft_upload_f64
+        else:
+            P = ctypes.POINTER(ctypes.c_float)
+            fn = self.lib.gft_upload_f32
+        _lib.check(fn(self.h, ctypes.cast(scalars_ptr, P), ctypes.cast(vectors_ptr, P), int(time_iter)), self.h)
+
+    def download(self, dtype=None):
+        dtype = np.dtype(dtype or self.dtype)
+        ss, vs = self._shapes()
+        sc = np.empty(ss, dtype=dtype)
+        ve = np.empty(vs, dtype=dtype)
+        self.download_into(sc, ve)
+        return sc, ve
+
+    def download_into(self, sc: np.ndarray, ve: np.ndarray) -> None:
+        if sc.dtype == np.float64:
+            fn, ptr = self.lib.gft_download_f64, ctypes.POINTER(ctypes.c_double)
+        else:
+            fn, ptr = self.lib.gft_download_f32, ctypes.POINTER(ctypes.c_float)
+        _lib.check(fn(self.h, sc.ctypes.data_as(ptr), ve.ctypes.data_as(ptr)), self.h)
+
+    def download_ptr(self, scalars_ptr: int, vectors_ptr: int, f64: bool) -> None:
+        if f64:
+            P, fn = ctypes.POINTER(ctypes.c_double), self.lib.gft_download_f64
+        else:
+            P, fn = ctypes.POINTER(ctypes.c_float), self.lib.gft_download_f32
+        _lib.check(fn(self.h, ctypes.cast(scalars_ptr, P), ctypes.cast(vectors_ptr, P)), self.h)
+
+    def init_fields(self, ic: InitialData) -> None:
+        c = _lib.GftIC()
+        c.seed = int(ic.seed)
+        for k in range(8):
+            c.mean[k] = float((list(ic.mean) + [0.0] * 8)[k])
+            c.sigma[k] = float((list(ic.sigma) + [0.0] * 8)[k])
+        c.theta_sigma, c.eps_sigma = float(ic.theta_sigma), float(ic.eps_sigma)
+        c.wall_width, c.wall_value = float(ic.wall_width), float(ic.wall_value)
+        _lib.check(self.lib.gft_init_fields(self.h, ctypes.byref(c)), self.h)
+
+    # -- time stepping -------------------------------------------------------
+    def evolve(self, n_steps: int, max_rows: int | None = None) -> list:
+        """Advance n_steps; returns the analyser rows logged on the way."""
+        if max_rows is None:
+            max_rows = n_steps + 1
+        rows = (_lib.GftObservables * max(max_rows, 1))()
+        n = ctypes.c_int(0)
+        self.last_warnings = _lib.check(
+            self.lib.gft_evolve(self.h, int(n_steps), rows, int(max_rows), ctypes.byref(n)), self.h)
+        return [_row_dict(rows[i]) for i in range(n.value)]
+
+    def observe(self) -> dict:
+        r = _lib.GftObservables()
+        _lib.check(self.lib.gft_observe(self.h, ctypes.byref(r)), self.h)
+        return _row_dict(r)
+
+    @property
+    def time_iter(self) -> int:
+        return int(self.lib.gft_time_iter(self.h))
+
+    def step_kernel_ms(self):
+        n = ctypes.c_int(0)
+        ms = self.lib.gft_step_kernel_ms(self.h, ctypes.byref(n))
+        return ms, n.value
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.gft_stream(self.h) or 0)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.gft_device_bytes(self.h))

@@ -1,0 +1,158 @@
+/*
+ * gft.h -- C ABI of the B200 lattice evolver (libgft_b200.so).
+ *
+ * Drop-in boundary for GFTEvolver's time stepper.  The reference evolves the
+ * lattice through per-site virtual calls (Potential, Gradient, WilsonLoop,
+ * BoundaryCondition, Analyser) from the loop in Lattice::evolve
+ * (Core/Source/Lattice.cpp:755-876) and each Periodic::evolve
+ * (BoundaryConditions/Source/Periodic.cpp:205-268).  This library replaces that
+ * loop for the whole lattice at once: the plugin choices become a model
+ * selector plus parameters, the periodic boundary becomes index wrap, and the
+ * Energy / GaugeCondition analysers become fused device reductions that fill
+ * gft_observables rows.
+ *
+ * Conventions
+ *   - Host field buffers use the reference layout (Lattice.cpp:358-367,
+ *     658-671): scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][15] with
+ *     per direction [theta_Y, c0, c1, c2, c3] (quaternion representation).
+ *     Level index = the reference's time slot; at time step time_iter the
+ *     "now" slot is (time_iter + 1) % 2 (Lattice.cpp:773-774).
+ *   - Device memory is owned by the handle; host buffers are caller-owned and
+ *     copied.  One handle per CUDA stream; thread-safe across handles, not
+ *     within one handle.
+ *   - Return value: 0 = success, < 0 = error (see GFT_E_*), > 0 = warning
+ *     bitmask (GFT_W_*).  The reference prints "Panic" and continues when an
+ *     asin or sqrt argument leaves its domain
+ *     (WilsonLoops/Source/StandardModel.cpp:474-491); here the condition is
+ *     counted on the device and reported as a warning bit.
+ */
+#ifndef GFT_H
+#define GFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GFT_OK 0
+#define GFT_E_INVALID (-1)      /* bad argument / configuration (reference: std::runtime_error at construction) */
+#define GFT_E_UNSUPPORTED (-2)  /* combination not built (e.g. generator representation) */
+#define GFT_E_CUDA (-3)         /* CUDA runtime error; see gft_last_error */
+#define GFT_E_NOMEM (-4)        /* device allocation failed */
+#define GFT_E_STATE (-5)        /* call out of order (e.g. evolve before upload) */
+
+#define GFT_W_ASIN_DOMAIN 1     /* |RHS_Y| > 1 somewhere (theta update used asin outside [-1,1]) */
+#define GFT_W_SQRT_DOMAIN 2     /* |c|^2 > 1 somewhere (SU(2) update used sqrt of a negative number) */
+#define GFT_W_NONFINITE 4       /* a non-finite value was written */
+
+/* ---- model / form selectors -------------------------------------------- */
+/* Model.cfg plugin triples (Core/Header/Model.hpp:19-21) that are built. */
+#define GFT_MODEL_SM 1    /* SO_N potential + Gradients::StandardModel + WilsonLoops::StandardModel */
+#define GFT_MODEL_2HDM 2  /* Double_SO_N + Gradients::TwoHDM + WilsonLoops::TwoHDM (gaugeNum = 4) */
+
+/* Arithmetic forms. */
+#define GFT_FORM_REF 0    /* reference arithmetic: per-site math in FP64 in the reference's operation
+                             order; storage = `storage_bytes` (4: the reference as shipped, 8: FP64 storage) */
+#define GFT_FORM_FP64 1   /* plain FP64 form: FP64 storage and math, reassociated for throughput */
+#define GFT_FORM_MIXED 2  /* FP32 storage and force math; FP64 for link momentum, updates,
+                             renormalisation and reductions */
+
+typedef struct gft_config {
+    int model;                     /* GFT_MODEL_* */
+    int form;                      /* GFT_FORM_* */
+    int storage_bytes;             /* GFT_FORM_REF only: 4 or 8 */
+    int device;                    /* CUDA device ordinal */
+    int nx, ny, nz;                /* Core/Config/Lattice.cfg */
+    double dx, dy, dz, dt;
+    double g, gp;                  /* WilsonLoops/Config/*.cfg */
+    double div_tol;                /* division-by-zero tolerance for the inverse couplings */
+    double damping;                /* Core/Config/Model.cfg: damping factor */
+    int nt_damped;                 /*   number of damped time steps */
+    double lambda, eta_sqr;        /* Potentials/Config/SO_N.cfg */
+    double m1, m2, l1, l2, l3;     /* Potentials/Config/Double_SO_N.cfg */
+    double m12r, l4p5, l6r, l7r;
+    double m12i, l4m5, l5i, l6i, l7i;
+    int break_son, break_uhalfn, apply_norm;
+    double energy_offset;
+    int energy_every;              /* Analysers/Config/Energy.cfg output frequency; 0 = no Energy analyser */
+    int gauss_every;               /* Analysers/Config/GaugeCondition.cfg frequency; 0 = off */
+} gft_config;
+
+/* One row of global observables (Analysers/Source/Energy.cpp:169-220,
+ * Analysers/Source/GaugeCondition.cpp:167-226).  Energies are integrated over
+ * the lattice (sum x dx dy dz); the Gauss entries are the integrated and the
+ * maximum |violation| per constraint equation.  plaq_* and phi_sq are means
+ * with no reference counterpart. */
+typedef struct gft_observables {
+    int time_iter;
+    int has_energy, has_gauss;
+    double energy, potential, gradient, kinetic, magnetic, electric;
+    double gauss_int[4], gauss_max[4];
+    double plaq_su2, plaq_u1, phi_sq;
+} gft_observables;
+
+/* Initial data generated on the device (no reference counterpart: the
+ * reference ships only RandomUniform, InitialConditions/Source/RandomUniform.cpp:60-77).
+ * Both time levels are set equal (E = 0, pi = 0).  Scalars: component c ~
+ * N(mean[c], sigma[c]^2), plus a periodic tanh double wall on component 0 when
+ * wall_width > 0.  Links: theta_Y ~ N(0, theta_sigma^2); SU(2) =
+ * (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform on S^2. */
+typedef struct gft_ic {
+    uint64_t seed;
+    double mean[8], sigma[8];
+    double theta_sigma, eps_sigma;
+    double wall_width, wall_value;
+} gft_ic;
+
+typedef struct gft_handle gft_handle;
+
+/* Lattice construction (replaces Lattice::Lattice, Core/Source/Lattice.cpp:679-722,
+ * and Model::configure, Core/Source/Model.cpp:145-234). */
+int gft_create(const gft_config* cfg, gft_handle** out);
+void gft_destroy(gft_handle* h);
+
+/* Field transfer in the reference layout (both levels).  `time_iter` is the
+ * reference step counter the data belongs to (0 for initial data). */
+int gft_upload_f32(gft_handle* h, const float* scalars, const float* vectors, int time_iter);
+int gft_upload_f64(gft_handle* h, const double* scalars, const double* vectors, int time_iter);
+int gft_download_f32(gft_handle* h, float* scalars, float* vectors);
+int gft_download_f64(gft_handle* h, double* scalars, double* vectors);
+
+/* Generate initial data on the device (InitialCondition::setInitialFields,
+ * InitialConditions/Header/InitialCondition.hpp:24). */
+int gft_init_fields(gft_handle* h, const gft_ic* ic);
+
+/* Evolve n_steps time steps (the body of Lattice::evolve's time loop).  Rows
+ * are written for every step on which an analyser logs (time_iter % every ==
+ * 0); *n_rows receives the number written (at most max_rows). */
+int gft_evolve(gft_handle* h, int n_steps, gft_observables* rows, int max_rows, int* n_rows);
+
+/* Observables of the current state without stepping (energy terms at the
+ * current level pair, plaquette means, <phi^dag phi>). */
+int gft_observe(gft_handle* h, gft_observables* row);
+
+/* Current reference step counter. */
+int gft_time_iter(const gft_handle* h);
+
+/* Device-resident access for callers that keep the state on the GPU:
+ * the stream the handle launches on, and the number of device bytes it holds. */
+void* gft_stream(gft_handle* h);
+size_t gft_device_bytes(const gft_handle* h);
+
+/* Average duration in milliseconds of the step kernel over the launches since
+ * the last call (CUDA events on the handle's stream); 0 if none. */
+double gft_step_kernel_ms(gft_handle* h, int* launches);
+
+/* Message for the last error on this handle (or the last global error if h is NULL). */
+const char* gft_last_error(const gft_handle* h);
+
+/* Library / build information. */
+const char* gft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,80 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference itself.
+
+Each fixture holds the initial data, the reference's fields after ``nt``
+steps and the Energy / GaugeCondition analysers' raw sums per logged step,
+produced by the unmodified GFTEvolver sources compiled by
+``oracle/build_ref.sh`` (``oracle/_ref/ref32`` = float storage as shipped,
+``oracle/_ref/ref64`` = the same sources with float -> double).
+
+Run from the repository root in the container where the reference is
+mounted:  ``sh oracle/build_ref.sh && python tests/golden/make_golden.py``
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as orc  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+RANDOM_LINKS = dict(theta_sigma=0.1, eps_sigma=0.1)
+
+# name -> (params overrides, IC overrides, steps, storage list)
+CASES = {
+    "sm_4x5x6": (dict(model=orc.MODEL_SM, nx=4, ny=5, nz=6, energy_every=2, gauss_every=3),
+                 dict(seed=11, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 10, ("f32", "f64")),
+    "2hdm_5x4x3": (dict(model=orc.MODEL_2HDM, nx=5, ny=4, nz=3, energy_every=2, gauss_every=3),
+                   dict(seed=12, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 10, ("f32", "f64")),
+    "sm_1x1x1": (dict(model=orc.MODEL_SM, nx=1, ny=1, nz=1, energy_every=1, gauss_every=1),
+                 dict(seed=13, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 5, ("f32",)),
+    "sm_2x2x2": (dict(model=orc.MODEL_SM, nx=2, ny=2, nz=2, energy_every=1, gauss_every=2),
+                 dict(seed=14, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 5, ("f32", "f64")),
+    "sm_3x1x7": (dict(model=orc.MODEL_SM, nx=3, ny=1, nz=7, energy_every=1, gauss_every=1),
+                 dict(seed=15, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 5, ("f32",)),
+    "sm_damped_aniso_6x5x4": (dict(model=orc.MODEL_SM, nx=6, ny=5, nz=4, dx=0.5, dy=0.7, dz=1.3, damping=1.0,
+                                   nt_damped=4, energy_every=3, gauss_every=2),
+                              dict(seed=16, mean=[0.5] * 8, sigma=[0.2] * 8, **RANDOM_LINKS), 8, ("f32",)),
+    "sm_identity_8x8x8": (dict(model=orc.MODEL_SM, nx=8, ny=8, nz=8, energy_every=5, gauss_every=5),
+                          dict(seed=17, mean=[0.0] * 8, sigma=[0.1] * 8), 10, ("f32", "f64")),
+    "2hdm_wall_4x4x12": (dict(model=orc.MODEL_2HDM, nx=4, ny=4, nz=12, energy_every=4, gauss_every=4),
+                         dict(seed=18, mean=[0.0] * 8, sigma=[0.05] * 8, wall_width=2.0, wall_value=1.0), 8, ("f64",)),
+}
+
+
+def make(name: str) -> None:
+    pover, icover, nt, storages = CASES[name]
+    p = orc.Params(**pover)
+    ic = orc.ICSpec(**icover)
+    for st in storages:
+        fp64 = st == "f64"
+        dtype = np.float64 if fp64 else np.float32
+        sc, ve = orc.init_fields(p, ic, dtype)
+        rs, rv, rows, _ = refrun.run(p, sc, ve, nt, fp64=fp64)
+        meta = {"params": p.__dict__, "ic": ic.__dict__, "nt": nt, "storage": st,
+                "generator": "oracle/_ref/" + ("ref64" if fp64 else "ref32")}
+        out = os.path.join(HERE, f"{name}_{st}.npz")
+        np.savez_compressed(
+            out, ic_scalars=sc, ic_vectors=ve, scalars=rs, vectors=rv,
+            row_time_iter=np.array([r["time_iter"] for r in rows], dtype=np.int64),
+            row_has_energy=np.array([r["has_energy"] for r in rows], dtype=bool),
+            row_has_gauss=np.array([r["has_gauss"] for r in rows], dtype=bool),
+            row_ref_energy=np.array([r["ref_energy"] for r in rows], dtype=np.float64).reshape(-1, 6),
+            row_ref_gauss_int=np.array([r["ref_gauss_int"] for r in rows], dtype=np.float64).reshape(-1, 4),
+            row_gauss_max=np.array([r["gauss_max"] for r in rows], dtype=np.float64).reshape(-1, 4),
+            meta=np.array(json.dumps(meta)))
+        print("wrote", os.path.relpath(out, ROOT), os.path.getsize(out), "bytes")
+
+
+if __name__ == "__main__":
+    if not (refrun.available(False) and refrun.available(True)):
+        sys.exit("reference binaries missing: run sh oracle/build_ref.sh first")
+    for n in (sys.argv[1:] or CASES):
+        make(n)

@@ -1,0 +1,192 @@
+"""CUDA path vs the oracle and the reference's golden fixtures (GPU).
+
+Tolerances (stated per form):
+  ref32  float storage, reference arithmetic (FP64 per site, no FMA): equal to
+         the reference except where CUDA's sin/cos/asin differ from glibc in
+         the last bit; fields within 8 float ulps of |value| and at most 1% of
+         words differ at all; energies within 1e-6 relative.
+  ref64  double storage, reference arithmetic: fields within 1e-13 relative.
+  fp64   plain FP64 form (reassociated): fields within 1e-12 relative
+         (max |a - b| / max |b| per field array) after 10 steps, observables
+         within 1e-12 relative.
+  mixed  FP32 storage / mixed arithmetic vs the FP64 oracle: fields within
+         2e-6 absolute after 10 steps (|fields| ~ 1), energies 1e-6 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_files, load_golden
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = golden_files()
+
+
+def _lp(meta_params):
+    from gftevolver_b200 import LatticeParams
+    return LatticeParams(**meta_params)
+
+
+def run_gpu(params, form, sc, ve, nt, time_iter=0):
+    from gftevolver_b200 import Evolver
+    with Evolver(params, form=form) as ev:
+        ev.upload(sc, ve, time_iter)
+        rows = ev.evolve(nt)
+        warn = ev.last_warnings
+        osc, ove = ev.download(sc.dtype)
+    return osc, ove, rows, warn
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def ulp_close(a, b, nulp):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    tol = nulp * np.spacing(np.maximum(np.abs(a), np.abs(b)).astype(a.dtype))
+    return np.abs(a.astype(np.float64) - b.astype(np.float64)) <= tol.astype(np.float64) + 1e-30
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if p.endswith("_f32.npz")],
+                         ids=[os.path.basename(p) for p in GOLDEN if p.endswith("_f32.npz")])
+def test_ref32_matches_reference_golden(path):
+    z, meta = load_golden(path)
+    p = _lp(meta["params"])
+    sc, ve, rows, warn = run_gpu(p, "ref32", z["ic_scalars"], z["ic_vectors"], meta["nt"])
+    assert warn == 0
+    for got, want in ((sc, z["scalars"]), (ve, z["vectors"])):
+        ok = ulp_close(got, want, 8)
+        assert ok.all(), f"max diff {np.max(np.abs(got - want))}"
+        assert np.mean(got != want) <= 0.01
+    assert [r["time_iter"] for r in rows] == list(z["row_time_iter"])
+    dv = p.dx * p.dy * p.dz
+    for r, e, gm in zip(rows, z["row_ref_energy"], z["row_gauss_max"]):
+        if r["has_energy"]:
+            np.testing.assert_allclose(r["energy"], e[0] * dv, rtol=2e-5)
+        if r["has_gauss"]:
+            np.testing.assert_allclose(r["gauss_max"], gm, rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if p.endswith("_f64.npz")],
+                         ids=[os.path.basename(p) for p in GOLDEN if p.endswith("_f64.npz")])
+@pytest.mark.parametrize("form,tol", [("ref64", 1e-13), ("fp64", 1e-12)])
+def test_fp64_forms_match_reference_golden(path, form, tol):
+    z, meta = load_golden(path)
+    p = _lp(meta["params"])
+    sc, ve, rows, warn = run_gpu(p, form, z["ic_scalars"], z["ic_vectors"], meta["nt"])
+    assert warn == 0
+    assert rel_err(sc, z["scalars"]) <= tol
+    assert rel_err(ve, z["vectors"]) <= tol
+    dv = p.dx * p.dy * p.dz
+    for r, e, gm in zip(rows, z["row_ref_energy"], z["row_gauss_max"]):
+        if r["has_energy"]:
+            np.testing.assert_allclose(r["energy"], e[0] * dv, rtol=1e-11)
+        if r["has_gauss"]:
+            # Gauss residuals are rounding-level numbers; compare on the scale of the charge terms
+            assert np.all(np.abs(np.array(r["gauss_max"]) - gm) <= 1e-12)
+
+
+@pytest.mark.parametrize("model", [1, 2], ids=["sm", "2hdm"])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (5, 6, 7), (16, 12, 33)])
+def test_forms_vs_oracle_random(oracle_mod, model, shape):
+    """Random links and Gaussian scalars, 10 steps, all forms against the oracle."""
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=5, gauss_every=5)
+    ic = oracle_mod.ICSpec(seed=1234 + nx, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8,
+                           theta_sigma=0.1, eps_sigma=0.1)
+    p = _lp(op.__dict__)
+    sc64, ve64 = oracle_mod.init_fields(op, ic, np.float64)
+    o_sc, o_ve = sc64.copy(), ve64.copy()
+    o_rows, _ = oracle_mod.evolve(op, o_sc, o_ve, 10)
+    # plain FP64 form
+    sc, ve, rows, _ = run_gpu(p, "fp64", sc64, ve64, 10)
+    assert rel_err(sc, o_sc) <= 1e-12
+    assert rel_err(ve, o_ve) <= 1e-12
+    for a, b in zip(rows, o_rows):
+        assert a["time_iter"] == b["time_iter"]
+        if b["has_energy"]:
+            for k in ("energy", "potential", "gradient", "kinetic", "magnetic", "electric"):
+                assert abs(a[k] - b[k]) <= 1e-12 * max(abs(b["energy"]), 1.0), k
+            assert abs(a["plaq_su2"] - b["plaq_su2"]) <= 1e-13
+            assert abs(a["plaq_u1"] - b["plaq_u1"]) <= 1e-13
+            assert abs(a["phi_sq"] - b["phi_sq"]) <= 1e-12
+    # mixed form against the FP64 oracle
+    sc32, ve32 = oracle_mod.init_fields(op, ic, np.float32)
+    sc, ve, rows, _ = run_gpu(p, "mixed", sc32, ve32, 10)
+    assert np.max(np.abs(sc.astype(np.float64) - o_sc)) <= 2e-6
+    assert np.max(np.abs(ve.astype(np.float64) - o_ve)) <= 2e-6
+    for a, b in zip(rows, o_rows):
+        if b["has_energy"]:
+            assert abs(a["energy"] - b["energy"]) <= 1e-6 * abs(b["energy"])
+    # reference arithmetic, float storage, against the float oracle
+    o32_sc, o32_ve = sc32.copy(), ve32.copy()
+    oracle_mod.evolve(op, o32_sc, o32_ve, 10)
+    sc, ve, rows, _ = run_gpu(p, "ref32", sc32, ve32, 10)
+    assert ulp_close(sc, o32_sc, 8).all()
+    assert ulp_close(ve, o32_ve, 8).all()
+
+
+def test_time_iter_parity_and_chunking(oracle_mod):
+    """Evolving 3 + 4 steps equals 7 steps; the now/past slot follows time_iter (Lattice.cpp:773)."""
+    op = oracle_mod.Params(nx=6, ny=5, nz=4, energy_every=2, gauss_every=3)
+    ic = oracle_mod.ICSpec(seed=3, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(op, ic, np.float64)
+    o_sc, o_ve = sc.copy(), ve.copy()
+    o_rows, _ = oracle_mod.evolve(op, o_sc, o_ve, 7)
+    from gftevolver_b200 import Evolver
+    with Evolver(_lp(op.__dict__), form="fp64") as ev:
+        ev.upload(sc, ve, 0)
+        rows = ev.evolve(3) + ev.evolve(4)
+        assert ev.time_iter == 7
+        g_sc, g_ve = ev.download()
+    assert rel_err(g_sc, o_sc) <= 1e-12 and rel_err(g_ve, o_ve) <= 1e-12
+    assert [r["time_iter"] for r in rows] == [r["time_iter"] for r in o_rows]
+
+
+def test_device_initial_data_matches_oracle(oracle_mod):
+    from gftevolver_b200 import Evolver, InitialData
+    op = oracle_mod.Params(model=2, nx=6, ny=7, nz=20)
+    spec = dict(seed=77, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1, wall_width=5.0,
+                wall_value=1.0)
+    for form, dtype, tol in (("fp64", np.float64, 1e-14), ("mixed", np.float32, 2.5e-7)):
+        with Evolver(_lp(op.__dict__), form=form) as ev:
+            ev.init_fields(InitialData(**spec))
+            g_sc, g_ve = ev.download()
+        o_sc, o_ve = oracle_mod.init_fields(op, oracle_mod.ICSpec(**spec), dtype)
+        assert np.max(np.abs(g_sc.astype(np.float64) - o_sc)) <= tol * 4
+        assert np.max(np.abs(g_ve.astype(np.float64) - o_ve)) <= tol
+
+
+def test_domain_warning_is_reported(oracle_mod):
+    """A link RHS outside asin's / sqrt's domain sets GFT_W_* bits (the reference prints "Panic", StandardModel.cpp:474-491)."""
+    op = oracle_mod.Params(nx=4, ny=4, nz=4)
+    ic = oracle_mod.ICSpec(seed=9, mean=[1.0] * 8, sigma=[0.5] * 8, theta_sigma=1.0, eps_sigma=1.0)
+    sc, ve = oracle_mod.init_fields(op, ic, np.float64)
+    sc *= 300.0  # currents g^2 J dt^2 of order 10: |RHS| > 1 at many sites
+    _, _, _, warn = run_gpu(_lp(op.__dict__), "fp64", sc, ve, 1)
+    o_sc, o_ve = sc.copy(), ve.copy()
+    _, owarn = oracle_mod.evolve(op, o_sc, o_ve, 1)
+    assert owarn & 3 != 0
+    assert warn & 3 == owarn & 3
+
+
+def test_observe_does_not_advance(oracle_mod):
+    from gftevolver_b200 import Evolver
+    op = oracle_mod.Params(nx=8, ny=8, nz=8, energy_every=1)
+    ic = oracle_mod.ICSpec(seed=4, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(op, ic, np.float64)
+    with Evolver(_lp(op.__dict__), form="fp64") as ev:
+        ev.upload(sc, ve, 0)
+        o = ev.observe()
+        assert ev.time_iter == 0
+        r = ev.evolve(1)[0]
+        a_sc, a_ve = ev.download()
+    assert abs(o["energy"] - r["energy"]) <= 1e-12 * abs(r["energy"])
+    o_sc, o_ve = sc.copy(), ve.copy()
+    oracle_mod.evolve(op, o_sc, o_ve, 1)
+    assert rel_err(a_sc, o_sc) <= 1e-12

@@ -1,0 +1,94 @@
+"""The CPU oracle against the reference itself (CPU only).
+
+The golden fixtures were produced by the unmodified reference sources
+(tests/golden/make_golden.py); the oracle must reproduce them bit for bit:
+fields after every step and the analysers' float running sums (which also
+pins the reference's site order, boundary regions first).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_files, load_golden
+
+GOLDEN = golden_files()
+
+
+def _params(oracle_mod, meta):
+    return oracle_mod.Params(**meta["params"])
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_reproduces_reference_golden(oracle_mod, path):
+    z, meta = load_golden(path)
+    p = _params(oracle_mod, meta)
+    sc = z["ic_scalars"].copy()
+    ve = z["ic_vectors"].copy()
+    rows, warn = oracle_mod.evolve(p, sc, ve, meta["nt"])
+    assert warn == 0
+    # bit-exact fields (both time levels)
+    np.testing.assert_array_equal(sc, z["scalars"])
+    np.testing.assert_array_equal(ve, z["vectors"])
+    # analyser rows: same steps, bit-exact sums in the reference's precision and order
+    assert [r["time_iter"] for r in rows] == list(z["row_time_iter"])
+    assert [r["has_energy"] for r in rows] == list(z["row_has_energy"])
+    assert [r["has_gauss"] for r in rows] == list(z["row_has_gauss"])
+    for r, e, gi, gm in zip(rows, z["row_ref_energy"], z["row_ref_gauss_int"], z["row_gauss_max"]):
+        if r["has_energy"]:
+            assert r["ref_energy"] == list(e)
+        if r["has_gauss"]:
+            assert r["ref_gauss_int"] == list(gi)
+            assert r["gauss_max"] == list(gm)
+
+
+def test_golden_ic_is_reproducible(oracle_mod):
+    """The oracle's initial-data generator regenerates the stored initial data."""
+    for path in GOLDEN:
+        z, meta = load_golden(path)
+        p = _params(oracle_mod, meta)
+        ic = oracle_mod.ICSpec(**meta["ic"])
+        dtype = np.float64 if meta["storage"] == "f64" else np.float32
+        sc, ve = oracle_mod.init_fields(p, ic, dtype)
+        np.testing.assert_allclose(sc, z["ic_scalars"], rtol=0, atol=4 * np.finfo(dtype).eps)
+        np.testing.assert_allclose(ve, z["ic_vectors"], rtol=0, atol=4 * np.finfo(dtype).eps)
+
+
+def test_oracle_free_field_limit(oracle_mod):
+    """g = g' = 0, lambda = 0 and identity links: the scalar update is the lattice wave equation."""
+    p = oracle_mod.Params(nx=5, ny=4, nz=6, g=0.0, gp=0.0, lam=0.0)
+    ic = oracle_mod.ICSpec(seed=5, mean=[0.3] * 8, sigma=[0.2] * 8)
+    sc, ve = oracle_mod.init_fields(p, ic, np.float64)
+    phi = sc[1].copy()
+    past = sc[0].copy()
+    oracle_mod.evolve(p, sc, ve, 1)
+    lap = -6.0 * phi
+    for ax in range(3):
+        lap += np.roll(phi, 1, axis=ax) + np.roll(phi, -1, axis=ax)
+    expect = 2 * phi - past + p.dt ** 2 * lap
+    np.testing.assert_allclose(sc[0], expect, rtol=0, atol=1e-15)
+
+
+def test_oracle_rejects_bad_config(oracle_mod):
+    p = oracle_mod.Params(model=7, nx=2, ny=2, nz=2)
+    sc = np.zeros((2, 2, 2, 2, p.nsc), np.float32)
+    ve = np.zeros((2, 2, 2, 2, 15), np.float32)
+    with pytest.raises(ValueError):
+        oracle_mod.evolve(p, sc, ve, 1)
+
+
+def test_live_reference_matches_oracle_when_built(oracle_mod):
+    """If oracle/_ref was built here (the reference is mounted), compare live on a fresh random case."""
+    from oracle import refrun
+    if not (refrun.available(False) and refrun.available(True)):
+        pytest.skip("reference binaries not built in this environment")
+    for model in (oracle_mod.MODEL_SM, oracle_mod.MODEL_2HDM):
+        for dtype in (np.float32, np.float64):
+            p = oracle_mod.Params(model=model, nx=3, ny=4, nz=5, energy_every=2, gauss_every=2)
+            ic = oracle_mod.ICSpec(seed=99, mean=[0.8] * 8, sigma=[0.15] * 8, theta_sigma=0.2, eps_sigma=0.2)
+            sc, ve = oracle_mod.init_fields(p, ic, dtype)
+            sc0, ve0 = sc.copy(), ve.copy()
+            oracle_mod.evolve(p, sc, ve, 4)
+            rs, rv, _, _ = refrun.run(p, sc0, ve0, 4, fp64=dtype == np.float64)
+            np.testing.assert_array_equal(sc, rs)
+            np.testing.assert_array_equal(ve, rv)
