@@ -128,24 +128,30 @@ StepParams make_params(const gft_handle* h, int time_iter, bool energy)
     return P;
 }
 
+// Every array of a level starts on a 64-word boundary (256 B for float,
+// 512 B for double) so that the 16-byte vector accesses of q[] and ph[] are
+// aligned for any lattice size.
+size_t padded_sites(int nsite) { return ((size_t)nsite + 63) / 64 * 64; }
+
 template <class S>
 void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
 {
+    const size_t np = padded_sites(nsite);
     S* p = static_cast<S*>(mem);
     for (int d = 0; d < 3; d++) {
         L.q[d] = p;
-        p += 4 * (size_t)nsite;
+        p += 4 * np;
     }
     for (int d = 0; d < 3; d++) {
         L.th[d] = p;
-        p += (size_t)nsite;
+        p += np;
     }
     L.ph[0] = p;
-    p += 4 * (size_t)nsite;
+    p += 4 * np;
     L.ph[1] = (nsc == 8) ? p : nullptr;
 }
 
-size_t level_words(int nsite, int nsc) { return (size_t)nsite * (15 + (size_t)nsc); }
+size_t level_words(int nsite, int nsc) { return padded_sites(nsite) * (15 + (size_t)nsc); }
 
 int step_blocks(const gft_handle* h, const StepParams& P)
 {

@@ -38,6 +38,7 @@ class LatticeParams:
     dt: float = 0.05
     g: float = 0.65
     gp: float = 0.35
+    gpp: float = 0.5           # Higgs-family coupling (TwoHDM gaugeNum 5/7; unused by the built models)
     div_tol: float = 1e-9
     damping: float = 0.0
     nt_damped: int = 0
