@@ -90,6 +90,7 @@ SIGNATURES = {
     "gft_stream": (ctypes.c_void_p, [_H]),
     "gft_device_bytes": (ctypes.c_size_t, [_H]),
     "gft_step_kernel_ms": (ctypes.c_double, [_H, ctypes.POINTER(ctypes.c_int)]),
+    "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gft_last_error": (ctypes.c_char_p, [_H]),
     "gft_version": (ctypes.c_char_p, []),
 }

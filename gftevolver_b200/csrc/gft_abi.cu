@@ -601,6 +601,18 @@ int gft_observe(gft_handle* h, gft_observables* row)
     return GFT_OK;
 }
 
+int gft_selftest_math(int device, double* out)
+{
+    if (!out) return GFT_E_INVALID;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = run_math_selftest(1 << 22, out);
+    if (e != cudaSuccess) {
+        set_global_error(std::string("gft_selftest_math: ") + cudaGetErrorString(e));
+        return GFT_E_CUDA;
+    }
+    return GFT_OK;
+}
+
 double gft_step_kernel_ms(gft_handle* h, int* launches)
 {
     if (launches) *launches = 0;

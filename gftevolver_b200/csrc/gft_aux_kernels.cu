@@ -1,6 +1,9 @@
 // gft_aux_kernels.cu -- layout conversion, initial data and reduction finalisation.
+#include <cstring>
+
 #include "gft_device.cuh"
 #include "gft_launch.h"
+#include "gft_math.cuh"
 
 namespace gft {
 namespace {
@@ -156,7 +159,58 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __r
     }
 }
 
+// Self-test of gft_math.cuh against CUDA's functions: max abs error of
+// sin/cos and max relative error of asin, float and double, over n points.
+__global__ void math_selftest_kernel(int n, unsigned long long* err_bits)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // arguments: a dense sweep of [-40, 40], then small magnitudes down to 1e-8
+    double x;
+    if (i < n / 2) {
+        x = -40.0 + 80.0 * ((double)i + 0.5) / (double)(n / 2);
+    } else {
+        const double t = ((double)(i - n / 2) + 0.5) / (double)(n - n / 2);
+        x = ((i & 1) ? -1.0 : 1.0) * exp(log(1e-8) * (1.0 - t) + log(0.5) * t);
+    }
+    float sf, cf;
+    gsincos((float)x, sf, cf);
+    const double xf = (double)(float)x;
+    const double e0 = fabs((double)sf - sin(xf)), e1 = fabs((double)cf - cos(xf));
+    const double e2 = fabs((double)gsin((float)x) - sin(xf));
+    double sd, cd;
+    gsincos(x, sd, cd);
+    const double e3 = fabs(sd - sin(x)), e4 = fabs(cd - cos(x)), e5 = fabs(gsin(x) - sin(x));
+    double e6 = 0.0, e7 = 0.0;
+    const double ax = fabs(x);
+    if (ax <= 0.999) {
+        e6 = fabs((double)gasin((float)x) - asin(xf)) / fmax(fabs(asin(xf)), 1e-300);
+        e7 = fabs(gasin(x) - asin(x)) / fmax(fabs(asin(x)), 1e-300);
+    }
+    const double e[8] = {e0, e1, e2, e3, e4, e5, e6, e7};
+    for (int k = 0; k < 8; k++) atomicMax(err_bits + k, (unsigned long long)__double_as_longlong(e[k]));
+}
+
 }  // namespace
+
+cudaError_t run_math_selftest(int n, double* out8)
+{
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+    cudaMemset(d, 0, 8 * sizeof(unsigned long long));
+    math_selftest_kernel<<<(n + 255) / 256, 256>>>(n, d);
+    e = cudaGetLastError();
+    unsigned long long h[8] = {0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    for (int k = 0; k < 8; k++) {
+        double v;
+        memcpy(&v, &h[k], sizeof(double));
+        out8[k] = v;
+    }
+    return e;
+}
 
 template <class S, class H>
 cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s)

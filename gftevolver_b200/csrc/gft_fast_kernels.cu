@@ -1,10 +1,14 @@
 // gft_fast_kernels.cu -- throughput forms of the leapfrog step.
 //
 //   GFT_FORM_FP64  : S = double, every operation in FP64.
-//   GFT_FORM_MIXED : S = float storage; forces (staples, sines, covariant
-//                    transports, currents, potential) in FP32; the link
-//                    momentum vec(U_now U_past^dag), the update sums, the
-//                    quaternion renormalisation and all reductions in FP64.
+//   GFT_FORM_MIXED : S = float storage and arithmetic.  Where precision would
+//                    be lost in float the operations are rearranged instead of
+//                    widened: the link momentum is vec((U_now - U_past) U_past^dag)
+//                    (exactly vec(U_now U_past^dag), without the O(1) terms that
+//                    cancel), the leapfrog sums add a small increment to the
+//                    current value in one rounding, and the quaternion
+//                    renormalisation evaluates |U|^2 - 1 with fused multiply-adds.
+//                    Reductions accumulate in FP64 with compensated summation.
 //
 // Same physics as the reference's per-site update (Core/Source/Model.cpp:339-373,
 // WilsonLoops/Source/StandardModel.cpp:324-514, Gradients/Source/StandardModel.cpp:72-100,
@@ -19,20 +23,16 @@
 //     the staples of links i and j.  Intermediate renormalisation is dropped:
 //     it changes products of unit quaternions only at the rounding level.
 //   * the U(1) plaquette angle of plane (i,j) is computed once for both links.
+//   * sin, cos and asin are the range-reduced series of gft_math.cuh.
 // One thread per site (x, y, z); the grid covers (z, y) tiles of 32 x 4 and
 // one x plane per grid row; neighbour reads hit L1/L2.
 #include "gft_device.cuh"
 #include "gft_launch.h"
+#include "gft_math.cuh"
 
 namespace gft {
 namespace {
 
-__device__ __forceinline__ void sc_(float x, float& s, float& c) { sincosf(x, &s, &c); }
-__device__ __forceinline__ void sc_(double x, double& s, double& c) { sincos(x, &s, &c); }
-__device__ __forceinline__ float sin_(float x) { return sinf(x); }
-__device__ __forceinline__ double sin_(double x) { return sin(x); }
-__device__ __forceinline__ float asin_(float x) { return asinf(x); }
-__device__ __forceinline__ double asin_(double x) { return asin(x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 
@@ -62,11 +62,31 @@ __device__ __forceinline__ double one_minus_trace(Q<C> a)
     return v2 / (nrm * (nrm + (double)a.w));
 }
 
+// Neighbour offsets: the site index is linear in (x, y, z), so the wrap of
+// each axis contributes an independent offset.
+struct Offs {
+    int c, m[3], p[3];
+};
+
+__device__ __forceinline__ Offs offsets(const StepParams& P, int x, int y, int z)
+{
+    Offs o;
+    const int plane = P.ny * P.nz;
+    o.c = (x * P.ny + y) * P.nz + z;
+    o.m[0] = (x == 0) ? (P.nx - 1) * plane : -plane;
+    o.p[0] = (x + 1 == P.nx) ? -(P.nx - 1) * plane : plane;
+    o.m[1] = (y == 0) ? (P.ny - 1) * P.nz : -P.nz;
+    o.p[1] = (y + 1 == P.ny) ? -(P.ny - 1) * P.nz : P.nz;
+    o.m[2] = (z == 0) ? P.nz - 1 : -1;
+    o.p[2] = (z + 1 == P.nz) ? -(P.nz - 1) : 1;
+    return o;
+}
+
 template <class S, int MODEL, bool ENERGY>
 __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> past,
                                                         unsigned* status, double* partials)
 {
-    using C = S;  // force arithmetic: FP64 form -> double, mixed form -> float
+    using C = S;  // FP64 form -> double, mixed form -> float
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -78,15 +98,16 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
     unsigned warn = 0;
 
     if (active) {
-        const Nbr n = neighbours(P, x, y, z);
+        const Offs o = offsets(P, x, y, z);
+        const int c = o.c;
         const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
 
         Q<C> U[3];
         C th[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            U[a] = ld4<C>(now.q[a], n.c);
-            th[a] = ld1<C>(now.th[a], n.c);
+            U[a] = ld4<C>(now.q[a], c);
+            th[a] = ld1<C>(now.th[a], c);
         }
 
         // ---- magnetic term: U(1) sines and SU(2) staple sums ----
@@ -102,14 +123,15 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         for (int pl = 0; pl < 3; pl++) {
             const int i = (pl == 2) ? 1 : 0;
             const int j = (pl == 0) ? 1 : 2;
-            const Q<C> Uj_pi = ld4<C>(now.q[j], n.p[i]);
-            const Q<C> Ui_pj = ld4<C>(now.q[i], n.p[j]);
-            const C thj_pi = ld1<C>(now.th[j], n.p[i]);
-            const C thi_pj = ld1<C>(now.th[i], n.p[j]);
+            const int pi = c + o.p[i], pj = c + o.p[j];
+            const Q<C> Uj_pi = ld4<C>(now.q[j], pi);
+            const Q<C> Ui_pj = ld4<C>(now.q[i], pj);
+            const C thj_pi = ld1<C>(now.th[j], pi);
+            const C thi_pj = ld1<C>(now.th[i], pj);
             // F_ij(x) = theta_i(x) + theta_j(x+i) - theta_i(x+j) - theta_j(x); the reference's
             // local angle is -F for link i and +F for link j (StandardModel.cpp:348-353).
             const C F = th[i] + thj_pi - thi_pj - th[j];
-            const C sF = sin_(F);
+            const C sF = gsin(F);
             MgY[i] -= sF * lap[j];
             MgY[j] += sF * lap[i];
             const Q<C> Cij = qmul(qconj(Uj_pi), Ui_pj);
@@ -133,13 +155,13 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 if (j == i) continue;
-                const int mj = n.m[j];
-                const int dg = n.dg[i][j];
+                const int mj = c + o.m[j];
+                const int dg = mj + o.p[i];  // x + i - j
                 const Q<C> Uj_mj = ld4<C>(now.q[j], mj);
                 const Q<C> Ui_mj = ld4<C>(now.q[i], mj);
                 const Q<C> Uj_dg = ld4<C>(now.q[j], dg);
                 const C neigh = -ld1<C>(now.th[j], dg) - ld1<C>(now.th[i], mj) + ld1<C>(now.th[j], mj) + th[i];
-                MgY[i] -= sin_(neigh) * lap[j];
+                MgY[i] -= gsin(neigh) * lap[j];
                 const Q<C> B = qmul(qmul(Uj_mj, qconj(Ui_mj)), qconj(Uj_dg));
                 SB[i] = qadd_scaled(SB[i], lap[j], B);
             }
@@ -158,7 +180,7 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         // ---- scalar sector: covariant Laplacian D and currents J ----
         Q<C> fc[ND];
 #pragma unroll
-        for (int db = 0; db < ND; db++) fc[db] = ld4<C>(now.ph[db], n.c);
+        for (int db = 0; db < ND; db++) fc[db] = ld4<C>(now.ph[db], c);
         Q<C> D[ND];
 #pragma unroll
         for (int db = 0; db < ND; db++) {
@@ -169,18 +191,18 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         double grad_e = 0.0;
 #pragma unroll
         for (int a = 0; a < 3; a++) {
+            const int ma = c + o.m[a], pa = c + o.p[a];
             C sn, cs;
-            sc_(th[a], sn, cs);
+            gsincos(th[a], sn, cs);
             C sm, cm;
-            const C thm = ld1<C>(now.th[a], n.m[a]);
-            sc_(thm, sm, cm);
-            const Q<C> Um = ld4<C>(now.q[a], n.m[a]);
+            gsincos(ld1<C>(now.th[a], ma), sm, cm);
+            const Q<C> Um = ld4<C>(now.q[a], ma);
             const Q<C> Uc = qconj(U[a]);
             C j0 = 0, j1 = 0, j2 = 0, j3 = 0;
 #pragma unroll
             for (int db = 0; db < ND; db++) {
-                const Q<C> fp = ld4<C>(now.ph[db], n.p[a]);
-                const Q<C> fm = ld4<C>(now.ph[db], n.m[a]);
+                const Q<C> fp = ld4<C>(now.ph[db], pa);
+                const Q<C> fm = ld4<C>(now.ph[db], ma);
                 // D: U_a(x-a) phi(x-a) + U_a(x)^dag phi(x+a)
                 const Q<C> tm = transport(Um, cm, sm, fm);
                 const Q<C> tp = transport(Uc, cs, -sn, fp);
@@ -264,21 +286,23 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
             }
         }
 
-        // ---- scalar leapfrog (Model.cpp:347-356), summed in FP64 ----
+        // ---- scalar leapfrog (Model.cpp:347-356):
+        //      phi(t+dt) = phi + [(phi - phi_past)(1 - damping) + dt^2 (D - dV)], one rounding at the end
         double kin_e = 0.0, phisq = 0.0;
         bool finite = true;
+        const C dt2 = (C)P.dt2;
+        const C keep = (C)(1.0 - P.damping_step);
 #pragma unroll
         for (int db = 0; db < ND; db++) {
-            const Q<C> fpast = ld4<C>(past.ph[db], n.c);
+            const Q<C> fpast = ld4<C>(past.ph[db], c);
             const C fn[4] = {fc[db].w, fc[db].x, fc[db].y, fc[db].z};
             const C fo[4] = {fpast.w, fpast.x, fpast.y, fpast.z};
             const C dd[4] = {D[db].w, D[db].x, D[db].y, D[db].z};
-            double out[4];
+            C out[4];
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const C vel = fn[k] - fo[k];
-                const C acc = (C)P.dt2 * (dd[k] - Pot[db][k]);
-                out[k] = (double)fn[k] + ((double)vel + (double)acc - P.damping_step * (double)vel);
+                out[k] = fn[k] + (keep * vel + dt2 * (dd[k] - Pot[db][k]));
                 finite = finite && isfinite(out[k]);
                 if (ENERGY) {
                     const double v = (double)vel / P.dt;
@@ -286,49 +310,58 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
                     phisq += (double)fn[k] * (double)fn[k];
                 }
             }
-            st4(past.ph[db], n.c, (S)out[0], (S)out[1], (S)out[2], (S)out[3]);
+            st4(past.ph[db], c, out[0], out[1], out[2], out[3]);
         }
 
         // ---- link update (WilsonLoops/Source/StandardModel.cpp:456-514) ----
         double elec_e = 0.0;
+        const C gY = (C)P.gsq[0], gI = (C)P.gsq[1];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const Q<double> Un = qcast<double>(U[d]);
-            const Q<double> Up = ld4<double>(past.q[d], n.c);
-            const C thp = ld1<C>(past.th[d], n.c);
-            // link momentum: vec(U_now U_past^dag) and sin(theta_now - theta_past), FP64 products
-            const Q<double> E = qmul(Un, qconj(Up));
+            const Q<C> Un = U[d];
+            const Q<C> Up = ld4<C>(past.q[d], c);
+            const C thp = ld1<C>(past.th[d], c);
+            // link momentum vec(U_now U_past^dag) = vec((U_now - U_past) U_past^dag)
+            const Q<C> dlt = {Un.w - Up.w, Un.x - Up.x, Un.y - Up.y, Un.z - Up.z};
+            C E1, E2, E3;
+            qmul_vec(dlt, qconj(Up), E1, E2, E3);
             const C dth = th[d] - thp;
-            const double elY = (double)sin_(dth);
-            const double gY = P.gsq[0], gI = P.gsq[1];
-            const double keep = 1.0 - P.damping_step;
-            const double R0 = keep * elY + P.dt2 * ((double)MgY[d] + gY * (double)J[d][0]);
-            const double R1 = keep * E.x + P.dt2 * ((double)Mg[d][0] + gI * (double)J[d][1]);
-            const double R2 = keep * E.y + P.dt2 * ((double)Mg[d][1] + gI * (double)J[d][2]);
-            const double R3 = keep * E.z + P.dt2 * ((double)Mg[d][2] + gI * (double)J[d][3]);
+            const C R0 = keep * gsin(dth) + dt2 * (MgY[d] + gY * J[d][0]);
+            const C R1 = keep * E1 + dt2 * (Mg[d][0] + gI * J[d][1]);
+            const C R2 = keep * E2 + dt2 * (Mg[d][1] + gI * J[d][2]);
+            const C R3 = keep * E3 + dt2 * (Mg[d][2] + gI * J[d][3]);
             if (ENERGY) {
-                const double dthd = (double)dth;
-                elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt
-                          * (P.inv_g_sqr * one_minus_trace(E) + P.inv_gp_sqr * 2.0 * sin(0.5 * dthd) * sin(0.5 * dthd));
+                // 1 - (U_now U_past^dag)_0 / |U_now U_past^dag| and 1 - cos(dtheta) = 2 sin^2(dtheta/2)
+                const Q<double> Ed = {(double)Un.w * Up.w + (double)Un.x * Up.x + (double)Un.y * Up.y +
+                                          (double)Un.z * Up.z,
+                                      (double)E1, (double)E2, (double)E3};
+                const double h = sin(0.5 * (double)dth);
+                elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt * (P.inv_g_sqr * one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * h * h);
             }
-            if (R0 * R0 > 1.0) warn |= kWarnAsin;
+            if (R0 * R0 > (C)1) warn |= kWarnAsin;
             // theta(t+dt) = theta(t) + asin(RHS_Y)
-            const double thn = (double)th[d] + (double)asin_((C)R0);
-            // u = (sqrt(1-|c|^2), c); U(t+dt) = normalise(u U(t)).  u - 1 = (-|c|^2/(1+sqrt(1-|c|^2)), c)
-            const double cm = R1 * R1 + R2 * R2 + R3 * R3;
-            if (cm > 1.0) warn |= kWarnSqrt;
-            const C cmC = (C)cm;
-            const C u0m1 = -cmC / ((C)1 + sqrt_((C)1 - cmC));
-            const Q<C> du = {u0m1, (C)R1, (C)R2, (C)R3};
-            const Q<C> dU = qmul(du, U[d]);  // (u - 1) U(t): small, FP32 suffices in the mixed form
-            Q<double> Unew = {Un.w + (double)dU.w, Un.x + (double)dU.x, Un.y + (double)dU.y, Un.z + (double)dU.z};
-            const double n2 = Unew.w * Unew.w + Unew.x * Unew.x + Unew.y * Unew.y + Unew.z * Unew.z;
-            const double sc = rsqrt(n2);
-            Unew = {Unew.w * sc, Unew.x * sc, Unew.y * sc, Unew.z * sc};
+            const C thn = th[d] + gasin(R0);
+            // u = (sqrt(1-|c|^2), c); U(t+dt) = normalise(u U(t)), written as U + correction:
+            //   dU = (u - 1) U with u0 - 1 = -|c|^2 / (1 + sqrt(1 - |c|^2)),
+            //   |U + dU|^2 - 1 = (|U|^2 - 1) + 2 U.dU + |dU|^2 =: e,  1/sqrt(1+e) - 1 = -e/2 + 3e^2/8
+            const C cm = R1 * R1 + R2 * R2 + R3 * R3;
+            if (cm > (C)1) warn |= kWarnSqrt;
+            const C u0m1 = -cm / ((C)1 + sqrt_((C)1 - cm));
+            const Q<C> dU = qmul(Q<C>{u0m1, R1, R2, R3}, Un);
+            C e = fma(Un.w, Un.w, (C)-1);
+            e = fma(Un.x, Un.x, e);
+            e = fma(Un.y, Un.y, e);
+            e = fma(Un.z, Un.z, e);
+            const C udu = Un.w * dU.w + Un.x * dU.x + Un.y * dU.y + Un.z * dU.z;
+            const C dd = dU.w * dU.w + dU.x * dU.x + dU.y * dU.y + dU.z * dU.z;
+            e += (C)2 * udu + dd;
+            const C fm1 = e * ((C)0.375 * e - (C)0.5);
+            const Q<C> Unew = {Un.w + (dU.w + fm1 * (Un.w + dU.w)), Un.x + (dU.x + fm1 * (Un.x + dU.x)),
+                               Un.y + (dU.y + fm1 * (Un.y + dU.y)), Un.z + (dU.z + fm1 * (Un.z + dU.z))};
             finite = finite && isfinite(thn) && isfinite(Unew.w) && isfinite(Unew.x) && isfinite(Unew.y) &&
                      isfinite(Unew.z);
-            past.th[d][n.c] = (S)thn;
-            st4(past.q[d], n.c, (S)Unew.w, (S)Unew.x, (S)Unew.y, (S)Unew.z);
+            past.th[d][c] = thn;
+            st4(past.q[d], c, Unew.w, Unew.x, Unew.y, Unew.z);
         }
         if (!finite) warn |= kWarnNonFinite;
 
@@ -365,17 +398,19 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
     if (z < P.nz && y < P.ny) {
-        const Nbr n = neighbours(P, x, y, z);
+        const Offs o = offsets(P, x, y, z);
+        const int c = o.c;
         double el[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double la = ld1<double>(fut.th[d], n.c) - ld1<double>(now.th[d], n.c);
-            const double na = ld1<double>(fut.th[d], n.m[d]) - ld1<double>(now.th[d], n.m[d]);
+            const int md = c + o.m[d];
+            const double la = ld1<double>(fut.th[d], c) - ld1<double>(now.th[d], c);
+            const double na = ld1<double>(fut.th[d], md) - ld1<double>(now.th[d], md);
             el[0] += (sin(la) - sin(na)) * P.lap[d];
             // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
             double a1, a2, a3, b1, b2, b3;
-            qmul_vec(qconj(ld4<double>(now.q[d], n.c)), ld4<double>(fut.q[d], n.c), a1, a2, a3);
-            qmul_vec(ld4<double>(fut.q[d], n.m[d]), qconj(ld4<double>(now.q[d], n.m[d])), b1, b2, b3);
+            qmul_vec(qconj(ld4<double>(now.q[d], c)), ld4<double>(fut.q[d], c), a1, a2, a3);
+            qmul_vec(ld4<double>(fut.q[d], md), qconj(ld4<double>(now.q[d], md)), b1, b2, b3);
             el[1] += (a1 - b1) * P.lap[d];
             el[2] += (a2 - b2) * P.lap[d];
             el[3] += (a3 - b3) * P.lap[d];
@@ -383,8 +418,8 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
         double gr[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int db = 0; db < ND; db++) {
-            const Q<double> p = ld4<double>(now.ph[db], n.c);
-            const Q<double> q = ld4<double>(fut.ph[db], n.c);
+            const Q<double> p = ld4<double>(now.ph[db], c);
+            const Q<double> q = ld4<double>(fut.ph[db], c);
             gr[0] += 0.25 * (p.w * q.x - p.x * q.w + p.y * q.z - p.z * q.y);
             gr[1] += 0.25 * (p.w * q.z - p.x * q.y + p.y * q.x - p.z * q.w);
             gr[2] += 0.25 * (-p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x);

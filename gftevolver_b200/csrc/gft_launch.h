@@ -47,4 +47,7 @@ cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic,
 cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_host,
                             double* out, cudaStream_t s);
 
+// Elementary-function self-test (gft_math.cuh vs CUDA's functions) on the current device.
+cudaError_t run_math_selftest(int n, double* out8);
+
 }  // namespace gft

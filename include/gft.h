@@ -146,6 +146,13 @@ size_t gft_device_bytes(const gft_handle* h);
  * the last call (CUDA events on the handle's stream); 0 if none. */
 double gft_step_kernel_ms(gft_handle* h, int* launches);
 
+/* Diagnostic with no reference counterpart: evaluates the library's own
+ * sin/cos/asin (range-reduced series used by the throughput forms) against
+ * CUDA's functions on `device`.  out[8] = max abs error of float sincos.sin,
+ * float sincos.cos, float sin, double sincos.sin, double sincos.cos, double sin;
+ * max relative error of float asin, double asin. */
+int gft_selftest_math(int device, double* out);
+
 /* Message for the last error on this handle (or the last global error if h is NULL). */
 const char* gft_last_error(const gft_handle* h);
 
