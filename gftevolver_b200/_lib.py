@@ -19,6 +19,7 @@ GFT_E_UNSUPPORTED = -2
 GFT_E_CUDA = -3
 GFT_E_NOMEM = -4
 GFT_E_STATE = -5
+GFT_E_TIMEOUT = -6
 
 GFT_W_ASIN_DOMAIN = 1
 GFT_W_SQRT_DOMAIN = 2
@@ -91,6 +92,7 @@ SIGNATURES = {
     "gft_device_bytes": (ctypes.c_size_t, [_H]),
     "gft_step_kernel_ms": (ctypes.c_double, [_H, ctypes.POINTER(ctypes.c_int)]),
     "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "gft_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gft_last_error": (ctypes.c_char_p, [_H]),
     "gft_version": (ctypes.c_char_p, []),
 }

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = [
     ("gft_ref_kernels.cu", ["-fmad=false"]),
     ("gft_fast_kernels.cu", []),
+    ("gft_tiled_kernels.cu", []),
     ("gft_aux_kernels.cu", []),
     ("gft_abi.cu", []),
 ]

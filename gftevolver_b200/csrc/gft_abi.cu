@@ -44,6 +44,7 @@ struct gft_handle {
     unsigned* d_status = nullptr;
     double* d_part_e = nullptr;
     double* d_part_g = nullptr;
+    int part_cap = 0;           // blocks the partial buffers hold
     double* d_scale = nullptr;  // kRowSlots scale factors
     double* d_rows = nullptr;
     int rows_cap = 0;
@@ -57,6 +58,12 @@ struct gft_handle {
     int ev_used = 0;
     std::string err;
     size_t dev_bytes = 0;
+    // step kernel selection for the throughput forms
+    int kernel_kind = 0;    // 0 auto, 1 global-memory kernel, 2 tiled (TMA) kernel
+    int tile_variant = 0;   // tiled: index into the built tile shapes
+    int march = 32;         // tiled: planes per CTA along x
+    bool tiled_ready = false;
+    TMaps tm[2];
 
     int fail(int code, const std::string& msg)
     {
@@ -153,19 +160,37 @@ void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
 
 size_t level_words(int nsite, int nsc) { return padded_sites(nsite) * (15 + (size_t)nsc); }
 
-int step_blocks(const gft_handle* h, const StepParams& P)
+bool use_tiled(const gft_handle* h, const StepParams& P)
 {
-    return (h->cfg.form == GFT_FORM_REF) ? ref_launch_blocks(P) : fast_launch_blocks(P, 0);
+    if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1) return false;
+    return tiled_supported(P, h->tile_variant);
 }
 
+int step_blocks(const gft_handle* h, const StepParams& P)
+{
+    if (h->cfg.form == GFT_FORM_REF) return ref_launch_blocks(P);
+    if (use_tiled(h, P)) return tiled_blocks(P, h->tile_variant, h->march);
+    return fast_launch_blocks(P, 0);
+}
+
+// `tn` is the index (0 or 1) of the handle level passed as `now`.
 template <class S>
-cudaError_t launch_step(gft_handle* h, const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past,
+cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelPtrs<S>& now, const LevelPtrs<S>& past,
                         bool energy)
 {
     const int model = h->cfg.model;
     if (h->cfg.form == GFT_FORM_REF) {
         if (model == GFT_MODEL_SM) return launch_ref_step<S, kModelSM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
         return launch_ref_step<S, kModel2HDM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
+    }
+    if constexpr (sizeof(S) == 4) {
+        if (use_tiled(h, P)) {
+            if (model == GFT_MODEL_SM)
+                return launch_tiled_step<S, kModelSM>(h->tm[tn], P, now, past, h->tile_variant, h->march, h->d_status,
+                                                      h->d_part_e, energy, h->stream);
+            return launch_tiled_step<S, kModel2HDM>(h->tm[tn], P, now, past, h->tile_variant, h->march, h->d_status,
+                                                    h->d_part_e, energy, h->stream);
+        }
     }
     if (model == GFT_MODEL_SM)
         return launch_fast_step<S, kModelSM>(P, now, past, h->d_status, h->d_part_e, energy, 0, h->stream);
@@ -283,7 +308,29 @@ int gft_create(const gft_config* cfg, gft_handle** out)
             carve<double>(h->level_mem[t], h->nsite, h->nsc, h->ld[t]);
     }
     const StepParams P = make_params(h, 0, false);
-    const int nb = std::max(step_blocks(h, P), fast_gauss_blocks(P));
+    if (cfg->form == GFT_FORM_MIXED) {
+        bool ok = true;
+        for (int t = 0; t < 2 && ok; t++) {
+            int ty, tz;
+            tiled_tile(0, ty, tz);
+            ok = tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &h->tm[t]);
+        }
+        h->tiled_ready = ok;
+        // default tile: the largest built shape the lattice divides
+        h->tile_variant = 0;
+        while (h->tile_variant < kTiledVariants && !tiled_supported(P, h->tile_variant)) h->tile_variant++;
+        if (h->tile_variant == kTiledVariants) h->tiled_ready = false;
+        else if (h->tile_variant != 0) {
+            for (int t = 0; t < 2 && ok; t++) {
+                int ty, tz;
+                tiled_tile(h->tile_variant, ty, tz);
+                ok = tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &h->tm[t]);
+            }
+            h->tiled_ready = ok;
+        }
+    }
+    int nb = std::max(fast_launch_blocks(P, 0), fast_gauss_blocks(P));
+    nb = std::max(nb, ref_launch_blocks(P));
     const size_t pe = (size_t)nb * kObsCount * sizeof(double), pg = (size_t)nb * kGaussSlots * sizeof(double);
     h->rows_cap = 64;
     if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess ||
@@ -294,6 +341,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
         gft_destroy(h);
         return GFT_E_NOMEM;
     }
+    h->part_cap = nb;
     h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap);
     double scale[kRowSlots];
     const double dv = cfg->dx * cfg->dy * cfg->dz;
@@ -486,7 +534,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         const StepParams P = make_params(h, ti, e);
         const bool prof = h->profile && h->ev_used < kMaxProfiled;
         if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
-        err = launch_step<S>(h, P, lv[tn], lv[tp], e);
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e);
         if (prof) {
             cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
             h->ev_used++;
@@ -515,6 +563,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
     if (err == cudaSuccess) err = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
     if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve");
+    if (status & 8u) return h->fail(GFT_E_TIMEOUT, "gft_evolve: a device wait timed out (tensor-copy barrier)");
     const int nw = rows ? std::min(row, std::max(max_rows, 0)) : 0;
     for (int r = 0; r < nw; r++) fill_row(&rows[r], meta[r].ti, meta[r].e, meta[r].g, host.data() + (size_t)r * kRowSlots);
     if (n_rows) *n_rows = nw;
@@ -583,11 +632,11 @@ int gft_observe(gft_handle* h, gft_observables* row)
         if (is_f64_storage(h)) {
             LevelPtrs<double> tmp;
             carve<double>(h->d_stage, h->nsite, h->nsc, tmp);
-            e = launch_step<double>(h, P, h->ld[tn], tmp, true);
+            e = launch_step<double>(h, P, tn, h->ld[tn], tmp, true);
         } else {
             LevelPtrs<float> tmp;
             carve<float>(h->d_stage, h->nsite, h->nsc, tmp);
-            e = launch_step<float>(h, P, h->lf[tn], tmp, true);
+            e = launch_step<float>(h, P, tn, h->lf[tn], tmp, true);
         }
     }
     // the step wrote into the copy; restore nothing (the levels are untouched)
@@ -598,6 +647,50 @@ int gft_observe(gft_handle* h, gft_observables* row)
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "gft_observe");
     fill_row(row, ti, true, false, host.data());
+    return GFT_OK;
+}
+
+int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
+{
+    if (!h) return GFT_E_INVALID;
+    if (kind < 0 || kind > 2 || march < 1) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad kind or march");
+    if (kind == 1) {
+        h->kernel_kind = 1;
+        return GFT_OK;
+    }
+    if (h->cfg.form != GFT_FORM_MIXED) {
+        if (kind == 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
+        h->kernel_kind = 0;
+        return GFT_OK;
+    }
+    if (tile < 0 || tile >= kTiledVariants) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad tile index");
+    cudaSetDevice(h->cfg.device);
+    const StepParams P = make_params(h, h->time_iter, false);
+    if (!tiled_supported(P, tile))
+        return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the lattice shape does not divide into this tile");
+    int ty, tz;
+    tiled_tile(tile, ty, tz);
+    TMaps tm[2];
+    for (int t = 0; t < 2; t++)
+        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &tm[t]))
+            return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed");
+    const int nb = tiled_blocks(P, tile, march);
+    if (nb > h->part_cap) {
+        cudaStreamSynchronize(h->stream);
+        double* pe = nullptr;
+        if (cudaMalloc(&pe, (size_t)nb * kObsCount * sizeof(double)) != cudaSuccess)
+            return h->fail(GFT_E_NOMEM, "gft_set_kernel: partials allocation failed");
+        cudaFree(h->d_part_e);
+        h->d_part_e = pe;
+        h->dev_bytes += (size_t)(nb - h->part_cap) * kObsCount * sizeof(double);
+        h->part_cap = nb;
+    }
+    h->tm[0] = tm[0];
+    h->tm[1] = tm[1];
+    h->tiled_ready = true;
+    h->tile_variant = tile;
+    h->march = march;
+    h->kernel_kind = kind;
     return GFT_OK;
 }
 

@@ -115,47 +115,81 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
     }
 }
 
-// One block: slot k summed over blocks with Neumaier compensation (k < max_from)
-// or maximised (k >= max_from), in a fixed order (deterministic).
-constexpr int kFinThreads = 256;
+// One block reduces the per-block partials [nblocks][nslots]: each thread
+// accumulates whole rows (coalesced), slot k with Neumaier compensation
+// (k < max_from) or as a maximum (k >= max_from); then thread 0 combines the
+// per-thread results in thread order.  The order is fixed, so the result is
+// deterministic.
+constexpr int kFinThreads = 1024;
+constexpr int kMaxSlots = 16;
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __restrict__ partials, int nblocks,
                                                                int nslots, int max_from, const double* scale,
                                                                double* out)
 {
-    __shared__ double s_sum[kFinThreads];
-    __shared__ double s_cmp[kFinThreads];
-    for (int k = 0; k < nslots; k++) {
-        const bool is_max = k >= max_from;
-        double sum = 0.0, comp = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-            const double v = partials[(size_t)b * nslots + k];
-            if (is_max) {
-                sum = fmax(sum, v);
+    __shared__ double s_sum[kMaxSlots][kFinThreads / 32];
+    __shared__ double s_cmp[kMaxSlots][kFinThreads / 32];
+    double sum[kMaxSlots], comp[kMaxSlots];
+#pragma unroll
+    for (int k = 0; k < kMaxSlots; k++) {
+        sum[k] = 0.0;
+        comp[k] = 0.0;
+    }
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const double* row = partials + (size_t)b * nslots;
+#pragma unroll
+        for (int k = 0; k < kMaxSlots; k++) {
+            if (k >= nslots) break;
+            const double v = row[k];
+            if (k >= max_from) {
+                sum[k] = fmax(sum[k], v);
             } else {
-                const double t = sum + v;
-                comp += (fabs(sum) >= fabs(v)) ? (sum - t) + v : (v - t) + sum;
-                sum = t;
+                const double t = sum[k] + v;
+                comp[k] += (fabs(sum[k]) >= fabs(v)) ? (sum[k] - t) + v : (v - t) + sum[k];
+                sum[k] = t;
             }
         }
-        s_sum[threadIdx.x] = sum;
-        s_cmp[threadIdx.x] = comp;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tsum = 0.0, tcomp = 0.0;
-            for (int t = 0; t < (int)blockDim.x; t++) {
-                if (is_max) {
-                    tsum = fmax(tsum, s_sum[t]);
-                } else {
-                    const double v = s_sum[t];
-                    const double u = tsum + v;
-                    tcomp += (fabs(tsum) >= fabs(v)) ? (tsum - u) + v : (v - u) + tsum;
-                    tsum = u;
-                    tcomp += s_cmp[t];
-                }
+    }
+    // warp level: fold compensation in, then a fixed shuffle tree
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kMaxSlots; k++) {
+        if (k >= nslots) break;
+        double v = (k >= max_from) ? sum[k] : sum[k] + comp[k];
+        double c = 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            // xor partners compute identical sums (addition is commutative)
+            const double w = __shfl_xor_sync(0xffffffffu, v, o);
+            const double cw = __shfl_xor_sync(0xffffffffu, c, o);
+            if (k >= max_from) {
+                v = fmax(v, w);
+            } else {
+                const double t = v + w;
+                c = c + cw + ((fabs(v) >= fabs(w)) ? (v - t) + w : (w - t) + v);
+                v = t;
             }
-            out[k] = (is_max ? tsum : tsum + tcomp) * scale[k];
         }
-        __syncthreads();
+        if (lane == 0) {
+            s_sum[k][warp] = v;
+            s_cmp[k][warp] = c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)nslots) {
+        const int k = threadIdx.x;
+        const bool is_max = k >= max_from;
+        double tsum = 0.0, tcomp = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            const double v = s_sum[k][w];
+            if (is_max) {
+                tsum = fmax(tsum, v);
+            } else {
+                const double u = tsum + v;
+                tcomp += (fabs(tsum) >= fabs(v)) ? (tsum - u) + v : (v - u) + tsum;
+                tsum = u;
+                tcomp += s_cmp[k][w];
+            }
+        }
+        out[k] = (is_max ? tsum : tsum + tcomp) * scale[k];
     }
 }
 

@@ -1,6 +1,7 @@
 // gft_launch.h -- host-side launchers of the device kernels (internal).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "gft_device.cuh"
@@ -26,6 +27,29 @@ cudaError_t launch_fast_gauss(const StepParams& P, const LevelPtrs<S>& now, cons
                               cudaStream_t stream);
 int fast_launch_blocks(const StepParams& P, int variant);
 int fast_gauss_blocks(const StepParams& P);
+
+// Tiled throughput kernel (gft_tiled_kernels.cu): TMA-staged planes, x-march.
+// Tensor maps of the "now" level: quaternions and doublets as {4, nz, ny, nx},
+// hypercharge phases as {nz, ny, nx}.
+struct TMaps {
+    CUtensorMap q[3];
+    CUtensorMap th[3];
+    CUtensorMap ph[2];
+};
+template <class S>
+bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, TMaps* out);
+bool tiled_supported(const StepParams& P, int variant);
+int tiled_blocks(const StepParams& P, int variant, int lx);
+template <class S, int MODEL>
+cudaError_t launch_tiled_step(const TMaps& maps, const StepParams& P, const LevelPtrs<S>& now,
+                              const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
+                              bool energy, cudaStream_t stream);
+constexpr int kTiledVariants = 3;  // 8x32, 4x32, 4x16 (TY x TZ)
+inline void tiled_tile(int variant, int& ty, int& tz)
+{
+    ty = (variant == 0) ? 8 : 4;
+    tz = (variant == 2) ? 16 : 32;
+}
 
 // Auxiliary kernels (gft_aux_kernels.cu).
 template <class S, class H>

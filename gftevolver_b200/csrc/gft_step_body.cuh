@@ -1,0 +1,364 @@
+// gft_step_body.cuh -- the per-site leapfrog update of the throughput forms,
+// written once against a field accessor so that the same arithmetic serves the
+// global-memory kernel (neighbours read through L1/L2) and the tiled kernel
+// (neighbours read from TMA-staged shared-memory planes).
+//
+// Physics: the reference's per-site update (Core/Source/Model.cpp:339-373,
+// WilsonLoops/Source/StandardModel.cpp:324-514, Gradients/Source/StandardModel.cpp:72-100,
+// 272-363, Potentials/Source/SO_N.cpp:57-75, Potentials/Source/Double_SO_N.cpp:244-341),
+// reassociated:
+//   * the reference builds, for every link i and plane j, the loops
+//       P1 = U_j(x+i)^dag U_i(x+j) U_j(x) U_i(x)^dag,
+//       P2 = U_i(x) U_j(x-j) U_i(x-j)^dag U_j(x+i-j)^dag,
+//     renormalising intermediate products.  Here the staples are summed first,
+//       SA_i = sum_j w_j U_j(x+i)^dag U_i(x+j) U_j(x),   SB_i = sum_j w_j U_j(x-j) U_i(x-j)^dag U_j(x+i-j)^dag,
+//     and vec(P1) - vec(P2) summed over j becomes vec(SA_i U_i^dag) - vec(U_i SB_i)
+//     (the vector part is linear).  C_ij = U_j(x+i)^dag U_i(x+j) is shared by
+//     the staples of links i and j.  Intermediate renormalisation is dropped:
+//     it changes products of unit quaternions only at the rounding level.
+//   * the U(1) plaquette angle of plane (i,j) is computed once for both links.
+//   * sin, cos and asin are the range-reduced series of gft_math.cuh.
+// Precision of the mixed form (C = float): operations that would lose
+// precision in float are rearranged rather than widened -- the link momentum
+// is vec((U_now - U_past) U_past^dag) (exactly vec(U_now U_past^dag) without
+// the O(1) terms that cancel), leapfrog sums add a small increment to the
+// current value with one rounding, and the renormalisation evaluates
+// |U|^2 - 1 with fused multiply-adds.  Energies accumulate in FP64.
+#pragma once
+
+#include "gft_device.cuh"
+#include "gft_math.cuh"
+
+namespace gft {
+
+__device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+
+// Doublet phi rotated by the hypercharge phase (cos, sin) then acted on by the
+// SU(2) quaternion u as the real 4x4 of Gradients/Source/StandardModel.cpp:94-97.
+template <class C>
+__device__ __forceinline__ Q<C> transport(Q<C> u, C cs, C sn, Q<C> f)
+{
+    const C h0 = cs * f.w - sn * f.x;
+    const C h1 = cs * f.x + sn * f.w;
+    const C h2 = cs * f.y - sn * f.z;
+    const C h3 = cs * f.z + sn * f.y;
+    Q<C> t;
+    t.w = u.w * h0 - u.z * h1 + u.y * h2 - u.x * h3;
+    t.x = u.z * h0 + u.w * h1 + u.x * h2 + u.y * h3;
+    t.y = -u.y * h0 - u.x * h1 + u.w * h2 + u.z * h3;
+    t.z = u.x * h0 - u.y * h1 - u.z * h2 + u.w * h3;
+    return t;
+}
+
+// 1 - a0/|a| computed without cancellation: |vec a|^2 / (|a| (|a| + a0)).
+template <class C>
+__device__ __forceinline__ double one_minus_trace(Q<C> a)
+{
+    const double v2 = (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z;
+    const double nrm = sqrt((double)a.w * a.w + v2);
+    return v2 / (nrm * (nrm + (double)a.w));
+}
+
+// Neighbour references of one site, in the accessor's own reference type:
+//   c = x, m[a] = x - e_a, p[a] = x + e_a, dg(i, j) = x + e_i - e_j (i != j).
+template <class R>
+struct Stencil {
+    R c, m[3], p[3];
+    R d01, d02, d10, d12, d20, d21;
+    __device__ __forceinline__ R dg(int i, int j) const
+    {
+        return (i == 0) ? (j == 1 ? d01 : d02) : (i == 1) ? (j == 0 ? d10 : d12) : (j == 0 ? d20 : d21);
+    }
+};
+
+// Own-site access to the past level (read, then overwritten with t + dt).
+template <class S>
+struct PastSite {
+    LevelPtrs<S> L;
+    int s;
+};
+
+// The per-site update.  A provides q(d, R) -> Q<C>, th(d, R) -> C, ph(k, R) -> Q<C>
+// for the "now" level.  obs receives the energy-step observables.
+template <class S, int MODEL, bool ENERGY, class A, class R>
+__device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S> ps,
+                                          double (&obs)[kObsCount], unsigned& warn)
+{
+    using C = S;  // FP64 form -> double, mixed form -> float
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
+
+    Q<C> U[3];
+    C th[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        U[a] = acc.q(a, n.c);
+        th[a] = acc.th(a, n.c);
+    }
+
+    // ---- magnetic term: U(1) sines and SU(2) staple sums ----
+    C MgY[3] = {(C)0, (C)0, (C)0};
+    Q<C> SA[3], SB[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        SA[a] = {(C)0, (C)0, (C)0, (C)0};
+        SB[a] = {(C)0, (C)0, (C)0, (C)0};
+    }
+    double mag_e = 0.0, plaq2 = 0.0, plaq1 = 0.0;
+#pragma unroll
+    for (int pl = 0; pl < 3; pl++) {
+        const int i = (pl == 2) ? 1 : 0;
+        const int j = (pl == 0) ? 1 : 2;
+        const Q<C> Uj_pi = acc.q(j, n.p[i]);
+        const Q<C> Ui_pj = acc.q(i, n.p[j]);
+        // F_ij(x) = theta_i(x) + theta_j(x+i) - theta_i(x+j) - theta_j(x); the reference's
+        // local angle is -F for link i and +F for link j (StandardModel.cpp:348-353).
+        const C F = th[i] + acc.th(j, n.p[i]) - acc.th(i, n.p[j]) - th[j];
+        const C sF = gsin(F);
+        MgY[i] -= sF * lap[j];
+        MgY[j] += sF * lap[i];
+        const Q<C> Cij = qmul(qconj(Uj_pi), Ui_pj);
+        const Q<C> Aij = qmul(Cij, U[j]);
+        const Q<C> Aji = qmul(qconj(Cij), U[i]);
+        SA[i] = qadd_scaled(SA[i], lap[j], Aij);
+        SA[j] = qadd_scaled(SA[j], lap[i], Aji);
+        if (ENERGY) {
+            // plaquette P1 = Aij U_i^dag: both orientations have the same trace
+            const Q<C> P1 = qmul(Aij, qconj(U[i]));
+            const double omt = one_minus_trace(P1);
+            const double wF = (double)F;
+            const double omc = 2.0 * sin(0.5 * wF) * sin(0.5 * wF);
+            mag_e += 4.0 * P.lap[i] * P.lap[j] * (P.inv_g_sqr * omt + P.inv_gp_sqr * omc);
+            plaq2 += 1.0 - omt;
+            plaq1 += cos(wF);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            if (j == i) continue;
+            const R mj = n.m[j];
+            const R dg = n.dg(i, j);
+            const Q<C> Uj_mj = acc.q(j, mj);
+            const Q<C> Ui_mj = acc.q(i, mj);
+            const Q<C> Uj_dg = acc.q(j, dg);
+            const C neigh = -acc.th(j, dg) - acc.th(i, mj) + acc.th(j, mj) + th[i];
+            MgY[i] -= gsin(neigh) * lap[j];
+            const Q<C> B = qmul(qmul(Uj_mj, qconj(Ui_mj)), qconj(Uj_dg));
+            SB[i] = qadd_scaled(SB[i], lap[j], B);
+        }
+    }
+    C Mg[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        C a1, a2, a3, b1, b2, b3;
+        qmul_vec(SA[i], qconj(U[i]), a1, a2, a3);
+        qmul_vec(U[i], SB[i], b1, b2, b3);
+        Mg[i][0] = a1 - b1;
+        Mg[i][1] = a2 - b2;
+        Mg[i][2] = a3 - b3;
+    }
+
+    // ---- scalar sector: covariant Laplacian D and currents J ----
+    Q<C> fc[ND];
+#pragma unroll
+    for (int db = 0; db < ND; db++) fc[db] = acc.ph(db, n.c);
+    Q<C> D[ND];
+#pragma unroll
+    for (int db = 0; db < ND; db++) {
+        const C w = (C)(-2.0 * (P.lap[0] + P.lap[1] + P.lap[2]));
+        D[db] = {w * fc[db].w, w * fc[db].x, w * fc[db].y, w * fc[db].z};
+    }
+    C J[3][4];
+    double grad_e = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        C sn, cs;
+        gsincos(th[a], sn, cs);
+        C sm, cm;
+        gsincos(acc.th(a, n.m[a]), sm, cm);
+        const Q<C> Um = acc.q(a, n.m[a]);
+        const Q<C> Uc = qconj(U[a]);
+        C j0 = 0, j1 = 0, j2 = 0, j3 = 0;
+#pragma unroll
+        for (int db = 0; db < ND; db++) {
+            const Q<C> fp = acc.ph(db, n.p[a]);
+            const Q<C> fm = acc.ph(db, n.m[a]);
+            // D: U_a(x-a) phi(x-a) + U_a(x)^dag phi(x+a)
+            const Q<C> tm = transport(Um, cm, sm, fm);
+            const Q<C> tp = transport(Uc, cs, -sn, fp);
+            D[db] = qadd_scaled(D[db], lap[a], tm);
+            D[db] = qadd_scaled(D[db], lap[a], tp);
+            // J: Im of (U_a(x) phi(x))^dag sigma phi(x+a)
+            const Q<C> t = transport(U[a], cs, sn, fc[db]);
+            j0 += t.w * fp.x - t.x * fp.w + t.y * fp.z - t.z * fp.y;
+            j1 += t.w * fp.z - t.x * fp.y + t.y * fp.x - t.z * fp.w;
+            j2 += -t.w * fp.y - t.x * fp.z + t.y * fp.w + t.z * fp.x;
+            j3 += t.w * fp.x - t.x * fp.w - t.y * fp.z + t.z * fp.y;
+            if (ENERGY) {
+                const double e0 = (double)fp.w - t.w, e1 = (double)fp.x - t.x;
+                const double e2 = (double)fp.y - t.y, e3 = (double)fp.z - t.z;
+                grad_e += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+            }
+        }
+        J[a][0] = (C)0.25 * j0;
+        J[a][1] = (C)0.25 * j1;
+        J[a][2] = (C)0.25 * j2;
+        J[a][3] = (C)0.25 * j3;
+    }
+
+    // ---- potential dV/dphi ----
+    C Pot[ND][4];
+    double pot_e = 0.0;
+    if (MODEL == kModelSM) {
+        const C fsq = fc[0].w * fc[0].w + fc[0].x * fc[0].x + fc[0].y * fc[0].y + fc[0].z * fc[0].z;
+        const C k = (C)P.lambda * (fsq - (C)P.eta_sqr);
+        Pot[0][0] = k * fc[0].w;
+        Pot[0][1] = k * fc[0].x;
+        Pot[0][2] = k * fc[0].y;
+        Pot[0][3] = k * fc[0].z;
+        if (ENERGY) {
+            const double t = (double)fsq - P.eta_sqr;
+            pot_e = 0.25 * P.lambda * t * t;
+        }
+    } else {
+        const Q<C> f1 = fc[0], f2 = fc[ND - 1];
+        const C s1 = f1.w * f1.w + f1.x * f1.x + f1.y * f1.y + f1.z * f1.z;
+        const C s2 = f2.w * f2.w + f2.x * f2.x + f2.y * f2.y + f2.z * f2.z;
+        const C dot = P.break_son ? f1.w * f2.w + f1.x * f2.x + f1.y * f2.y + f1.z * f2.z : (C)0;
+        const C anti = (P.break_son && P.break_uhalfn) ? f1.w * f2.x - f1.x * f2.w + f1.y * f2.z - f1.z * f2.y : (C)0;
+        const C a1 = (C)(-2.0 * P.m1) + (C)(4.0 * P.l1) * s1 + (C)(2.0 * P.l3) * s2;
+        const C a2 = (C)(-2.0 * P.m2) + (C)(4.0 * P.l2) * s2 + (C)(2.0 * P.l3) * s1;
+        // single SO(N): (-m12r + 2 l4p5 dot + l6r s1 + l7r s2) f_other + 2 l6r|l7r dot f_self
+        const C bs = (C)(-P.m12r) + (C)(2.0 * P.l4p5) * dot + (C)P.l6r * s1 + (C)P.l7r * s2;
+        const C b1 = (C)(2.0 * P.l6r) * dot, b2 = (C)(2.0 * P.l7r) * dot;
+        // U(N/2): (m12i + 2 l4m5 anti - 2 l5i dot - l6i s1 - l7i s2) J f_other - 2 l5i anti f_other - 2 l6i|l7i anti f_self
+        const C cu = (C)P.m12i + (C)(2.0 * P.l4m5) * anti - (C)(2.0 * P.l5i) * dot - (C)P.l6i * s1 - (C)P.l7i * s2;
+        const C c5 = (C)(2.0 * P.l5i) * anti;
+        const C c1 = (C)(2.0 * P.l6i) * anti, c2 = (C)(2.0 * P.l7i) * anti;
+        const C f1v[4] = {f1.w, f1.x, f1.y, f1.z};
+        const C f2v[4] = {f2.w, f2.x, f2.y, f2.z};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int alt = 1 - 2 * (k % 2);
+            C v1 = a1 * f1v[k];
+            C v2 = a2 * f2v[k];
+            if (P.break_son) {
+                v1 += bs * f2v[k] + b1 * f1v[k];
+                v2 += bs * f1v[k] + b2 * f2v[k];
+                if (P.break_uhalfn) {
+                    v1 += cu * (C)alt * f2v[k + alt] - c5 * f2v[k] - c1 * f1v[k];
+                    v2 += -cu * (C)alt * f1v[k + alt] - c5 * f1v[k] - c2 * f2v[k];
+                }
+            }
+            Pot[0][k] = v1;
+            Pot[ND - 1][k] = v2;
+        }
+        if (ENERGY) {
+            const double d1 = s1, d2 = s2, dd = dot, da = anti;
+            double v = -P.m1 * d1 - P.m2 * d2 + P.l1 * d1 * d1 + P.l2 * d2 * d2 + P.l3 * d1 * d2;
+            if (P.break_son) {
+                v += -P.m12r * dd + P.l4p5 * dd * dd + P.l6r * d1 * dd + P.l7r * d2 * dd;
+                if (P.break_uhalfn)
+                    v += P.m12i * da + P.l4m5 * da * da - 2.0 * P.l5i * dd * da - P.l6i * d1 * da - P.l7i * d2 * da;
+            }
+            if (P.apply_norm) v += P.energy_offset;
+            pot_e = v;
+        }
+    }
+
+    // ---- scalar leapfrog (Model.cpp:347-356):
+    //      phi(t+dt) = phi + [(phi - phi_past)(1 - damping) + dt^2 (D - dV)], one rounding at the end
+    double kin_e = 0.0, phisq = 0.0;
+    bool finite = true;
+    const C dt2 = (C)P.dt2;
+    const C keep = (C)(1.0 - P.damping_step);
+#pragma unroll
+    for (int db = 0; db < ND; db++) {
+        const Q<C> fpast = ld4<C>(ps.L.ph[db], ps.s);
+        const C fn[4] = {fc[db].w, fc[db].x, fc[db].y, fc[db].z};
+        const C fo[4] = {fpast.w, fpast.x, fpast.y, fpast.z};
+        const C dd[4] = {D[db].w, D[db].x, D[db].y, D[db].z};
+        C out[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const C vel = fn[k] - fo[k];
+            out[k] = fn[k] + (keep * vel + dt2 * (dd[k] - Pot[db][k]));
+            finite = finite && isfinite(out[k]);
+            if (ENERGY) {
+                const double v = (double)vel / P.dt;
+                kin_e += 0.5 * v * v;
+                phisq += (double)fn[k] * (double)fn[k];
+            }
+        }
+        st4(ps.L.ph[db], ps.s, out[0], out[1], out[2], out[3]);
+    }
+
+    // ---- link update (WilsonLoops/Source/StandardModel.cpp:456-514) ----
+    double elec_e = 0.0;
+    const C gY = (C)P.gsq[0], gI = (C)P.gsq[1];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const Q<C> Un = U[d];
+        const Q<C> Up = ld4<C>(ps.L.q[d], ps.s);
+        const C thp = ld1<C>(ps.L.th[d], ps.s);
+        // link momentum vec(U_now U_past^dag) = vec((U_now - U_past) U_past^dag)
+        const Q<C> dlt = {Un.w - Up.w, Un.x - Up.x, Un.y - Up.y, Un.z - Up.z};
+        C E1, E2, E3;
+        qmul_vec(dlt, qconj(Up), E1, E2, E3);
+        const C dth = th[d] - thp;
+        const C R0 = keep * gsin(dth) + dt2 * (MgY[d] + gY * J[d][0]);
+        const C R1 = keep * E1 + dt2 * (Mg[d][0] + gI * J[d][1]);
+        const C R2 = keep * E2 + dt2 * (Mg[d][1] + gI * J[d][2]);
+        const C R3 = keep * E3 + dt2 * (Mg[d][2] + gI * J[d][3]);
+        if (ENERGY) {
+            // 1 - (U_now U_past^dag)_0 / |U_now U_past^dag| and 1 - cos(dtheta) = 2 sin^2(dtheta/2)
+            const Q<double> Ed = {(double)Un.w * Up.w + (double)Un.x * Up.x + (double)Un.y * Up.y +
+                                      (double)Un.z * Up.z,
+                                  (double)E1, (double)E2, (double)E3};
+            const double h = sin(0.5 * (double)dth);
+            elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt * (P.inv_g_sqr * one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * h * h);
+        }
+        if (R0 * R0 > (C)1) warn |= kWarnAsin;
+        // theta(t+dt) = theta(t) + asin(RHS_Y)
+        const C thn = th[d] + gasin(R0);
+        // u = (sqrt(1-|c|^2), c); U(t+dt) = normalise(u U(t)), written as U + correction:
+        //   dU = (u - 1) U with u0 - 1 = -|c|^2 / (1 + sqrt(1 - |c|^2)),
+        //   |U + dU|^2 - 1 = (|U|^2 - 1) + 2 U.dU + |dU|^2 =: e,  1/sqrt(1+e) - 1 = -e/2 + 3e^2/8
+        const C cm = R1 * R1 + R2 * R2 + R3 * R3;
+        if (cm > (C)1) warn |= kWarnSqrt;
+        const C u0m1 = -cm / ((C)1 + sqrt_((C)1 - cm));
+        const Q<C> dU = qmul(Q<C>{u0m1, R1, R2, R3}, Un);
+        C e = fma(Un.w, Un.w, (C)-1);
+        e = fma(Un.x, Un.x, e);
+        e = fma(Un.y, Un.y, e);
+        e = fma(Un.z, Un.z, e);
+        const C udu = Un.w * dU.w + Un.x * dU.x + Un.y * dU.y + Un.z * dU.z;
+        const C dd = dU.w * dU.w + dU.x * dU.x + dU.y * dU.y + dU.z * dU.z;
+        e += (C)2 * udu + dd;
+        const C fm1 = e * ((C)0.375 * e - (C)0.5);
+        const Q<C> Unew = {Un.w + (dU.w + fm1 * (Un.w + dU.w)), Un.x + (dU.x + fm1 * (Un.x + dU.x)),
+                           Un.y + (dU.y + fm1 * (Un.y + dU.y)), Un.z + (dU.z + fm1 * (Un.z + dU.z))};
+        finite = finite && isfinite(thn) && isfinite(Unew.w) && isfinite(Unew.x) && isfinite(Unew.y) &&
+                 isfinite(Unew.z);
+        ps.L.th[d][ps.s] = thn;
+        st4(ps.L.q[d], ps.s, Unew.w, Unew.x, Unew.y, Unew.z);
+    }
+    if (!finite) warn |= kWarnNonFinite;
+
+    if (ENERGY) {
+        obs[kObsPotential] += pot_e;
+        obs[kObsGradient] += grad_e;
+        obs[kObsKinetic] += kin_e;
+        obs[kObsMagnetic] += mag_e;
+        obs[kObsElectric] += elec_e;
+        obs[kObsEnergy] += pot_e + grad_e + kin_e + mag_e + elec_e;
+        obs[kObsPlaqSU2] += plaq2;
+        obs[kObsPlaqU1] += plaq1;
+        obs[kObsPhiSq] += phisq;
+    }
+}
+
+}  // namespace gft

@@ -215,6 +215,10 @@ class Evolver:
             self.lib.gft_evolve(self.h, int(n_steps), rows, int(max_rows), ctypes.byref(n)), self.h)
         return [_row_dict(rows[i]) for i in range(n.value)]
 
+    def set_kernel(self, kind: int = 0, tile: int = 0, march: int = 32) -> None:
+        """Step kernel of the throughput forms: 0 auto, 1 one thread per site, 2 TMA-staged tiles."""
+        _lib.check(self.lib.gft_set_kernel(self.h, int(kind), int(tile), int(march)), self.h)
+
     def observe(self) -> dict:
         r = _lib.GftObservables()
         _lib.check(self.lib.gft_observe(self.h, ctypes.byref(r)), self.h)

@@ -43,6 +43,7 @@ extern "C" {
 #define GFT_E_CUDA (-3)         /* CUDA runtime error; see gft_last_error */
 #define GFT_E_NOMEM (-4)        /* device allocation failed */
 #define GFT_E_STATE (-5)        /* call out of order (e.g. evolve before upload) */
+#define GFT_E_TIMEOUT (-6)      /* a bounded device-side wait gave up; the step's results are invalid */
 
 #define GFT_W_ASIN_DOMAIN 1     /* |RHS_Y| > 1 somewhere (theta update used asin outside [-1,1]) */
 #define GFT_W_SQRT_DOMAIN 2     /* |c|^2 > 1 somewhere (SU(2) update used sqrt of a negative number) */
@@ -145,6 +146,15 @@ size_t gft_device_bytes(const gft_handle* h);
 /* Average duration in milliseconds of the step kernel over the launches since
  * the last call (CUDA events on the handle's stream); 0 if none. */
 double gft_step_kernel_ms(gft_handle* h, int* launches);
+
+/* Step-kernel selection for the throughput forms (no reference counterpart):
+ * kind 0 = automatic (the tiled kernel for the mixed form when the lattice
+ * divides into a built tile, else the one-thread-per-site kernel), 1 = one
+ * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
+ * marching along x (mixed form).  tile = tile shape (0: 8 x 32, 1: 4 x 32,
+ * 2: 4 x 16 sites in y x z); march = planes per CTA along x.  Returns
+ * GFT_E_UNSUPPORTED when the lattice does not divide into the tile. */
+int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
 /* Diagnostic with no reference counterpart: evaluates the library's own
  * sin/cos/asin (range-reduced series used by the throughput forms) against

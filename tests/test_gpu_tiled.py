@@ -1,0 +1,77 @@
+"""The TMA-staged tiled step kernel (mixed form) against the one-thread-per-site
+kernel and the oracle (GPU).
+
+Both kernels evaluate the same per-site arithmetic (gft_step_body.cuh); only
+where the neighbours come from differs (shared-memory planes vs L1/L2), so the
+fields must agree to a few float ulps (the compiler may contract differently)
+and the observables to 1e-12 relative.  Cases cover every tile shape, march
+lengths that do not divide nx, lattices where every tile touches the periodic
+boundary, and the 2HDM model.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(oracle_mod, model, shape, seed=31):
+    from gftevolver_b200 import LatticeParams
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=3, gauss_every=3)
+    ic = oracle_mod.ICSpec(seed=seed, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
+                           eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(op, ic, np.float32)
+    return op, LatticeParams(**op.__dict__), sc, ve
+
+
+def _run(p, sc, ve, nt, kind, tile=0, march=32):
+    from gftevolver_b200 import Evolver
+    with Evolver(p, form="mixed") as ev:
+        ev.set_kernel(kind, tile, march)
+        ev.upload(sc, ve, 0)
+        rows = ev.evolve(nt)
+        out = ev.download()
+    return out[0], out[1], rows
+
+
+def _close(a, b, nulp=4):
+    tol = nulp * np.spacing(np.maximum(np.abs(a), np.abs(b)).astype(np.float32)).astype(np.float64)
+    return np.all(np.abs(a.astype(np.float64) - b.astype(np.float64)) <= tol + 1e-30)
+
+
+@pytest.mark.parametrize("model", [1, 2], ids=["sm", "2hdm"])
+@pytest.mark.parametrize("shape,tile,march", [
+    ((8, 8, 32), 0, 32),      # one tile per plane: every halo wraps
+    ((12, 16, 64), 0, 5),     # march does not divide nx
+    ((7, 8, 32), 1, 3),
+    ((9, 12, 48), 2, 4),      # 4 x 16 tiles
+    ((3, 4, 16), 2, 1),       # march 1
+    ((20, 16, 32), 1, 64),    # march > nx
+])
+def test_tiled_matches_global_kernel(oracle_mod, model, shape, tile, march):
+    op, p, sc, ve = _setup(oracle_mod, model, shape)
+    g_sc, g_ve, g_rows = _run(p, sc, ve, 7, kind=1)
+    t_sc, t_ve, t_rows = _run(p, sc, ve, 7, kind=2, tile=tile, march=march)
+    assert _close(t_sc, g_sc) and _close(t_ve, g_ve)
+    assert len(t_rows) == len(g_rows)
+    for a, b in zip(t_rows, g_rows):
+        assert a["time_iter"] == b["time_iter"]
+        for k in ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "plaq_su2", "plaq_u1"):
+            assert abs(a[k] - b[k]) <= 1e-9 * max(1.0, abs(b[k])), k
+    # and against the FP64 oracle within the mixed-form bound
+    o_sc, o_ve = oracle_mod.init_fields(op, oracle_mod.ICSpec(seed=31, mean=[1.0 if model == 1 else 0.7] * 8,
+                                                              sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1),
+                                        np.float64)
+    oracle_mod.evolve(op, o_sc, o_ve, 7)
+    assert np.max(np.abs(t_sc.astype(np.float64) - o_sc)) <= 6e-6
+    assert np.max(np.abs(t_ve.astype(np.float64) - o_ve)) <= 6e-6
+
+
+def test_tiled_rejects_indivisible_lattice(oracle_mod):
+    from gftevolver_b200 import Evolver, GftError
+    _, p, sc, ve = _setup(oracle_mod, 1, (4, 6, 20))
+    with Evolver(p, form="mixed") as ev:
+        with pytest.raises(GftError):
+            ev.set_kernel(2, 0, 8)
+        ev.upload(sc, ve, 0)
+        ev.evolve(2)  # automatic choice falls back to the one-thread-per-site kernel
