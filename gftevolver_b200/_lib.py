@@ -24,6 +24,7 @@ GFT_E_TIMEOUT = -6
 GFT_W_ASIN_DOMAIN = 1
 GFT_W_SQRT_DOMAIN = 2
 GFT_W_NONFINITE = 4
+GFT_W_RANGE = 16
 
 GFT_MODEL_SM = 1
 GFT_MODEL_2HDM = 2

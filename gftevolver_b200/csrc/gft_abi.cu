@@ -567,7 +567,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
     const int nw = rows ? std::min(row, std::max(max_rows, 0)) : 0;
     for (int r = 0; r < nw; r++) fill_row(&rows[r], meta[r].ti, meta[r].e, meta[r].g, host.data() + (size_t)r * kRowSlots);
     if (n_rows) *n_rows = nw;
-    return (int)(status & (GFT_W_ASIN_DOMAIN | GFT_W_SQRT_DOMAIN | GFT_W_NONFINITE));
+    return (int)(status & (GFT_W_ASIN_DOMAIN | GFT_W_SQRT_DOMAIN | GFT_W_NONFINITE | GFT_W_RANGE));
 }
 
 }  // namespace

@@ -236,5 +236,6 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out,
 constexpr unsigned kWarnAsin = 1u;
 constexpr unsigned kWarnSqrt = 2u;
 constexpr unsigned kWarnNonFinite = 4u;
+constexpr unsigned kWarnRange = 16u;  // a link phase beyond the elementary functions' reduction range
 
 }  // namespace gft

@@ -67,7 +67,9 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         n.d12 = o.c + o.p[1] + o.m[2];
         n.d20 = o.c + o.p[2] + o.m[0];
         n.d21 = o.c + o.p[2] + o.m[1];
-        site_step<S, MODEL, ENERGY>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, obs, warn);
+        XCarry<S, (MODEL == kModelSM) ? 1 : 2> carry;
+        carry.valid = false;
+        site_step<S, MODEL, ENERGY>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn);
     }
     if (ENERGY) {
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);

@@ -7,8 +7,9 @@
 // truncated where the first omitted term is below the format's rounding:
 //   float : sin to r^13, cos to r^14  (omitted term <= 7e-10 at |r| = pi/2)
 //   double: sin to r^23, cos to r^24  (omitted term <= 1e-19)
-// Arguments beyond |x| > 2^13 (float) / 2^20 (double) fall back to the CUDA
-// library functions, whose reduction is exact for any argument.
+// The reduction uses the 1.5*2^p rounding constant (no conversion to integer):
+// it holds for |x| < 1.3e7 (float) / 1.4e15 (double); phases that large do not
+// occur in the evolution (the step kernels flag |theta| > 1e4).
 // asin: odd series x + x^3/6 + 3x^5/40 + ... for |x| <= 1/4 (float) or 1/8
 // (double) -- the link update's argument is dt * E ~ 1e-3 -- and CUDA's asin
 // otherwise.
@@ -75,37 +76,34 @@ __device__ __forceinline__ float sin_poly(float r)
     return fmaf(ps * r2, r, r);
 }
 
-// pi = PI_A + PI_B: PI_A = float(pi), PI_B = float(pi - PI_A)
-__device__ __forceinline__ float reduce_pi(float x, int& k)
+// x = k*pi + r: t = x/pi + 1.5*2^23 rounds x/pi to the integer k held in the
+// low mantissa bits of t (valid while |x/pi| < 2^22, i.e. |x| < 1.3e7; the
+// step kernels flag phases beyond 1e4 with GFT_W_RANGE); then
+// r = x - k*PI_A - k*PI_B with PI_A = float(pi), PI_B = float(pi - PI_A).
+// Returns r and the sign bit (-1)^k as an integer mask.
+__device__ __forceinline__ float reduce_pi(float x, unsigned& sign)
 {
-    const float kf = rintf(x * 0.3183098861837907f);
-    k = (int)kf;
+    const float t = fmaf(x, 0.3183098861837907f, 12582912.0f);
+    const float kf = t - 12582912.0f;
+    sign = __float_as_uint(t) << 31;
     const float r = fmaf(-kf, 3.1415927410125732f, x);
     return fmaf(-kf, -8.742277657347586e-08f, r);
 }
 
 __device__ __forceinline__ float gsin(float x)
 {
-    if (fabsf(x) > 8192.0f) return sinf(x);
-    int k;
-    const float r = reduce_pi(x, k);
-    const float s = sin_poly(r);
-    return (k & 1) ? -s : s;
+    unsigned sg;
+    const float r = reduce_pi(x, sg);
+    return __uint_as_float(__float_as_uint(sin_poly(r)) ^ sg);
 }
 
 __device__ __forceinline__ void gsincos(float x, float& s, float& c)
 {
-    if (fabsf(x) > 8192.0f) {
-        sincosf(x, &s, &c);
-        return;
-    }
-    int k;
-    const float r = reduce_pi(x, k);
+    unsigned sg;
+    const float r = reduce_pi(x, sg);
     sincos_poly(r, s, c);
-    if (k & 1) {
-        s = -s;
-        c = -c;
-    }
+    s = __uint_as_float(__float_as_uint(s) ^ sg);
+    c = __uint_as_float(__float_as_uint(c) ^ sg);
 }
 
 __device__ __forceinline__ float gasin(float x)
@@ -171,12 +169,14 @@ __device__ __forceinline__ double sin_poly(double r)
     return fma(ps * r2, r, r);
 }
 
-// pi = PI_A + PI_B + PI_C (each the double nearest to the remainder); with
-// FMA each step rounds once, so r carries a relative error of ~1 ulp.
-__device__ __forceinline__ double reduce_pi(double x, int& k)
+// As for float, with t = x/pi + 1.5*2^52 (valid while |x| < 1.4e15) and
+// pi = PI_A + PI_B + PI_C, each the double nearest to the remainder; with FMA
+// each step rounds once, so r carries a relative error of ~1 ulp.
+__device__ __forceinline__ double reduce_pi(double x, unsigned long long& sign)
 {
-    const double kd = rint(x * 0.3183098861837907);
-    k = (int)kd;
+    const double t = fma(x, 0.3183098861837907, 6755399441055744.0);
+    const double kd = t - 6755399441055744.0;
+    sign = (unsigned long long)__double_as_longlong(t) << 63;
     double r = fma(-kd, 3.141592653589793, x);
     r = fma(-kd, 1.2246467991473532e-16, r);
     return fma(-kd, -2.9947698097183397e-33, r);
@@ -184,26 +184,18 @@ __device__ __forceinline__ double reduce_pi(double x, int& k)
 
 __device__ __forceinline__ double gsin(double x)
 {
-    if (fabs(x) > 1048576.0) return sin(x);
-    int k;
-    const double r = reduce_pi(x, k);
-    const double s = sin_poly(r);
-    return (k & 1) ? -s : s;
+    unsigned long long sg;
+    const double r = reduce_pi(x, sg);
+    return __longlong_as_double(__double_as_longlong(sin_poly(r)) ^ (long long)sg);
 }
 
 __device__ __forceinline__ void gsincos(double x, double& s, double& c)
 {
-    if (fabs(x) > 1048576.0) {
-        sincos(x, &s, &c);
-        return;
-    }
-    int k;
-    const double r = reduce_pi(x, k);
+    unsigned long long sg;
+    const double r = reduce_pi(x, sg);
     sincos_poly(r, s, c);
-    if (k & 1) {
-        s = -s;
-        c = -c;
-    }
+    s = __longlong_as_double(__double_as_longlong(s) ^ (long long)sg);
+    c = __longlong_as_double(__double_as_longlong(c) ^ (long long)sg);
 }
 
 __device__ __forceinline__ double gasin(double x)
@@ -221,6 +213,22 @@ __device__ __forceinline__ double gasin(double x)
     p = fma(p, x2, 6.0 / 80.0);                 // n = 2
     p = fma(p, x2, 2.0 / 12.0);                 // n = 1
     return fma(p * x2, x, x);
+}
+
+// sqrt(1 - c) - 1 for the link update's |c|^2 = c (tiny in practice):
+// -c/2 - c^2/8 - c^3/16 - 5c^4/128 when c < 1/64 (float: the first omitted
+// term is 7c^4/128 < 4e-9 relative) or c < 1/8192 (double: < 2e-17), else the
+// exact -c / (1 + sqrt(1 - c)).
+__device__ __forceinline__ float sqrt1m_minus1(float c)
+{
+    if (c < 0.015625f) return c * fmaf(c, fmaf(c, fmaf(c, -5.0f / 128.0f, -1.0f / 16.0f), -1.0f / 8.0f), -0.5f);
+    return -c / (1.0f + sqrtf(1.0f - c));
+}
+
+__device__ __forceinline__ double sqrt1m_minus1(double c)
+{
+    if (c < 0.0001220703125) return c * fma(c, fma(c, fma(c, -5.0 / 128.0, -1.0 / 16.0), -1.0 / 8.0), -0.5);
+    return -c / (1.0 + sqrt(1.0 - c));
 }
 
 }  // namespace gft

@@ -72,6 +72,17 @@ struct Stencil {
     }
 };
 
+// Values a site computes that its +x neighbour needs, carried along an x-march:
+// the sines of the (0,1) and (0,2) plaquette angles, which are the x+e_0
+// site's lower U(1) loop angles, and the doublet transported along the x link,
+// U_0(x) R(theta_0(x)) phi(x), which is the x+e_0 site's D- term.
+template <class C, int ND>
+struct XCarry {
+    bool valid;
+    C s01, s02;
+    Q<C> t0[ND];
+};
+
 // Own-site access to the past level (read, then overwritten with t + dt).
 template <class S>
 struct PastSite {
@@ -83,10 +94,12 @@ struct PastSite {
 // for the "now" level.  obs receives the energy-step observables.
 template <class S, int MODEL, bool ENERGY, class A, class R>
 __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S> ps,
-                                          double (&obs)[kObsCount], unsigned& warn)
+                                          XCarry<S, (MODEL == kModelSM) ? 1 : 2>& carry, double (&obs)[kObsCount],
+                                          unsigned& warn)
 {
     using C = S;  // FP64 form -> double, mixed form -> float
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    const bool have = carry.valid;
     const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
 
     Q<C> U[3];
@@ -99,6 +112,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
 
     // ---- magnetic term: U(1) sines and SU(2) staple sums ----
     C MgY[3] = {(C)0, (C)0, (C)0};
+    // lower U(1) loops of the links 1 and 2 in the planes with x: the x-1 site's (0,1), (0,2) angles
+    const C prev01 = carry.s01, prev02 = carry.s02;
     Q<C> SA[3], SB[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -118,6 +133,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         const C sF = gsin(F);
         MgY[i] -= sF * lap[j];
         MgY[j] += sF * lap[i];
+        if (pl == 0) carry.s01 = sF;
+        if (pl == 1) carry.s02 = sF;
         const Q<C> Cij = qmul(qconj(Uj_pi), Ui_pj);
         const Q<C> Aij = qmul(Cij, U[j]);
         const Q<C> Aji = qmul(qconj(Cij), U[i]);
@@ -144,8 +161,12 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             const Q<C> Uj_mj = acc.q(j, mj);
             const Q<C> Ui_mj = acc.q(i, mj);
             const Q<C> Uj_dg = acc.q(j, dg);
-            const C neigh = -acc.th(j, dg) - acc.th(i, mj) + acc.th(j, mj) + th[i];
-            MgY[i] -= gsin(neigh) * lap[j];
+            if (j == 0 && have) {
+                MgY[i] -= ((i == 1) ? prev01 : prev02) * lap[0];
+            } else {
+                const C neigh = -acc.th(j, dg) - acc.th(i, mj) + acc.th(j, mj) + th[i];
+                MgY[i] -= gsin(neigh) * lap[j];
+            }
             const Q<C> B = qmul(qmul(Uj_mj, qconj(Ui_mj)), qconj(Uj_dg));
             SB[i] = qadd_scaled(SB[i], lap[j], B);
         }
@@ -177,22 +198,26 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     for (int a = 0; a < 3; a++) {
         C sn, cs;
         gsincos(th[a], sn, cs);
-        C sm, cm;
-        gsincos(acc.th(a, n.m[a]), sm, cm);
-        const Q<C> Um = acc.q(a, n.m[a]);
         const Q<C> Uc = qconj(U[a]);
         C j0 = 0, j1 = 0, j2 = 0, j3 = 0;
+        const bool from_carry = (a == 0) && have;
+        C sm = (C)0, cm = (C)1;
+        Q<C> Um = {(C)1, (C)0, (C)0, (C)0};
+        if (!from_carry) {
+            gsincos(acc.th(a, n.m[a]), sm, cm);
+            Um = acc.q(a, n.m[a]);
+        }
 #pragma unroll
         for (int db = 0; db < ND; db++) {
             const Q<C> fp = acc.ph(db, n.p[a]);
-            const Q<C> fm = acc.ph(db, n.m[a]);
-            // D: U_a(x-a) phi(x-a) + U_a(x)^dag phi(x+a)
-            const Q<C> tm = transport(Um, cm, sm, fm);
+            // D: U_a(x-a) phi(x-a) + U_a(x)^dag phi(x+a); the first is the x-1 site's transported doublet
+            const Q<C> tm = from_carry ? carry.t0[db] : transport(Um, cm, sm, acc.ph(db, n.m[a]));
             const Q<C> tp = transport(Uc, cs, -sn, fp);
             D[db] = qadd_scaled(D[db], lap[a], tm);
             D[db] = qadd_scaled(D[db], lap[a], tp);
             // J: Im of (U_a(x) phi(x))^dag sigma phi(x+a)
             const Q<C> t = transport(U[a], cs, sn, fc[db]);
+            if (a == 0) carry.t0[db] = t;
             j0 += t.w * fp.x - t.x * fp.w + t.y * fp.z - t.z * fp.y;
             j1 += t.w * fp.z - t.x * fp.y + t.y * fp.x - t.z * fp.w;
             j2 += -t.w * fp.y - t.x * fp.z + t.y * fp.w + t.z * fp.x;
@@ -272,7 +297,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     // ---- scalar leapfrog (Model.cpp:347-356):
     //      phi(t+dt) = phi + [(phi - phi_past)(1 - damping) + dt^2 (D - dV)], one rounding at the end
     double kin_e = 0.0, phisq = 0.0;
-    bool finite = true;
+    C check = (C)0;  // sum of every new value: non-finite iff one of them is
     const C dt2 = (C)P.dt2;
     const C keep = (C)(1.0 - P.damping_step);
 #pragma unroll
@@ -286,7 +311,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         for (int k = 0; k < 4; k++) {
             const C vel = fn[k] - fo[k];
             out[k] = fn[k] + (keep * vel + dt2 * (dd[k] - Pot[db][k]));
-            finite = finite && isfinite(out[k]);
+            check += out[k];
             if (ENERGY) {
                 const double v = (double)vel / P.dt;
                 kin_e += 0.5 * v * v;
@@ -322,6 +347,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt * (P.inv_g_sqr * one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * h * h);
         }
         if (R0 * R0 > (C)1) warn |= kWarnAsin;
+        if (fabs(th[d]) > (C)1e4) warn |= kWarnRange;
         // theta(t+dt) = theta(t) + asin(RHS_Y)
         const C thn = th[d] + gasin(R0);
         // u = (sqrt(1-|c|^2), c); U(t+dt) = normalise(u U(t)), written as U + correction:
@@ -329,7 +355,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         //   |U + dU|^2 - 1 = (|U|^2 - 1) + 2 U.dU + |dU|^2 =: e,  1/sqrt(1+e) - 1 = -e/2 + 3e^2/8
         const C cm = R1 * R1 + R2 * R2 + R3 * R3;
         if (cm > (C)1) warn |= kWarnSqrt;
-        const C u0m1 = -cm / ((C)1 + sqrt_((C)1 - cm));
+        const C u0m1 = sqrt1m_minus1(cm);
         const Q<C> dU = qmul(Q<C>{u0m1, R1, R2, R3}, Un);
         C e = fma(Un.w, Un.w, (C)-1);
         e = fma(Un.x, Un.x, e);
@@ -341,12 +367,12 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         const C fm1 = e * ((C)0.375 * e - (C)0.5);
         const Q<C> Unew = {Un.w + (dU.w + fm1 * (Un.w + dU.w)), Un.x + (dU.x + fm1 * (Un.x + dU.x)),
                            Un.y + (dU.y + fm1 * (Un.y + dU.y)), Un.z + (dU.z + fm1 * (Un.z + dU.z))};
-        finite = finite && isfinite(thn) && isfinite(Unew.w) && isfinite(Unew.x) && isfinite(Unew.y) &&
-                 isfinite(Unew.z);
+        check += thn + e;
         ps.L.th[d][ps.s] = thn;
         st4(ps.L.q[d], ps.s, Unew.w, Unew.x, Unew.y, Unew.z);
     }
-    if (!finite) warn |= kWarnNonFinite;
+    if (!isfinite(check)) warn |= kWarnNonFinite;
+    carry.valid = true;
 
     if (ENERGY) {
         obs[kObsPotential] += pot_e;

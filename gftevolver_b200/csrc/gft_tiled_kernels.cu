@@ -242,6 +242,8 @@ __global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_consta
     const int cq0 = (ty + 1) * G::QP + (tz + 1);
     const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
     const int y = y0 + ty, z = z0 + tz;
+    XCarry<S, ND> carry;
+    carry.valid = false;
 
     for (int i = 0; i < nloc; i++) {
         // planes i (x-1), i+1 (x), i+2 (x+1) must be resident; i+2 is new except at i = 0
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_consta
         n.d21 = {bc, cq0 - G::QP + 1, ch0 - G::HP + 1};
         const int x = x0 + i;
         const int s = (x * P.ny + y) * P.nz + z;
-        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, obs, warn);
+        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn);
 
         __syncthreads();  // every thread is done with plane i's buffer
         if (tid == 0 && i + G::NBUF < nplanes)

@@ -48,6 +48,7 @@ extern "C" {
 #define GFT_W_ASIN_DOMAIN 1     /* |RHS_Y| > 1 somewhere (theta update used asin outside [-1,1]) */
 #define GFT_W_SQRT_DOMAIN 2     /* |c|^2 > 1 somewhere (SU(2) update used sqrt of a negative number) */
 #define GFT_W_NONFINITE 4       /* a non-finite value was written */
+#define GFT_W_RANGE 16          /* a link phase |theta| > 1e4: the throughput forms' sin/cos lose accuracy */
 
 /* ---- model / form selectors -------------------------------------------- */
 /* Model.cfg plugin triples (Core/Header/Model.hpp:19-21) that are built. */
