@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=None, help="steps for the FP64 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", choices=["auto", "global", "tiled"], default="auto",
+                    help="step kernel of the throughput forms")
+    ap.add_argument("--tile", type=int, default=0, help="tiled kernel: tile shape index (0: 8x32, 1: 4x32, 2: 4x16)")
+    ap.add_argument("--march", type=int, default=32, help="tiled kernel: planes per CTA along x")
     return ap.parse_args()
 
 
@@ -262,8 +266,12 @@ def main():
     sbytes = 8 if form in ("fp64", "ref64") else 4
     balg = B_ALG[(args.model, sbytes)]
 
+    kind = {"auto": 0, "global": 1, "tiled": 2}[args.kernel]
+
     def timed_run(form_, steps, warmup, sampler=None):
         ev = Evolver(p, form=form_, device=local)
+        if form_ == "mixed" and (kind != 0 or args.tile != 0 or args.march != 32):
+            ev.set_kernel(kind, args.tile, args.march)
         ev.init_fields(ic)
         if warmup:
             ev.evolve(warmup)
@@ -360,7 +368,8 @@ def main():
                                f"energy+Gauss analysers every {LOG_EVERY} steps",
                    "lattice": [p.nx, p.ny, p.nz], "form": form, "log_every": LOG_EVERY,
                    "l2": "inputs larger than L2 (state %.2f GB per level pair)" % (2 * p.nsite * (15 + p.nsc) * sbytes / 1e9),
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "kernel": args.kernel, "tile": args.tile, "march": args.march},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "step kernel",
                      "bytes_per_site_update": balg, "avg_kernel_ms": kms, "kernel_launches_timed": nk},

@@ -63,7 +63,8 @@ struct gft_handle {
     int tile_variant = 0;   // tiled: index into the built tile shapes
     int march = 32;         // tiled: planes per CTA along x
     bool tiled_ready = false;
-    TMaps tm[2];
+    TMaps tm[2];   // staged "now" planes (with halo), per level
+    TMaps tp[2];   // past-level L2 prefetch boxes (no halo), per level
 
     int fail(int code, const std::string& msg)
     {
@@ -160,6 +161,18 @@ void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
 
 size_t level_words(int nsite, int nsc) { return padded_sites(nsite) * (15 + (size_t)nsc); }
 
+// Tensor maps of both levels for a tile shape: staged planes and past prefetch.
+bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm, TMaps* tp)
+{
+    int ty, tz;
+    tiled_tile(tile, ty, tz);
+    for (int t = 0; t < 2; t++) {
+        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, true, &tm[t])) return false;
+        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, false, &tp[t])) return false;
+    }
+    return true;
+}
+
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
     if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1) return false;
@@ -186,10 +199,10 @@ cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelP
     if constexpr (sizeof(S) == 4) {
         if (use_tiled(h, P)) {
             if (model == GFT_MODEL_SM)
-                return launch_tiled_step<S, kModelSM>(h->tm[tn], P, now, past, h->tile_variant, h->march, h->d_status,
-                                                      h->d_part_e, energy, h->stream);
-            return launch_tiled_step<S, kModel2HDM>(h->tm[tn], P, now, past, h->tile_variant, h->march, h->d_status,
-                                                    h->d_part_e, energy, h->stream);
+                return launch_tiled_step<S, kModelSM>(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
+                                                      h->d_status, h->d_part_e, energy, h->stream);
+            return launch_tiled_step<S, kModel2HDM>(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
+                                                    h->d_status, h->d_part_e, energy, h->stream);
         }
     }
     if (model == GFT_MODEL_SM)
@@ -309,25 +322,10 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     }
     const StepParams P = make_params(h, 0, false);
     if (cfg->form == GFT_FORM_MIXED) {
-        bool ok = true;
-        for (int t = 0; t < 2 && ok; t++) {
-            int ty, tz;
-            tiled_tile(0, ty, tz);
-            ok = tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &h->tm[t]);
-        }
-        h->tiled_ready = ok;
         // default tile: the largest built shape the lattice divides
         h->tile_variant = 0;
         while (h->tile_variant < kTiledVariants && !tiled_supported(P, h->tile_variant)) h->tile_variant++;
-        if (h->tile_variant == kTiledVariants) h->tiled_ready = false;
-        else if (h->tile_variant != 0) {
-            for (int t = 0; t < 2 && ok; t++) {
-                int ty, tz;
-                tiled_tile(h->tile_variant, ty, tz);
-                ok = tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &h->tm[t]);
-            }
-            h->tiled_ready = ok;
-        }
+        h->tiled_ready = h->tile_variant < kTiledVariants && encode_tiled(h, P, h->tile_variant, h->tm, h->tp);
     }
     int nb = std::max(fast_launch_blocks(P, 0), fast_gauss_blocks(P));
     nb = std::max(nb, ref_launch_blocks(P));
@@ -668,12 +666,9 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     const StepParams P = make_params(h, h->time_iter, false);
     if (!tiled_supported(P, tile))
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the lattice shape does not divide into this tile");
-    int ty, tz;
-    tiled_tile(tile, ty, tz);
-    TMaps tm[2];
-    for (int t = 0; t < 2; t++)
-        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, &tm[t]))
-            return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed");
+    TMaps tm[2], tp[2];
+    if (!encode_tiled(h, P, tile, tm, tp))
+        return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed");
     const int nb = tiled_blocks(P, tile, march);
     if (nb > h->part_cap) {
         cudaStreamSynchronize(h->stream);
@@ -687,6 +682,8 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     }
     h->tm[0] = tm[0];
     h->tm[1] = tm[1];
+    h->tp[0] = tp[0];
+    h->tp[1] = tp[1];
     h->tiled_ready = true;
     h->tile_variant = tile;
     h->march = march;

@@ -36,12 +36,14 @@ struct TMaps {
     CUtensorMap th[3];
     CUtensorMap ph[2];
 };
+// halo = true: boxes with the one-site halo (staged "now" planes); false: the
+// bare tile (L2 prefetch of the own-site past level).
 template <class S>
-bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, TMaps* out);
+bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, bool halo, TMaps* out);
 bool tiled_supported(const StepParams& P, int variant);
 int tiled_blocks(const StepParams& P, int variant, int lx);
 template <class S, int MODEL>
-cudaError_t launch_tiled_step(const TMaps& maps, const StepParams& P, const LevelPtrs<S>& now,
+cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
                               bool energy, cudaStream_t stream);
 constexpr int kTiledVariants = 3;  // 8x32, 4x32, 4x16 (TY x TZ)

@@ -92,6 +92,32 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+__device__ __forceinline__ void tma_prefetch_l2_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(c0),
+                 "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap* map, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(c0), "r"(c1),
+                 "r"(c2)
+                 : "memory");
+}
+
+// Warm L2 with the own-site past-level tile of plane X (boxes without halo).
+template <int ND>
+__device__ __forceinline__ void prefetch_past(const TMaps& pm, int X, int y0, int z0)
+{
+#pragma unroll
+    for (int d = 0; d < 3; d++) tma_prefetch_l2_4d(&pm.q[d], 0, z0, y0, X);
+#pragma unroll
+    for (int d = 0; d < 3; d++) tma_prefetch_l2_3d(&pm.th[d], z0, y0, X);
+#pragma unroll
+    for (int k = 0; k < ND; k++) tma_prefetch_l2_4d(&pm.ph[k], 0, z0, y0, X);
+}
+
 // Shared-memory plane geometry.
 template <class S, int TY, int TZ, int ND>
 struct Geom {
@@ -198,7 +224,8 @@ __device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const Le
 }
 
 template <class S, int MODEL, int TY, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_constant__ TMaps maps, StepParams P,
+__global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_constant__ TMaps maps,
+                                                             const __grid_constant__ TMaps pmaps, StepParams P,
                                                              LevelPtrs<S> now, LevelPtrs<S> past, int lx,
                                                              unsigned* status, double* partials)
 {
@@ -231,6 +258,10 @@ __global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_consta
     if (tid == 0) {
         for (int p = 0; p < min(G::NBUF, nplanes); p++)
             issue_plane<S, TY, TZ, ND>(maps, smem + p * G::BUF, &bars[p], plane_x(p), y0, z0);
+    }
+    if (tid == 32 % (TY * TZ)) {
+        // past level of the first two planes computed (relative planes 1 and 2)
+        for (int p = 1; p <= 2 && p <= nloc; p++) prefetch_past<ND>(pmaps, plane_x(p), y0, z0);
     }
 
     double obs[kObsCount];
@@ -278,6 +309,7 @@ __global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_consta
         site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn);
 
         __syncthreads();  // every thread is done with plane i's buffer
+        if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
         if (tid == 0 && i + G::NBUF < nplanes)
             issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
                                        plane_x(i + G::NBUF), y0, z0);
@@ -314,7 +346,7 @@ EncodeTiledFn encode_fn()
 }  // namespace
 
 template <class S>
-bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, TMaps* out)
+bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, bool halo, TMaps* out)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
@@ -325,11 +357,12 @@ bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int t
     // quaternion / doublet arrays: dims {4, nz, ny, nx}
     const cuuint64_t qdim[4] = {4, (cuuint64_t)P.nz, (cuuint64_t)P.ny, (cuuint64_t)P.nx};
     const cuuint64_t qstr[3] = {4 * es, 4 * es * P.nz, 4 * es * P.nz * P.ny};
-    const cuuint32_t qbox[4] = {4, (cuuint32_t)(tz + 2), (cuuint32_t)(ty + 2), 1};
+    const int hz = halo ? 2 : 0, hy = halo ? 2 : 0, hp = halo ? 2 * tp : 0;
+    const cuuint32_t qbox[4] = {4, (cuuint32_t)(tz + hz), (cuuint32_t)(ty + hy), 1};
     // theta arrays: dims {nz, ny, nx}
     const cuuint64_t hdim[3] = {(cuuint64_t)P.nz, (cuuint64_t)P.ny, (cuuint64_t)P.nx};
     const cuuint64_t hstr[2] = {es * P.nz, es * P.nz * P.ny};
-    const cuuint32_t hbox[3] = {(cuuint32_t)(tz + 2 * tp), (cuuint32_t)(ty + 2), 1};
+    const cuuint32_t hbox[3] = {(cuuint32_t)(tz + hp), (cuuint32_t)(ty + hy), 1};
     for (int d = 0; d < 3; d++) {
         if (enc(&out->q[d], dt, 4, L.q[d], qdim, qstr, qbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
@@ -369,7 +402,7 @@ int tiled_blocks(const StepParams& P, int variant, int lx)
 }
 
 template <class S, int MODEL, int TY, int TZ>
-static cudaError_t launch_tiled_t(const TMaps& maps, const StepParams& P, const LevelPtrs<S>& now,
+static cudaError_t launch_tiled_t(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                                   const LevelPtrs<S>& past, int lx, unsigned* status, double* partials, bool energy,
                                   cudaStream_t stream)
 {
@@ -380,34 +413,34 @@ static cudaError_t launch_tiled_t(const TMaps& maps, const StepParams& P, const 
     if (energy) {
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, true>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, P, now, past, lx, status, partials);
+        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, now, past, lx, status, partials);
     } else {
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, P, now, past, lx, status, partials);
+        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, now, past, lx, status, partials);
     }
     return cudaGetLastError();
 }
 
 template <class S, int MODEL>
-cudaError_t launch_tiled_step(const TMaps& maps, const StepParams& P, const LevelPtrs<S>& now,
+cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
                               bool energy, cudaStream_t stream)
 {
     switch (variant) {
-    case 0: return launch_tiled_t<S, MODEL, 8, 32>(maps, P, now, past, lx, status, partials, energy, stream);
-    case 1: return launch_tiled_t<S, MODEL, 4, 32>(maps, P, now, past, lx, status, partials, energy, stream);
-    default: return launch_tiled_t<S, MODEL, 4, 16>(maps, P, now, past, lx, status, partials, energy, stream);
+    case 0: return launch_tiled_t<S, MODEL, 8, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
+    case 1: return launch_tiled_t<S, MODEL, 4, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
+    default: return launch_tiled_t<S, MODEL, 4, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
     }
 }
 
-template bool tiled_encode_maps<float>(const StepParams&, const LevelPtrs<float>&, int, int, int, TMaps*);
-template bool tiled_encode_maps<double>(const StepParams&, const LevelPtrs<double>&, int, int, int, TMaps*);
-template cudaError_t launch_tiled_step<float, kModelSM>(const TMaps&, const StepParams&, const LevelPtrs<float>&,
-                                                        const LevelPtrs<float>&, int, int, unsigned*, double*, bool,
-                                                        cudaStream_t);
-template cudaError_t launch_tiled_step<float, kModel2HDM>(const TMaps&, const StepParams&, const LevelPtrs<float>&,
-                                                          const LevelPtrs<float>&, int, int, unsigned*, double*, bool,
-                                                          cudaStream_t);
+template bool tiled_encode_maps<float>(const StepParams&, const LevelPtrs<float>&, int, int, int, bool, TMaps*);
+template bool tiled_encode_maps<double>(const StepParams&, const LevelPtrs<double>&, int, int, int, bool, TMaps*);
+template cudaError_t launch_tiled_step<float, kModelSM>(const TMaps&, const TMaps&, const StepParams&,
+                                                        const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
+                                                        unsigned*, double*, bool, cudaStream_t);
+template cudaError_t launch_tiled_step<float, kModel2HDM>(const TMaps&, const TMaps&, const StepParams&,
+                                                          const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
+                                                          unsigned*, double*, bool, cudaStream_t);
 
 }  // namespace gft
