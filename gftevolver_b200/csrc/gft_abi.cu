@@ -11,7 +11,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gft.h"
+#include "gft.h"
 #include "gft_launch.h"
 
 using namespace gft;
