@@ -181,6 +181,51 @@ __device__ __forceinline__ void issue_plane(const TMaps& maps, unsigned char* bu
     for (int k = 0; k < ND; k++) tma_load_4d(buf + G::OFF_PH + k * G::QB, &maps.ph[k], 0, z0 - 1, y0 - 1, X, bar);
 }
 
+// Halo cell handled by thread `tid` (2*QP + 2*TY cells: rows 0 and TY+1, then
+// columns 0 and TZ+1); false if tid has none.
+template <int TY, int QP>
+__device__ __forceinline__ bool halo_cell(int tid, int& ly, int& lz)
+{
+    if (tid >= 2 * QP + 2 * TY) return false;
+    if (tid < QP) {
+        ly = 0;
+        lz = tid;
+    } else if (tid < 2 * QP) {
+        ly = TY + 1;
+        lz = tid - QP;
+    } else if (tid < 2 * QP + TY) {
+        ly = 1 + (tid - 2 * QP);
+        lz = 0;
+    } else {
+        ly = 1 + (tid - 2 * QP - TY);
+        lz = QP - 1;
+    }
+    return true;
+}
+
+// Warm L2 with the wrapped halo sites of plane X (one plane before they are
+// patched), so the patch loads do not wait on DRAM.
+template <class S, int TY, int TZ, int ND>
+__device__ __forceinline__ void prefetch_wrapped_halo(const StepParams& P, const LevelPtrs<S>& now, int X, int y0,
+                                                      int z0, int tid)
+{
+    using G = Geom<S, TY, TZ, ND>;
+    int ly, lz;
+    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
+    int y = y0 - 1 + ly, z = z0 - 1 + lz;
+    if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;
+    y = (y < 0) ? y + P.ny : (y >= P.ny ? y - P.ny : y);
+    z = (z < 0) ? z + P.nz : (z >= P.nz ? z - P.nz : z);
+    const size_t s = ((size_t)X * P.ny + y) * P.nz + z;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(now.q[d] + 4 * s));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(now.th[d] + s));
+    }
+#pragma unroll
+    for (int k = 0; k < ND; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(now.ph[k] + 4 * s));
+}
+
 // Halo cells of plane X whose (y, z) leaves the lattice: load the wrapped
 // site from global memory into the staged plane.
 template <class S, int TY, int TZ, int ND>
@@ -188,22 +233,8 @@ __device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const Le
                                                    int X, int y0, int z0, int tid)
 {
     using G = Geom<S, TY, TZ, ND>;
-    constexpr int NH = 2 * G::QP + 2 * TY;
-    if (tid >= NH) return;
     int ly, lz;
-    if (tid < G::QP) {
-        ly = 0;
-        lz = tid;
-    } else if (tid < 2 * G::QP) {
-        ly = TY + 1;
-        lz = tid - G::QP;
-    } else if (tid < 2 * G::QP + TY) {
-        ly = 1 + (tid - 2 * G::QP);
-        lz = 0;
-    } else {
-        ly = 1 + (tid - 2 * G::QP - TY);
-        lz = TZ + 1;
-    }
+    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
     int y = y0 - 1 + ly, z = z0 - 1 + lz;
     if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;  // delivered by the tensor copy
     y = (y < 0) ? y + P.ny : (y >= P.ny ? y - P.ny : y);
@@ -310,6 +341,8 @@ __global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_consta
 
         __syncthreads();  // every thread is done with plane i's buffer
         if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
+        // plane i+3 is waited (and patched) in the next iteration
+        if (wraps && i + 3 < nplanes) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 3), y0, z0, tid);
         if (tid == 0 && i + G::NBUF < nplanes)
             issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
                                        plane_x(i + G::NBUF), y0, z0);
