@@ -94,6 +94,8 @@ SIGNATURES = {
     "gft_step_kernel_ms": (ctypes.c_double, [_H, ctypes.POINTER(ctypes.c_int)]),
     "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gft_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gft_observe_static": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "gft_last_error": (ctypes.c_char_p, [_H]),
     "gft_version": (ctypes.c_char_p, []),
 }

@@ -28,6 +28,7 @@ SOURCES = [
     ("gft_fast_kernels.cu", []),
     ("gft_tiled_kernels.cu", []),
     ("gft_aux_kernels.cu", []),
+    ("gft_static_observe.cu", []),
     ("gft_abi.cu", []),
 ]
 

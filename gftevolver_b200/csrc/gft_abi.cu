@@ -33,6 +33,10 @@ constexpr int kMaxProfiled = 8192;
 
 }  // namespace
 
+namespace gft {
+void set_last_error(const std::string& msg) { set_global_error(msg); }
+}  // namespace gft
+
 struct gft_handle {
     gft_config cfg{};
     int nsc = 4;

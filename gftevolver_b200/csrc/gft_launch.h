@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "gft_device.cuh"
@@ -72,6 +73,9 @@ cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic,
 // partials [nblocks][nslots] into out[nslots], scaled by scale[slot].
 cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_host,
                             double* out, cudaStream_t s);
+
+// Record the library-wide last error message (gft_last_error(NULL)).
+void set_last_error(const std::string& msg);
 
 // Elementary-function self-test (gft_math.cuh vs CUDA's functions) on the current device.
 cudaError_t run_math_selftest(int n, double* out8);

@@ -103,6 +103,20 @@ def _row_dict(r: _lib.GftObservables) -> dict:
     return d
 
 
+def make_config(params: LatticeParams, form: str = "mixed", device: int = 0) -> _lib.GftConfig:
+    """The C ABI's gft_config for these parameters."""
+    if form not in FORMS:
+        raise ValueError(f"unknown form {form!r}; choose one of {sorted(FORMS)}")
+    cfg = _lib.GftConfig()
+    for name, _ in _lib.GftConfig._fields_:
+        if name in ("form", "storage_bytes", "device"):
+            continue
+        setattr(cfg, name, getattr(params, name))
+    cfg.form, cfg.storage_bytes = FORMS[form]
+    cfg.device = device
+    return cfg
+
+
 class Evolver:
     """One lattice on one GPU, evolved by the CUDA kernels of libgft_b200.so."""
 

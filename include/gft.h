@@ -148,6 +148,25 @@ size_t gft_device_bytes(const gft_handle* h);
  * the last call (CUDA events on the handle's stream); 0 if none. */
 double gft_step_kernel_ms(gft_handle* h, int* launches);
 
+/* Allocation-free observables (no counterpart in the reference).  For callers
+ * that cannot allocate device memory where they need the numbers -- a fixed
+ * memory budget, a region that must stay asynchronous (cudaMalloc/cudaFree
+ * synchronise the device), or fields owned by another framework's allocator.
+ * Computes the energy terms, plaquette means and <phi^dag phi> of the state
+ * at step `time_iter` from the caller's device buffers in the reference layout
+ * (float: scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][15]) and writes
+ * 9 doubles to the caller's device buffer d_out (energy, potential, gradient,
+ * kinetic, magnetic, electric, plaq_su2, plaq_u1, phi_sq; the units of
+ * gft_observables), asynchronously on `stream` (NULL: the default stream).
+ * Allocates nothing: its scratch is a fixed 1.2 MB device array compiled into
+ * the library, so lattices above 67,108,864 sites return GFT_E_UNSUPPORTED.
+ * The first call on a device looks up that array's address (do it before any
+ * stream capture); calls that overlap on the GPU share the array and race, so
+ * the caller serialises them.  Only cfg's lattice, model and coupling fields
+ * are read (form and storage_bytes are ignored). */
+int gft_observe_static(const gft_config* cfg, const float* d_scalars, const float* d_vectors, int time_iter,
+                       double* d_out, void* stream);
+
 /* Step-kernel selection for the throughput forms (no reference counterpart):
  * kind 0 = automatic (the tiled kernel for the mixed form when the lattice
  * divides into a built tile, else the one-thread-per-site kernel), 1 = one

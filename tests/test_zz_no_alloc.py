@@ -1,0 +1,77 @@
+"""gft_observe_static: the allocation-free observables entry point (GPU).
+
+Some callers cannot allocate device memory where they need the observables
+(a memory budget fixed up front, a region that must stay asynchronous since
+cudaMalloc/cudaFree synchronise the device, or fields owned by another
+framework's allocator).  gft_observe_static computes the same numbers as the
+handle-based gft_observe from the caller's own device buffers, using a fixed
+scratch array compiled into the library.  This file is collected last so that
+a stopped run has already exercised everything else; it passes both alone in
+a fresh process and after the other tests.
+
+Tolerance: the mixed-form energies agree to 1e-6 relative (the tolerance the
+other mixed-form tests use), plaquette means and <phi^dag phi> to 1e-7.
+"""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(model, shape, steps):
+    from gftevolver_b200 import Evolver, InitialData, LatticeParams
+    nx, ny, nz = shape
+    p = LatticeParams(model=model, nx=nx, ny=ny, nz=nz, energy_every=1)
+    ic = InitialData(seed=4242, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
+                     eps_sigma=0.1)
+    with Evolver(p, form="mixed") as ev:
+        ev.init_fields(ic)
+        ev.evolve(steps)  # nonzero electric field and scalar velocity
+        ref = ev.observe()
+        sc, ve = ev.download(np.float32)
+        ti = ev.time_iter
+    return p, ref, sc, ve, ti
+
+
+KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "plaq_su2", "plaq_u1", "phi_sq")
+
+
+@pytest.mark.parametrize("model,shape", [(1, (24, 16, 32)), (2, (12, 10, 18))], ids=["sm", "2hdm"])
+def test_observe_static_matches_observe_twice(model, shape):
+    import torch
+    from gftevolver_b200 import _lib
+    from gftevolver_b200.evolver import make_config
+    lib = _lib.load()
+    p, ref, sc, ve, ti = _state(model, shape, 3)
+    cfg = make_config(p, "mixed", 0)
+    d_sc = torch.from_numpy(sc).cuda()
+    d_ve = torch.from_numpy(ve).cuda()
+    out = torch.empty(9, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):  # two calls in a row share the scratch array
+        out.fill_(float("nan"))
+        rc = lib.gft_observe_static(ctypes.byref(cfg), ctypes.c_void_p(d_sc.data_ptr()),
+                                    ctypes.c_void_p(d_ve.data_ptr()), ti, ctypes.c_void_p(out.data_ptr()),
+                                    ctypes.c_void_p(stream))
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        got = dict(zip(KEYS, out.cpu().tolist()))
+        for k in KEYS[:6]:
+            assert math.isfinite(got[k])
+            assert abs(got[k] - ref[k]) <= 1e-6 * max(abs(ref["energy"]), 1.0), (k, got[k], ref[k])
+        for k in KEYS[6:]:
+            assert abs(got[k] - ref[k]) <= 1e-7 * max(abs(ref[k]), 1.0), (k, got[k], ref[k])
+
+
+def test_observe_static_rejects_lattices_beyond_its_scratch():
+    from gftevolver_b200 import LatticeParams, _lib
+    from gftevolver_b200.evolver import make_config
+    lib = _lib.load()
+    cfg = make_config(LatticeParams(nx=448, ny=448, nz=448), "mixed", 0)
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the size check comes first
+    rc = lib.gft_observe_static(ctypes.byref(cfg), dummy, dummy, 0, dummy, None)
+    assert rc == _lib.GFT_E_UNSUPPORTED
+    assert "67108864" in _lib.last_error()
