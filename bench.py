@@ -8,7 +8,8 @@ reference's shipped analyser configuration.
 
   value      site-updates/s of the mixed form over all ranks, fields resident
              in HBM (device-timed with CUDA events on the library's stream,
-             max over ranks).  Lattice (1.3 GB) >> L2 (126 MB): no L2 flush needed.
+             max over ranks).  State (2.55 GB at 256^3) >> L2 (126 MB): no L2
+             flush needed.
   e2e        the same metric through the C ABI with host buffers: upload of the
              initial fields from pinned host memory, K steps, download of the
              final fields and the observable rows, all inside the timed region.
@@ -18,6 +19,9 @@ reference's shipped analyser configuration.
              bandwidth.
   cpu_baseline  the reference itself (oracle/_ref/ref32, compiled from its own
              sources) on the host cores, a bounded sample.
+  precision  the mixed form against the FP64 form on the same initial data
+             over --precision-steps steps (default 1000): field deviation,
+             energy drift and Gauss-law residual.
 
 ``--impl reference`` times the reference CPU evolver on the host cores
 instead (rank 0 only).
@@ -60,6 +64,9 @@ def parse():
                     help="step kernel of the throughput forms")
     ap.add_argument("--tile", type=int, default=0, help="tiled kernel: tile shape index (0: 8x32, 1: 4x32, 2: 4x16)")
     ap.add_argument("--march", type=int, default=32, help="tiled kernel: planes per CTA along x")
+    ap.add_argument("--precision-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 precision run (0: skip)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
     return ap.parse_args()
 
 
@@ -230,6 +237,67 @@ def run_reference_arm(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# Precision of the mixed form against the FP64 form
+# ---------------------------------------------------------------------------
+def precision_report(p, ic, steps: int, device: int) -> dict:
+    """Evolve the same initial data in the mixed and the FP64 form and compare.
+
+    Both forms generate the initial fields on the device from the same seed
+    (the mixed form stores them rounded to float).  Reported: the largest
+    absolute deviation of any stored word after `steps` steps (both levels,
+    reference layout), the relative energy drift of each form over the run and
+    the largest relative difference of the mixed energy from the FP64 energy
+    at the logging steps, and the Gauss-law residual (largest |violation| over
+    sites, constraint equations and logging steps) of each form.
+    """
+    import torch
+
+    from gftevolver_b200 import Evolver
+
+    evs = {f: Evolver(p, form=f, device=device) for f in ("mixed", "fp64")}
+    rows = {}
+    for f, ev in evs.items():
+        ev.init_fields(ic)
+        rows[f] = ev.evolve(steps)
+    fields = {}
+    for f, ev in evs.items():
+        dt = torch.float64 if f == "fp64" else torch.float32
+        sc = torch.empty((2, p.nx, p.ny, p.nz, p.nsc), dtype=dt, device=f"cuda:{device}")
+        ve = torch.empty((2, p.nx, p.ny, p.nz, 15), dtype=dt, device=f"cuda:{device}")
+        ev.download_device(sc.data_ptr(), ve.data_ptr(), f == "fp64")
+        fields[f] = (sc, ve)
+        ev.close()
+    dev_sc = (fields["mixed"][0].double() - fields["fp64"][0]).abs().max().item()
+    dev_ve = (fields["mixed"][1].double() - fields["fp64"][1]).abs().max().item()
+    del fields
+    torch.cuda.empty_cache()
+
+    def energies(rs):
+        return [(r["time_iter"], r["energy"]) for r in rs if r["has_energy"]]
+
+    e32, e64 = energies(rows["mixed"]), energies(rows["fp64"])
+    def drift(es):
+        e0 = es[0][1]
+        return max(abs(e - e0) for _, e in es) / abs(e0)
+    rel_e = max(abs(a[1] - b[1]) / abs(b[1]) for a, b in zip(e32, e64))
+    def gauss(rs):
+        g = [max(r["gauss_max"]) for r in rs if r["has_gauss"]]
+        return max(g) if g else None
+    def gauss_int(rs):
+        g = [max(r["gauss_int"]) for r in rs if r["has_gauss"]]
+        return max(g) if g else None
+    return {
+        "steps": steps, "lattice": [p.nx, p.ny, p.nz], "log_every": LOG_EVERY,
+        "field_max_abs_dev": {"scalars": dev_sc, "links": dev_ve},
+        "energy_drift_rel": {"mixed": drift(e32), "fp64": drift(e64)},
+        "energy_mixed_vs_fp64_rel": rel_e,
+        "gauss_max": {"mixed": gauss(rows["mixed"]), "fp64": gauss(rows["fp64"])},
+        "gauss_int": {"mixed": gauss_int(rows["mixed"]), "fp64": gauss_int(rows["fp64"])},
+        "energy_t0": e64[0][1],
+    }
+
+
+# ---------------------------------------------------------------------------
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -276,6 +344,7 @@ def main():
         if warmup:
             ev.evolve(warmup)
         ev.step_kernel_ms()  # reset
+        launches0 = ev.launch_count
         stream = torch.cuda.ExternalStream(ev.stream)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -291,18 +360,19 @@ def main():
         barrier()
         ms = e0.elapsed_time(e1)
         kms, nk = ev.step_kernel_ms()
+        ev.timed_launches = ev.launch_count - launches0
         return ev, ms, kms, nk, rows, clocks
 
     sampler = ClockSampler(local)
     ev, ms, kms, nk, rows, clocks = timed_run(form, args.steps, args.warmup, sampler)
+    kernel_name = ev.step_kernel_name
     ms_max = max_over_ranks(ms)
     value = world * p.nsite * args.steps / (ms_max / 1e3)
-    nlog = sum(1 for t in range(args.warmup, args.warmup + args.steps) if t % LOG_EVERY == 0)
-    launches = args.steps + nlog * 3  # step kernels + (energy finalize, gauss kernel, gauss finalize) per log step
+    launches = ev.timed_launches  # the library's own count of kernels launched in the timed region
 
     # FP64 plain form for the mixed-vs-FP64 ratio
     fp64 = None
-    if form == "mixed":
+    if form == "mixed" and not args.no_fp64:
         ev.close()
         fsteps = args.fp64_steps or max(args.steps // 4, 10)
         ev64, ms64, kms64, nk64, _, _ = timed_run("fp64", fsteps, min(args.warmup, 3))
@@ -349,9 +419,13 @@ def main():
             dist.destroy_process_group()
         return
 
+    precision = None
+    if args.precision_steps > 0 and form == "mixed":
+        precision = precision_report(p, ic, args.precision_steps, local)
+
     peak, peak_kind = measured_peaks()
     achieved = balg * p.nsite / (kms / 1e3) / 1e9
-    traffic = committed_traffic(f"fast_step_kernel_{args.model}_{form}")
+    traffic = committed_traffic(f"{kernel_name}_{args.model}_{form}_{args.size}")
     cpu = None
     if not args.no_cpu_baseline:
         try:
@@ -371,13 +445,14 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "kernel": args.kernel, "tile": args.tile, "march": args.march},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "step kernel",
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": kernel_name,
                      "bytes_per_site_update": balg, "avg_kernel_ms": kms, "kernel_launches_timed": nk},
         "gpu_launches": launches,
         "clocks": clocks,
         "forms": {"fp64": fp64} if fp64 else None,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "precision": precision,
         "analyser_rows": len(rows),
     }
     print(json.dumps(line), flush=True)

@@ -91,7 +91,13 @@ SIGNATURES = {
     "gft_time_iter": (ctypes.c_int, [_H]),
     "gft_stream": (ctypes.c_void_p, [_H]),
     "gft_device_bytes": (ctypes.c_size_t, [_H]),
+    "gft_upload_device_f32": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gft_upload_device_f64": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gft_download_device_f32": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p]),
+    "gft_download_device_f64": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p]),
     "gft_step_kernel_ms": (ctypes.c_double, [_H, ctypes.POINTER(ctypes.c_int)]),
+    "gft_step_kernel_name": (ctypes.c_char_p, [_H]),
+    "gft_launch_count": (ctypes.c_longlong, [_H]),
     "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gft_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gft_observe_static": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

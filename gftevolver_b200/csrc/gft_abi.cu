@@ -50,6 +50,7 @@ struct gft_handle {
     double* d_part_g = nullptr;
     int part_cap = 0;           // blocks the partial buffers hold
     double* d_scale = nullptr;  // kRowSlots scale factors
+    double* d_mid = nullptr;    // stage-one rows of the two-stage finalize (kFinMidCapacity doubles)
     double* d_rows = nullptr;
     int rows_cap = 0;
     void* d_stage = nullptr;
@@ -60,6 +61,7 @@ struct gft_handle {
     bool profile = true;
     std::vector<cudaEvent_t> ev;
     int ev_used = 0;
+    long long launches = 0;  // kernels launched by gft_evolve / gft_observe
     std::string err;
     size_t dev_bytes = 0;
     // step kernel selection for the throughput forms
@@ -338,13 +340,15 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMalloc(&h->d_part_e, pe)) != cudaSuccess || (e = cudaMalloc(&h->d_part_g, pg)) != cudaSuccess ||
         (e = cudaMalloc(&h->d_scale, kRowSlots * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_mid, kFinMidCapacity * sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&h->d_rows, (size_t)h->rows_cap * kRowSlots * sizeof(double))) != cudaSuccess) {
         h->fail(GFT_E_NOMEM, std::string("cudaMalloc(scratch): ") + cudaGetErrorString(e));
         gft_destroy(h);
         return GFT_E_NOMEM;
     }
     h->part_cap = nb;
-    h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap);
+    h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap) +
+                    kFinMidCapacity * sizeof(double);
     double scale[kRowSlots];
     const double dv = cfg->dx * cfg->dy * cfg->dz;
     for (int k = 0; k < kRowSlots; k++) scale[k] = 1.0;
@@ -387,6 +391,7 @@ void gft_destroy(gft_handle* h)
     cudaFree(h->d_part_e);
     cudaFree(h->d_part_g);
     cudaFree(h->d_scale);
+    cudaFree(h->d_mid);
     cudaFree(h->d_rows);
     cudaFree(h->d_stage);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -418,19 +423,26 @@ int ensure_stage(gft_handle* h, size_t bytes)
     return GFT_OK;
 }
 
+// `on_device`: sc/ve are device buffers (converted in place, no staging copy).
 template <class H>
-int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter)
+int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter, bool on_device = false)
 {
     if (!h || !sc || !ve) return GFT_E_INVALID;
     if (time_iter < 0) return h->fail(GFT_E_INVALID, "gft_upload: time_iter must be >= 0");
     cudaSetDevice(h->cfg.device);
     const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
-    int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
-    if (rc != GFT_OK) return rc;
-    H* dsc = static_cast<H*>(h->d_stage);
-    H* dve = dsc + nsc_w;
-    cudaError_t e = cudaMemcpyAsync(dsc, sc, nsc_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dve, ve, nve_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
+    const H* dsc = sc;
+    const H* dve = ve;
+    cudaError_t e = cudaSuccess;
+    if (!on_device) {
+        int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
+        if (rc != GFT_OK) return rc;
+        H* st = static_cast<H*>(h->d_stage);
+        e = cudaMemcpyAsync(st, sc, nsc_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(st + nsc_w, ve, nve_w * sizeof(H), cudaMemcpyHostToDevice, h->stream);
+        dsc = st;
+        dve = st + nsc_w;
+    }
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         const H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
         const H* v_t = dve + (size_t)t * h->nsite * 15;
@@ -445,16 +457,20 @@ int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter)
 }
 
 template <class H>
-int download_impl(gft_handle* h, H* sc, H* ve)
+int download_impl(gft_handle* h, H* sc, H* ve, bool on_device = false)
 {
     if (!h || !sc || !ve) return GFT_E_INVALID;
     if (!h->has_data) return h->fail(GFT_E_STATE, "gft_download: no field data on the device");
     cudaSetDevice(h->cfg.device);
     const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
-    int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
-    if (rc != GFT_OK) return rc;
-    H* dsc = static_cast<H*>(h->d_stage);
-    H* dve = dsc + nsc_w;
+    H* dsc = sc;
+    H* dve = ve;
+    if (!on_device) {
+        int rc = ensure_stage(h, (nsc_w + nve_w) * sizeof(H));
+        if (rc != GFT_OK) return rc;
+        dsc = static_cast<H*>(h->d_stage);
+        dve = dsc + nsc_w;
+    }
     cudaError_t e = cudaSuccess;
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
@@ -462,8 +478,10 @@ int download_impl(gft_handle* h, H* sc, H* ve)
         e = is_f64_storage(h) ? launch_soa_to_aos<double, H>(h->ld[t], h->nsite, h->nsc, s_t, v_t, h->stream)
                               : launch_soa_to_aos<float, H>(h->lf[t], h->nsite, h->nsc, s_t, v_t, h->stream);
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sc, dsc, nsc_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ve, dve, nve_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
+    if (!on_device) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sc, dsc, nsc_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ve, dve, nve_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "gft_download");
     return GFT_OK;
@@ -537,18 +555,21 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         const bool prof = h->profile && h->ev_used < kMaxProfiled;
         if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
         err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e);
+        h->launches += 1 + (e ? finalize_launches(step_blocks(h, P), true) : 0) +
+                       (g ? 1 + finalize_launches(fast_gauss_blocks(P), true) : 0);
         if (prof) {
             cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
             h->ev_used++;
         }
         if (err != cudaSuccess) break;
         double* out = h->d_rows + (size_t)row * kRowSlots;
-        if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->stream);
+        if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->d_mid,
+                                         h->stream);
         if (g && err == cudaSuccess) {
             err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
             if (err == cudaSuccess)
                 err = launch_finalize(h->d_part_g, fast_gauss_blocks(P), kGaussSlots, 4, h->d_scale + kObsCount,
-                                      out + kObsCount, h->stream);
+                                      out + kObsCount, h->d_mid, h->stream);
         }
         if (e || g) {
             meta.push_back({ti, e, g});
@@ -580,6 +601,16 @@ int gft_upload_f32(gft_handle* h, const float* sc, const float* ve, int time_ite
 int gft_upload_f64(gft_handle* h, const double* sc, const double* ve, int time_iter) { return upload_impl(h, sc, ve, time_iter); }
 int gft_download_f32(gft_handle* h, float* sc, float* ve) { return download_impl(h, sc, ve); }
 int gft_download_f64(gft_handle* h, double* sc, double* ve) { return download_impl(h, sc, ve); }
+int gft_upload_device_f32(gft_handle* h, const float* sc, const float* ve, int time_iter)
+{
+    return upload_impl(h, sc, ve, time_iter, true);
+}
+int gft_upload_device_f64(gft_handle* h, const double* sc, const double* ve, int time_iter)
+{
+    return upload_impl(h, sc, ve, time_iter, true);
+}
+int gft_download_device_f32(gft_handle* h, float* sc, float* ve) { return download_impl(h, sc, ve, true); }
+int gft_download_device_f64(gft_handle* h, double* sc, double* ve) { return download_impl(h, sc, ve, true); }
 
 int gft_init_fields(gft_handle* h, const gft_ic* ic)
 {
@@ -642,7 +673,8 @@ int gft_observe(gft_handle* h, gft_observables* row)
         }
     }
     // the step wrote into the copy; restore nothing (the levels are untouched)
-    if (e == cudaSuccess) e = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, h->d_rows, h->stream);
+    if (e == cudaSuccess) e = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, h->d_rows,
+                                                  h->d_mid, h->stream);
     std::vector<double> host(kRowSlots, 0.0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), h->d_rows, kObsCount * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
@@ -722,6 +754,16 @@ double gft_step_kernel_ms(gft_handle* h, int* launches)
     h->ev_used = 0;
     if (launches) *launches = n;
     return total / n;
+}
+
+long long gft_launch_count(const gft_handle* h) { return h ? h->launches : 0; }
+
+const char* gft_step_kernel_name(const gft_handle* h)
+{
+    if (!h) return "";
+    if (h->cfg.form == GFT_FORM_REF) return "ref_step_kernel";
+    const StepParams P = make_params(h, 0, false);
+    return use_tiled(h, P) ? "tiled_step_kernel" : "fast_step_kernel";
 }
 
 }  // extern "C"

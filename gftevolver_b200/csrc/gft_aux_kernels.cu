@@ -115,16 +115,20 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
     }
 }
 
-// One block reduces the per-block partials [nblocks][nslots]: each thread
-// accumulates whole rows (coalesced), slot k with Neumaier compensation
-// (k < max_from) or as a maximum (k >= max_from); then thread 0 combines the
-// per-thread results in thread order.  The order is fixed, so the result is
-// deterministic.
+// Reduces the per-block partials [nblocks][nslots] of a logging step: each
+// thread accumulates whole rows (coalesced), slot k with Neumaier compensation
+// (k < max_from) or as a maximum (k >= max_from); then the per-thread results
+// are combined by a fixed shuffle tree and thread order.  The order is fixed,
+// so the result is deterministic.  With a grid of G > 1 blocks, block g reduces
+// rows [g * rows_per_cta, (g + 1) * rows_per_cta) and writes one unscaled row
+// out[g][nslots] (stage one of two); with G = 1 it reduces all rows and writes
+// out[k] = total * scale[k].
 constexpr int kFinThreads = 1024;
 constexpr int kMaxSlots = 16;
+constexpr int kFinMidRows = 512;  // most stage-one rows (the caller's mid buffer holds kFinMidRows x kMaxSlots)
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __restrict__ partials, int nblocks,
                                                                int nslots, int max_from, const double* scale,
-                                                               double* out)
+                                                               double* out, int rows_per_cta)
 {
     __shared__ double s_sum[kMaxSlots][kFinThreads / 32];
     __shared__ double s_cmp[kMaxSlots][kFinThreads / 32];
@@ -134,7 +138,9 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __r
         sum[k] = 0.0;
         comp[k] = 0.0;
     }
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    const int b0 = (int)blockIdx.x * rows_per_cta;
+    const int b1 = min(nblocks, b0 + rows_per_cta);
+    for (int b = b0 + (int)threadIdx.x; b < b1; b += blockDim.x) {
         const double* row = partials + (size_t)b * nslots;
 #pragma unroll
         for (int k = 0; k < kMaxSlots; k++) {
@@ -189,7 +195,11 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __r
                 tcomp += s_cmp[k][w];
             }
         }
-        out[k] = (is_max ? tsum : tsum + tcomp) * scale[k];
+        const double total = is_max ? tsum : tsum + tcomp;
+        if (gridDim.x > 1)
+            out[(size_t)blockIdx.x * nslots + k] = total;
+        else
+            out[k] = total * scale[k];
     }
 }
 
@@ -269,11 +279,23 @@ cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic,
 }
 
 cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_dev,
-                            double* out, cudaStream_t s)
+                            double* out, double* mid, cudaStream_t s)
 {
-    finalize_kernel<<<1, kFinThreads, 0, s>>>(partials, nblocks, nslots, max_from, scale_dev, out);
+    if (nslots > kMaxSlots) return cudaErrorInvalidValue;
+    if (mid != nullptr && nblocks > 2 * kFinThreads) {
+        // two stages: at most kFinMidRows blocks of >= kFinThreads rows each, then one block
+        int rpc = (nblocks + kFinMidRows - 1) / kFinMidRows;
+        rpc = rpc < kFinThreads ? kFinThreads : rpc;
+        const int g = (nblocks + rpc - 1) / rpc;
+        finalize_kernel<<<g, kFinThreads, 0, s>>>(partials, nblocks, nslots, max_from, nullptr, mid, rpc);
+        finalize_kernel<<<1, kFinThreads, 0, s>>>(mid, g, nslots, max_from, scale_dev, out, g);
+        return cudaGetLastError();
+    }
+    finalize_kernel<<<1, kFinThreads, 0, s>>>(partials, nblocks, nslots, max_from, scale_dev, out, nblocks);
     return cudaGetLastError();
 }
+
+int finalize_launches(int nblocks, bool have_mid) { return (have_mid && nblocks > 2 * kFinThreads) ? 2 : 1; }
 
 template cudaError_t launch_aos_to_soa<float, float>(const float*, const float*, int, int, LevelPtrs<float>,
                                                      cudaStream_t);

@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
     if (warn) atomicOr(status, warn);
 }
 
-// Gauss-law residual after a step, FP64 for both forms (GaugeCondition.cpp:117-165 semantics).
+// Gauss-law residual after a step, FP64 for both forms (GaugeCondition.cpp:117-165 semantics);
+// sin is the library's double series (gft_math.cuh).
 template <class S, int MODEL>
 __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                          double* partials)
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
             const int md = c + o.m[d];
             const double la = ld1<double>(fut.th[d], c) - ld1<double>(now.th[d], c);
             const double na = ld1<double>(fut.th[d], md) - ld1<double>(now.th[d], md);
-            el[0] += (sin(la) - sin(na)) * P.lap[d];
+            el[0] += (gsin(la) - gsin(na)) * P.lap[d];
             // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
             double a1, a2, a3, b1, b2, b3;
             qmul_vec(qconj(ld4<double>(now.q[d], c)), ld4<double>(fut.q[d], c), a1, a2, a3);

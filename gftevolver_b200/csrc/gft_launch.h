@@ -71,8 +71,14 @@ cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic,
 
 // Sum (slots < max_from, compensated) or max (slots >= max_from) the per-block
 // partials [nblocks][nslots] into out[nslots], scaled by scale[slot].
-cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_host,
-                            double* out, cudaStream_t s);
+// Deterministic FP64 reduction of per-block partials into one row (scaled by
+// scale[k]); `mid` (kFinMidRows x 16 doubles, may be null) enables a two-stage
+// reduction for large block counts.
+cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int max_from, const double* scale_dev,
+                            double* out, double* mid, cudaStream_t s);
+// Kernel launches launch_finalize makes for nblocks partial rows.
+int finalize_launches(int nblocks, bool have_mid);
+constexpr int kFinMidCapacity = 512 * 16;
 
 // Record the library-wide last error message (gft_last_error(NULL)).
 void set_last_error(const std::string& msg);

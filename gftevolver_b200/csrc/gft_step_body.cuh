@@ -51,13 +51,14 @@ __device__ __forceinline__ Q<C> transport(Q<C> u, C cs, C sn, Q<C> f)
     return t;
 }
 
-// 1 - a0/|a| computed without cancellation: |vec a|^2 / (|a| (|a| + a0)).
+// 1 - a0/|a| in the compute type without cancellation: |vec a|^2 / (|a| (|a| + a0))
+// when a0 >= 0, else 1 - a0/|a| directly (no cancellation there either).
 template <class C>
-__device__ __forceinline__ double one_minus_trace(Q<C> a)
+__device__ __forceinline__ C one_minus_trace(Q<C> a)
 {
-    const double v2 = (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z;
-    const double nrm = sqrt((double)a.w * a.w + v2);
-    return v2 / (nrm * (nrm + (double)a.w));
+    const C v2 = a.x * a.x + a.y * a.y + a.z * a.z;
+    const C nrm = sqrt_(a.w * a.w + v2);
+    return (a.w >= (C)0) ? v2 / (nrm * (nrm + a.w)) : (C)1 - a.w / nrm;
 }
 
 // Neighbour references of one site, in the accessor's own reference type:
@@ -141,14 +142,15 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         SA[i] = qadd_scaled(SA[i], lap[j], Aij);
         SA[j] = qadd_scaled(SA[j], lap[i], Aji);
         if (ENERGY) {
-            // plaquette P1 = Aij U_i^dag: both orientations have the same trace
+            // plaquette P1 = Aij U_i^dag: both orientations have the same trace;
+            // 1 - cos F = 2 sin^2(F/2) (no cancellation for small F)
             const Q<C> P1 = qmul(Aij, qconj(U[i]));
-            const double omt = one_minus_trace(P1);
-            const double wF = (double)F;
-            const double omc = 2.0 * sin(0.5 * wF) * sin(0.5 * wF);
+            const double omt = (double)one_minus_trace(P1);
+            const C hF = gsin((C)0.5 * F);
+            const double omc = 2.0 * (double)(hF * hF);
             mag_e += 4.0 * P.lap[i] * P.lap[j] * (P.inv_g_sqr * omt + P.inv_gp_sqr * omc);
             plaq2 += 1.0 - omt;
-            plaq1 += cos(wF);
+            plaq1 += 1.0 - omc;
         }
     }
 #pragma unroll
@@ -223,9 +225,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             j2 += -t.w * fp.y - t.x * fp.z + t.y * fp.w + t.z * fp.x;
             j3 += t.w * fp.x - t.x * fp.w - t.y * fp.z + t.z * fp.y;
             if (ENERGY) {
-                const double e0 = (double)fp.w - t.w, e1 = (double)fp.x - t.x;
-                const double e2 = (double)fp.y - t.y, e3 = (double)fp.z - t.z;
-                grad_e += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                const C e0 = fp.w - t.w, e1 = fp.x - t.x, e2 = fp.y - t.y, e3 = fp.z - t.z;
+                grad_e += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (double)(e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
             }
         }
         J[a][0] = (C)0.25 * j0;
@@ -313,9 +314,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             out[k] = fn[k] + (keep * vel + dt2 * (dd[k] - Pot[db][k]));
             check += out[k];
             if (ENERGY) {
-                const double v = (double)vel / P.dt;
-                kin_e += 0.5 * v * v;
-                phisq += (double)fn[k] * (double)fn[k];
+                kin_e += 0.5 * P.inv_sqr_dt * (double)(vel * vel);
+                phisq += (double)(fn[k] * fn[k]);
             }
         }
         st4(ps.L.ph[db], ps.s, out[0], out[1], out[2], out[3]);
@@ -340,11 +340,10 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         const C R3 = keep * E3 + dt2 * (Mg[d][2] + gI * J[d][3]);
         if (ENERGY) {
             // 1 - (U_now U_past^dag)_0 / |U_now U_past^dag| and 1 - cos(dtheta) = 2 sin^2(dtheta/2)
-            const Q<double> Ed = {(double)Un.w * Up.w + (double)Un.x * Up.x + (double)Un.y * Up.y +
-                                      (double)Un.z * Up.z,
-                                  (double)E1, (double)E2, (double)E3};
-            const double h = sin(0.5 * (double)dth);
-            elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt * (P.inv_g_sqr * one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * h * h);
+            const Q<C> Ed = {Un.w * Up.w + Un.x * Up.x + Un.y * Up.y + Un.z * Up.z, E1, E2, E3};
+            const C h = gsin((C)0.5 * dth);
+            elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt *
+                      (P.inv_g_sqr * (double)one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * (double)(h * h));
         }
         if (R0 * R0 > (C)1) warn |= kWarnAsin;
         if (fabs(th[d]) > (C)1e4) warn |= kWarnRange;

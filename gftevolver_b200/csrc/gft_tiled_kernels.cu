@@ -254,8 +254,10 @@ __device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const Le
     }
 }
 
+// At least 512 threads per SM resident (two 8 x 32 tiles): caps registers at 128
+// per thread, which the logging-step variant would otherwise exceed.
 template <class S, int MODEL, int TY, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(TY * TZ) tiled_step_kernel(const __grid_constant__ TMaps maps,
+__global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(const __grid_constant__ TMaps maps,
                                                              const __grid_constant__ TMaps pmaps, StepParams P,
                                                              LevelPtrs<S> now, LevelPtrs<S> past, int lx,
                                                              unsigned* status, double* partials)

@@ -208,6 +208,16 @@ class Evolver:
             P, fn = ctypes.POINTER(ctypes.c_float), self.lib.gft_download_f32
         _lib.check(fn(self.h, ctypes.cast(scalars_ptr, P), ctypes.cast(vectors_ptr, P)), self.h)
 
+    def upload_device(self, scalars_ptr: int, vectors_ptr: int, f64: bool, time_iter: int = 0) -> None:
+        """Upload from reference-layout buffers already in device memory (e.g. CUDA torch tensors)."""
+        fn = self.lib.gft_upload_device_f64 if f64 else self.lib.gft_upload_device_f32
+        _lib.check(fn(self.h, ctypes.c_void_p(scalars_ptr), ctypes.c_void_p(vectors_ptr), int(time_iter)), self.h)
+
+    def download_device(self, scalars_ptr: int, vectors_ptr: int, f64: bool) -> None:
+        """Write both levels, reference layout, into device buffers (e.g. CUDA torch tensors)."""
+        fn = self.lib.gft_download_device_f64 if f64 else self.lib.gft_download_device_f32
+        _lib.check(fn(self.h, ctypes.c_void_p(scalars_ptr), ctypes.c_void_p(vectors_ptr)), self.h)
+
     def init_fields(self, ic: InitialData) -> None:
         c = _lib.GftIC()
         c.seed = int(ic.seed)
@@ -246,6 +256,16 @@ class Evolver:
         n = ctypes.c_int(0)
         ms = self.lib.gft_step_kernel_ms(self.h, ctypes.byref(n))
         return ms, n.value
+
+    @property
+    def launch_count(self) -> int:
+        """Kernels launched by evolve() on this handle so far."""
+        return int(self.lib.gft_launch_count(self.h))
+
+    @property
+    def step_kernel_name(self) -> str:
+        """The step kernel gft_evolve launches for this handle (ref / fast / tiled)."""
+        return self.lib.gft_step_kernel_name(self.h).decode()
 
     @property
     def stream(self) -> int:

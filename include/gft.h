@@ -123,6 +123,14 @@ int gft_upload_f64(gft_handle* h, const double* scalars, const double* vectors, 
 int gft_download_f32(gft_handle* h, float* scalars, float* vectors);
 int gft_download_f64(gft_handle* h, double* scalars, double* vectors);
 
+/* The same transfers with the reference-layout buffers in device memory of the
+ * handle's device (no host copy, no staging buffer): for callers that keep the
+ * fields on the GPU.  Synchronous with respect to the handle's stream. */
+int gft_upload_device_f32(gft_handle* h, const float* d_scalars, const float* d_vectors, int time_iter);
+int gft_upload_device_f64(gft_handle* h, const double* d_scalars, const double* d_vectors, int time_iter);
+int gft_download_device_f32(gft_handle* h, float* d_scalars, float* d_vectors);
+int gft_download_device_f64(gft_handle* h, double* d_scalars, double* d_vectors);
+
 /* Generate initial data on the device (InitialCondition::setInitialFields,
  * InitialConditions/Header/InitialCondition.hpp:24). */
 int gft_init_fields(gft_handle* h, const gft_ic* ic);
@@ -147,6 +155,15 @@ size_t gft_device_bytes(const gft_handle* h);
 /* Average duration in milliseconds of the step kernel over the launches since
  * the last call (CUDA events on the handle's stream); 0 if none. */
 double gft_step_kernel_ms(gft_handle* h, int* launches);
+
+/* Name of the step kernel gft_evolve launches for this handle's form, lattice and
+ * gft_set_kernel choice ("ref_step_kernel", "fast_step_kernel" or
+ * "tiled_step_kernel"; no reference counterpart). */
+const char* gft_step_kernel_name(const gft_handle* h);
+
+/* Number of kernels gft_evolve has launched on this handle so far (step
+ * kernels, analyser reductions); a diagnostic with no reference counterpart. */
+long long gft_launch_count(const gft_handle* h);
 
 /* Allocation-free observables (no counterpart in the reference).  For callers
  * that cannot allocate device memory where they need the numbers -- a fixed

@@ -195,3 +195,42 @@ def test_observe_does_not_advance(oracle_mod):
     o_sc, o_ve = sc.copy(), ve.copy()
     oracle_mod.evolve(op, o_sc, o_ve, 1)
     assert rel_err(a_sc, o_sc) <= 1e-12
+
+
+@pytest.mark.parametrize("form", ["mixed", "fp64"])
+def test_device_buffer_transfers_match_host_transfers(oracle_mod, form):
+    """gft_upload_device_* / gft_download_device_* move the same reference-layout words as the host calls."""
+    import torch
+    from gftevolver_b200 import Evolver
+    op = oracle_mod.Params(nx=8, ny=6, nz=32, energy_every=2, gauss_every=2)
+    ic = oracle_mod.ICSpec(seed=12, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    dtype = np.float64 if form == "fp64" else np.float32
+    sc, ve = oracle_mod.init_fields(op, ic, dtype)
+    f64 = form == "fp64"
+    d_sc = torch.from_numpy(sc).cuda()
+    d_ve = torch.from_numpy(ve).cuda()
+    with Evolver(_lp(op.__dict__), form=form) as a, Evolver(_lp(op.__dict__), form=form) as b:
+        a.upload(sc, ve, 0)
+        b.upload_device(d_sc.data_ptr(), d_ve.data_ptr(), f64, 0)
+        ra, rb = a.evolve(3), b.evolve(3)
+        h_sc, h_ve = a.download()
+        o_sc, o_ve = torch.empty_like(d_sc), torch.empty_like(d_ve)
+        b.download_device(o_sc.data_ptr(), o_ve.data_ptr(), f64)
+    assert np.array_equal(h_sc, o_sc.cpu().numpy()) and np.array_equal(h_ve, o_ve.cpu().numpy())
+    assert [r["energy"] for r in ra] == [r["energy"] for r in rb]
+
+
+def test_step_kernel_name_follows_form_and_shape(oracle_mod):
+    from gftevolver_b200 import Evolver
+    op = oracle_mod.Params(nx=8, ny=8, nz=32)
+    with Evolver(_lp(op.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "tiled_step_kernel"
+        ev.set_kernel(1, 0, 32)
+        assert ev.step_kernel_name == "fast_step_kernel"
+    with Evolver(_lp(op.__dict__), form="fp64") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
+    with Evolver(_lp(op.__dict__), form="ref32") as ev:
+        assert ev.step_kernel_name == "ref_step_kernel"
+    odd = oracle_mod.Params(nx=5, ny=3, nz=7)
+    with Evolver(_lp(odd.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
