@@ -104,6 +104,24 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "gft_last_error": (ctypes.c_char_p, [_H]),
     "gft_version": (ctypes.c_char_p, []),
+    # ensembles
+    "gft_batch_create": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_int, ctypes.POINTER(_H)]),
+    "gft_batch_destroy": (None, [_H]),
+    "gft_batch_size": (ctypes.c_int, [_H]),
+    "gft_batch_init_fields": (ctypes.c_int, [_H, ctypes.POINTER(GftIC)]),
+    "gft_batch_upload_f32": (ctypes.c_int, [_H, ctypes.c_int, _FP, _FP, ctypes.c_int]),
+    "gft_batch_download_f32": (ctypes.c_int, [_H, ctypes.c_int, _FP, _FP]),
+    "gft_batch_evolve": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(GftObservables), ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int)]),
+    "gft_batch_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gft_batch_autotune": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "gft_batch_last_ms": (ctypes.c_double, [_H]),
+    "gft_batch_launch_count": (ctypes.c_longlong, [_H]),
+    "gft_batch_time_iter": (ctypes.c_int, [_H]),
+    "gft_batch_stream": (ctypes.c_void_p, [_H]),
+    "gft_batch_device_bytes": (ctypes.c_size_t, [_H]),
+    "gft_batch_last_error": (ctypes.c_char_p, [_H]),
 }
 
 _lock = threading.Lock()
@@ -145,4 +163,12 @@ def check(rc: int, h=None) -> int:
     """Raise on errors (< 0); return the warning bitmask (>= 0)."""
     if rc < 0:
         raise GftError(rc, last_error(h))
+    return rc
+
+
+def check_batch(rc: int, b) -> int:
+    """check() for gft_batch_* calls (their messages live on the batch)."""
+    if rc < 0:
+        msg = load().gft_batch_last_error(b) if b else None
+        raise GftError(rc, (msg.decode() if msg else "") or last_error(None))
     return rc

@@ -29,6 +29,7 @@ SOURCES = [
     ("gft_tiled_kernels.cu", []),
     ("gft_aux_kernels.cu", []),
     ("gft_static_observe.cu", []),
+    ("gft_ensemble.cu", []),
     ("gft_abi.cu", []),
 ]
 

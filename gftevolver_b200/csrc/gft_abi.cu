@@ -93,15 +93,15 @@ bool is_f64_storage(const gft_handle* h) { return h->sbytes == 8; }
 // storage, the couplings and the damping factor take the values the shipped
 // reference sees: getSqrCouplings returns float (WilsonLoops/Source/StandardModel.cpp:224-230)
 // and currentDamping is a float member (Core/Header/Model.hpp:38-40).
-StepParams make_params(const gft_handle* h, int time_iter, bool energy)
+}  // namespace
+
+StepParams gft::config_params(const gft_config& c, int nsite, bool f32ref, int time_iter, bool energy)
 {
-    const gft_config& c = h->cfg;
-    const bool f32ref = (c.form == GFT_FORM_REF) && h->sbytes == 4;
     StepParams P{};
     P.nx = c.nx;
     P.ny = c.ny;
     P.nz = c.nz;
-    P.nsite = h->nsite;
+    P.nsite = nsite;
     P.dt = c.dt;
     P.dt2 = c.dt * c.dt;
     const double sp[3] = {c.dx, c.dy, c.dz};
@@ -141,6 +141,25 @@ StepParams make_params(const gft_handle* h, int time_iter, bool energy)
     P.store_energy = energy ? 1 : 0;
     return P;
 }
+
+void gft::row_scales(const gft_config& c, int nsite, double* scale)
+{
+    const double dv = c.dx * c.dy * c.dz;
+    for (int k = 0; k < kRowSlots; k++) scale[k] = 1.0;
+    for (int k = kObsEnergy; k <= kObsElectric; k++) scale[k] = dv;
+    scale[kObsPlaqSU2] = 1.0 / (3.0 * nsite);
+    scale[kObsPlaqU1] = 1.0 / (3.0 * nsite);
+    scale[kObsPhiSq] = 1.0 / (double)nsite;
+    for (int k = 0; k < 4; k++) scale[kObsCount + k] = dv;
+}
+
+namespace {
+
+StepParams make_params(const gft_handle* h, int time_iter, bool energy)
+{
+    return config_params(h->cfg, h->nsite, (h->cfg.form == GFT_FORM_REF) && h->sbytes == 4, time_iter, energy);
+}
+
 
 // Every array of a level starts on a 64-word boundary (256 B for float,
 // 512 B for double) so that the 16-byte vector accesses of q[] and ph[] are
@@ -350,13 +369,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap) +
                     kFinMidCapacity * sizeof(double);
     double scale[kRowSlots];
-    const double dv = cfg->dx * cfg->dy * cfg->dz;
-    for (int k = 0; k < kRowSlots; k++) scale[k] = 1.0;
-    for (int k = kObsEnergy; k <= kObsElectric; k++) scale[k] = dv;
-    scale[kObsPlaqSU2] = 1.0 / (3.0 * h->nsite);
-    scale[kObsPlaqU1] = 1.0 / (3.0 * h->nsite);
-    scale[kObsPhiSq] = 1.0 / (double)h->nsite;
-    for (int k = 0; k < 4; k++) scale[kObsCount + k] = dv;
+    row_scales(*cfg, h->nsite, scale);
     cudaMemcpy(h->d_scale, scale, sizeof(scale), cudaMemcpyHostToDevice);
     cudaMemset(h->d_status, 0, sizeof(unsigned));
     h->ev.resize(2 * (size_t)kMaxProfiled);
@@ -594,6 +607,15 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
 }
 
 }  // namespace
+
+int gft::validate_config(const gft_config* c, std::string& why) { return validate(c, why); }
+void gft::fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v)
+{
+    fill_row(r, time_iter, e, g, v);
+}
+size_t gft::level_bytes_f32(int nsite, int nsc) { return level_words(nsite, nsc) * sizeof(float); }
+void gft::carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L) { carve<float>(mem, nsite, nsc, L); }
+void gft::set_error(const std::string& msg) { set_global_error(msg); }
 
 extern "C" {
 

@@ -3,6 +3,7 @@
 
 #include "gft_device.cuh"
 #include "gft_launch.h"
+#include "gft_reduce.cuh"
 #include "gft_math.cuh"
 
 namespace gft {
@@ -115,87 +116,21 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
     }
 }
 
-// Reduces the per-block partials [nblocks][nslots] of a logging step: each
-// thread accumulates whole rows (coalesced), slot k with Neumaier compensation
-// (k < max_from) or as a maximum (k >= max_from); then the per-thread results
-// are combined by a fixed shuffle tree and thread order.  The order is fixed,
-// so the result is deterministic.  With a grid of G > 1 blocks, block g reduces
-// rows [g * rows_per_cta, (g + 1) * rows_per_cta) and writes one unscaled row
-// out[g][nslots] (stage one of two); with G = 1 it reduces all rows and writes
-// out[k] = total * scale[k].
-constexpr int kFinThreads = 1024;
-constexpr int kMaxSlots = 16;
+// Reduces the per-block partials [nblocks][nslots] of a logging step (the
+// block reduction is reduce_rows_block, gft_reduce.cuh).  With a grid of G > 1
+// blocks, block g reduces rows [g * rows_per_cta, (g + 1) * rows_per_cta) and
+// writes one unscaled row out[g][nslots] (stage one of two); with G = 1 it
+// reduces all rows and writes out[k] = total * scale[k].
 constexpr int kFinMidRows = 512;  // most stage-one rows (the caller's mid buffer holds kFinMidRows x kMaxSlots)
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const double* __restrict__ partials, int nblocks,
                                                                int nslots, int max_from, const double* scale,
                                                                double* out, int rows_per_cta)
 {
-    __shared__ double s_sum[kMaxSlots][kFinThreads / 32];
-    __shared__ double s_cmp[kMaxSlots][kFinThreads / 32];
-    double sum[kMaxSlots], comp[kMaxSlots];
-#pragma unroll
-    for (int k = 0; k < kMaxSlots; k++) {
-        sum[k] = 0.0;
-        comp[k] = 0.0;
-    }
     const int b0 = (int)blockIdx.x * rows_per_cta;
     const int b1 = min(nblocks, b0 + rows_per_cta);
-    for (int b = b0 + (int)threadIdx.x; b < b1; b += blockDim.x) {
-        const double* row = partials + (size_t)b * nslots;
-#pragma unroll
-        for (int k = 0; k < kMaxSlots; k++) {
-            if (k >= nslots) break;
-            const double v = row[k];
-            if (k >= max_from) {
-                sum[k] = fmax(sum[k], v);
-            } else {
-                const double t = sum[k] + v;
-                comp[k] += (fabs(sum[k]) >= fabs(v)) ? (sum[k] - t) + v : (v - t) + sum[k];
-                sum[k] = t;
-            }
-        }
-    }
-    // warp level: fold compensation in, then a fixed shuffle tree
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < kMaxSlots; k++) {
-        if (k >= nslots) break;
-        double v = (k >= max_from) ? sum[k] : sum[k] + comp[k];
-        double c = 0.0;
-        for (int o = 16; o > 0; o >>= 1) {
-            // xor partners compute identical sums (addition is commutative)
-            const double w = __shfl_xor_sync(0xffffffffu, v, o);
-            const double cw = __shfl_xor_sync(0xffffffffu, c, o);
-            if (k >= max_from) {
-                v = fmax(v, w);
-            } else {
-                const double t = v + w;
-                c = c + cw + ((fabs(v) >= fabs(w)) ? (v - t) + w : (w - t) + v);
-                v = t;
-            }
-        }
-        if (lane == 0) {
-            s_sum[k][warp] = v;
-            s_cmp[k][warp] = c;
-        }
-    }
-    __syncthreads();
+    const double total = reduce_rows_block(partials, b0, b1, nslots, max_from);
     if (threadIdx.x < (unsigned)nslots) {
         const int k = threadIdx.x;
-        const bool is_max = k >= max_from;
-        double tsum = 0.0, tcomp = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-            const double v = s_sum[k][w];
-            if (is_max) {
-                tsum = fmax(tsum, v);
-            } else {
-                const double u = tsum + v;
-                tcomp += (fabs(tsum) >= fabs(v)) ? (tsum - u) + v : (v - u) + tsum;
-                tsum = u;
-                tcomp += s_cmp[k][w];
-            }
-        }
-        const double total = is_max ? tsum : tsum + tcomp;
         if (gridDim.x > 1)
             out[(size_t)blockIdx.x * nslots + k] = total;
         else

@@ -78,13 +78,11 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
     if (warn) atomicOr(status, warn);
 }
 
-// Gauss-law residual after a step, FP64 for both forms (GaugeCondition.cpp:117-165 semantics);
-// sin is the library's double series (gft_math.cuh).
+// Gauss-law residual after a step (gauss_site in gft_step_body.cuh).
 template <class S, int MODEL>
 __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                          double* partials)
 {
-    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.z;
@@ -93,38 +91,7 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
     if (z < P.nz && y < P.ny) {
         const Offs o = offsets(P, x, y, z);
-        const int c = o.c;
-        double el[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const int md = c + o.m[d];
-            const double la = ld1<double>(fut.th[d], c) - ld1<double>(now.th[d], c);
-            const double na = ld1<double>(fut.th[d], md) - ld1<double>(now.th[d], md);
-            el[0] += (gsin(la) - gsin(na)) * P.lap[d];
-            // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
-            double a1, a2, a3, b1, b2, b3;
-            qmul_vec(qconj(ld4<double>(now.q[d], c)), ld4<double>(fut.q[d], c), a1, a2, a3);
-            qmul_vec(ld4<double>(fut.q[d], md), qconj(ld4<double>(now.q[d], md)), b1, b2, b3);
-            el[1] += (a1 - b1) * P.lap[d];
-            el[2] += (a2 - b2) * P.lap[d];
-            el[3] += (a3 - b3) * P.lap[d];
-        }
-        double gr[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int db = 0; db < ND; db++) {
-            const Q<double> p = ld4<double>(now.ph[db], c);
-            const Q<double> q = ld4<double>(fut.ph[db], c);
-            gr[0] += 0.25 * (p.w * q.x - p.x * q.w + p.y * q.z - p.z * q.y);
-            gr[1] += 0.25 * (p.w * q.z - p.x * q.y + p.y * q.x - p.z * q.w);
-            gr[2] += 0.25 * (-p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x);
-            gr[3] += 0.25 * (p.w * q.x - p.x * q.w - p.y * q.z + p.z * q.y);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const double av = fabs(el[k] - P.gsq[k] * gr[k]);
-            v[k] = av;
-            v[4 + k] = av;
-        }
+        gauss_site<S, MODEL>(P, now, fut, o.c, o.c + o.m[0], o.c + o.m[1], o.c + o.m[2], v);
     }
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_reduce_store<kGaussSlots>(v, partials + (size_t)blk * kGaussSlots, 4);

@@ -5,6 +5,7 @@
 #include <string>
 #include <cuda_runtime.h>
 
+#include "gft.h"
 #include "gft_device.cuh"
 
 namespace gft {
@@ -47,11 +48,13 @@ template <class S, int MODEL>
 cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
                               bool energy, cudaStream_t stream);
-constexpr int kTiledVariants = 3;  // 8x32, 4x32, 4x16 (TY x TZ)
+constexpr int kTiledVariants = 4;  // 8x32, 4x32, 4x16 (TY x TZ)
 inline void tiled_tile(int variant, int& ty, int& tz)
 {
-    ty = (variant == 0) ? 8 : 4;
-    tz = (variant == 2) ? 16 : 32;
+    static const int shapes[4][2] = {{8, 32}, {4, 32}, {4, 16}, {16, 16}};
+    const int v = (variant >= 0 && variant < 4) ? variant : 0;
+    ty = shapes[v][0];
+    tz = shapes[v][1];
 }
 
 // Auxiliary kernels (gft_aux_kernels.cu).
@@ -82,6 +85,20 @@ constexpr int kFinMidCapacity = 512 * 16;
 
 // Record the library-wide last error message (gft_last_error(NULL)).
 void set_last_error(const std::string& msg);
+void set_error(const std::string& msg);
+
+// Shared by the single-lattice handle (gft_abi.cu) and the ensemble (gft_ensemble.cu).
+// Launch parameters of one step for a configuration (f32ref: the reference-
+// arithmetic form with float storage, whose couplings are rounded to float).
+StepParams config_params(const gft_config& c, int nsite, bool f32ref, int time_iter, bool energy);
+// Per-slot scale of an observables row: energies and Gauss integrals x dV, means / N.
+void row_scales(const gft_config& c, int nsite, double* scale);
+int validate_config(const gft_config* c, std::string& why);
+void fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v);
+// One time level of float storage: bytes, and the array pointers within it.
+size_t level_bytes_f32(int nsite, int nsc);
+void carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L);
+constexpr int kRowSlotCount = kObsCount + kGaussSlots;
 
 // Elementary-function self-test (gft_math.cuh vs CUDA's functions) on the current device.
 cudaError_t run_math_selftest(int n, double* out8);

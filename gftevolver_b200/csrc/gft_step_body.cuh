@@ -386,4 +386,47 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     }
 }
 
+// Gauss-law residual at site c after a step (Analysers/Source/GaugeCondition.cpp:117-165,
+// Core/Source/Model.cpp:323-337 semantics), in FP64 for every form; md[a] is
+// the site x - e_a.  v[k] = v[4 + k] = |violation of constraint k| (the
+// integrated and the maximum slot of the analyser).  sin is the library's
+// double series.
+template <class S, int MODEL>
+__device__ __forceinline__ void gauss_site(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut,
+                                           int c, int md0, int md1, int md2, double (&v)[kGaussSlots])
+{
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    const int md[3] = {md0, md1, md2};
+    double el[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double la = ld1<double>(fut.th[d], c) - ld1<double>(now.th[d], c);
+        const double na = ld1<double>(fut.th[d], md[d]) - ld1<double>(now.th[d], md[d]);
+        el[0] += (gsin(la) - gsin(na)) * P.lap[d];
+        // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
+        double a1, a2, a3, b1, b2, b3;
+        qmul_vec(qconj(ld4<double>(now.q[d], c)), ld4<double>(fut.q[d], c), a1, a2, a3);
+        qmul_vec(ld4<double>(fut.q[d], md[d]), qconj(ld4<double>(now.q[d], md[d])), b1, b2, b3);
+        el[1] += (a1 - b1) * P.lap[d];
+        el[2] += (a2 - b2) * P.lap[d];
+        el[3] += (a3 - b3) * P.lap[d];
+    }
+    double gr[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int db = 0; db < ND; db++) {
+        const Q<double> p = ld4<double>(now.ph[db], c);
+        const Q<double> q = ld4<double>(fut.ph[db], c);
+        gr[0] += 0.25 * (p.w * q.x - p.x * q.w + p.y * q.z - p.z * q.y);
+        gr[1] += 0.25 * (p.w * q.z - p.x * q.y + p.y * q.x - p.z * q.w);
+        gr[2] += 0.25 * (-p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x);
+        gr[3] += 0.25 * (p.w * q.x - p.x * q.w - p.y * q.z + p.z * q.y);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double av = fabs(el[k] - P.gsq[k] * gr[k]);
+        v[k] = av;
+        v[4 + k] = av;
+    }
+}
+
 }  // namespace gft

@@ -1,258 +1,17 @@
-// gft_tiled_kernels.cu -- the throughput step kernel with TMA-staged planes.
-//
-// Each CTA owns a (TY x TZ) tile of (y, z) columns and marches along x (the
-// slowest-varying axis) over a chunk of LX planes.  The "now" level of every
-// plane the stencil touches is brought into shared memory once, by the Tensor
-// Memory Accelerator: one cp.async.bulk.tensor per field array per plane, a
-// (TY+2) x (TZ+2) box including the one-site halo, completing on an mbarrier.
-// Four plane buffers form a ring: while plane x is computed from planes x-1, x
-// and x+1, the copy of plane x+2 is in flight.  Halo cells that wrap around
-// the periodic boundary (tiles on the lattice faces) are outside the tensor
-// and arrive zero-filled; the CTA overwrites them with plain loads of the
-// wrapped sites.  The own-site past level is read and written directly
-// (coalesced: consecutive threads are consecutive z).
-//
-// The per-site arithmetic is gft_step_body.cuh, identical to the global-memory
-// kernel; only the accessor differs.
-//
-// Bounded waits: every mbarrier wait gives up after 2 s of %globaltimer,
-// records kErrTimeout in the status word and ends the CTA.
+// gft_tiled_kernels.cu -- the throughput step kernel with TMA-staged planes:
+// one CTA per tile of (y, z) columns and x-chunk, the per-tile pipeline of
+// gft_tiled_tile.cuh.  Host side: tensor-map encoding and launch.
 #include <cuda.h>
 
 #include "gft_device.cuh"
 #include "gft_launch.h"
-#include "gft_step_body.cuh"
+#include "gft_tiled_tile.cuh"
 
 namespace gft {
 
 namespace {
 
-constexpr unsigned kErrTimeout = 8u;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long globaltimer_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Wait for phase `parity` of `bar`; false after 2 s.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (;;) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer_ns() - t0 > 2000000000ull) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
-                                            unsigned long long* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
-                                            unsigned long long* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_prefetch_l2_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3)
-{
-    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(c0),
-                 "r"(c1), "r"(c2), "r"(c3)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap* map, int c0, int c1, int c2)
-{
-    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(c0), "r"(c1),
-                 "r"(c2)
-                 : "memory");
-}
-
-// Warm L2 with the own-site past-level tile of plane X (boxes without halo).
-template <int ND>
-__device__ __forceinline__ void prefetch_past(const TMaps& pm, int X, int y0, int z0)
-{
-#pragma unroll
-    for (int d = 0; d < 3; d++) tma_prefetch_l2_4d(&pm.q[d], 0, z0, y0, X);
-#pragma unroll
-    for (int d = 0; d < 3; d++) tma_prefetch_l2_3d(&pm.th[d], z0, y0, X);
-#pragma unroll
-    for (int k = 0; k < ND; k++) tma_prefetch_l2_4d(&pm.ph[k], 0, z0, y0, X);
-}
-
-// Shared-memory plane geometry.
-template <class S, int TY, int TZ, int ND>
-struct Geom {
-    static constexpr int TP = 16 / (int)sizeof(S);  // theta box starts TP columns left (16-byte aligned)
-    static constexpr int ROWS = TY + 2;
-    static constexpr int QP = TZ + 2;           // pitch of q / phi tiles (records of 4 S)
-    static constexpr int HP = TZ + 2 * TP;      // pitch of theta tiles
-    static constexpr int QBOX = ROWS * QP * 4 * (int)sizeof(S);
-    static constexpr int HBOX = ROWS * HP * (int)sizeof(S);
-    static constexpr int QB = (QBOX + 127) / 128 * 128;
-    static constexpr int HB = (HBOX + 127) / 128 * 128;
-    static constexpr int OFF_TH = 3 * QB;
-    static constexpr int OFF_PH = 3 * QB + 3 * HB;
-    static constexpr int BUF = 3 * QB + 3 * HB + ND * QB;
-    static constexpr int NBUF = 4;
-    static constexpr unsigned TX = 3 * QBOX + 3 * HBOX + ND * QBOX;  // bytes per plane copy
-    static constexpr int SMEM = NBUF * BUF + 128 + 64;             // + alignment slack + barriers
-};
-
-// Reference to a site in a staged plane: buffer base, q/phi cell, theta cell.
-struct TRef {
-    const unsigned char* b;
-    int cq, ch;
-};
-
-template <class S, int TY, int TZ, int ND>
-struct TileAcc {
-    using G = Geom<S, TY, TZ, ND>;
-    __device__ __forceinline__ Q<S> q(int d, TRef r) const { return lds4(r.b + d * G::QB, r.cq); }
-    __device__ __forceinline__ S th(int d, TRef r) const
-    {
-        return reinterpret_cast<const S*>(r.b + G::OFF_TH + d * G::HB)[r.ch];
-    }
-    __device__ __forceinline__ Q<S> ph(int k, TRef r) const { return lds4(r.b + G::OFF_PH + k * G::QB, r.cq); }
-
-    __device__ __forceinline__ static Q<S> lds4(const unsigned char* base, int cell)
-    {
-        if constexpr (sizeof(S) == 4) {
-            const float4 v = reinterpret_cast<const float4*>(base)[cell];
-            return {(S)v.x, (S)v.y, (S)v.z, (S)v.w};
-        } else {
-            const double2* p = reinterpret_cast<const double2*>(base) + 2 * cell;
-            const double2 a = p[0], c = p[1];
-            return {(S)a.x, (S)a.y, (S)c.x, (S)c.y};
-        }
-    }
-};
-
-template <class S, int TY, int TZ, int ND>
-__device__ __forceinline__ void issue_plane(const TMaps& maps, unsigned char* buf, unsigned long long* bar, int X,
-                                            int y0, int z0)
-{
-    using G = Geom<S, TY, TZ, ND>;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(bar, G::TX);
-#pragma unroll
-    for (int d = 0; d < 3; d++) tma_load_4d(buf + d * G::QB, &maps.q[d], 0, z0 - 1, y0 - 1, X, bar);
-#pragma unroll
-    for (int d = 0; d < 3; d++) tma_load_3d(buf + G::OFF_TH + d * G::HB, &maps.th[d], z0 - G::TP, y0 - 1, X, bar);
-#pragma unroll
-    for (int k = 0; k < ND; k++) tma_load_4d(buf + G::OFF_PH + k * G::QB, &maps.ph[k], 0, z0 - 1, y0 - 1, X, bar);
-}
-
-// Halo cell handled by thread `tid` (2*QP + 2*TY cells: rows 0 and TY+1, then
-// columns 0 and TZ+1); false if tid has none.
-template <int TY, int QP>
-__device__ __forceinline__ bool halo_cell(int tid, int& ly, int& lz)
-{
-    if (tid >= 2 * QP + 2 * TY) return false;
-    if (tid < QP) {
-        ly = 0;
-        lz = tid;
-    } else if (tid < 2 * QP) {
-        ly = TY + 1;
-        lz = tid - QP;
-    } else if (tid < 2 * QP + TY) {
-        ly = 1 + (tid - 2 * QP);
-        lz = 0;
-    } else {
-        ly = 1 + (tid - 2 * QP - TY);
-        lz = QP - 1;
-    }
-    return true;
-}
-
-// Warm L2 with the wrapped halo sites of plane X (one plane before they are
-// patched), so the patch loads do not wait on DRAM.
-template <class S, int TY, int TZ, int ND>
-__device__ __forceinline__ void prefetch_wrapped_halo(const StepParams& P, const LevelPtrs<S>& now, int X, int y0,
-                                                      int z0, int tid)
-{
-    using G = Geom<S, TY, TZ, ND>;
-    int ly, lz;
-    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
-    int y = y0 - 1 + ly, z = z0 - 1 + lz;
-    if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;
-    y = (y < 0) ? y + P.ny : (y >= P.ny ? y - P.ny : y);
-    z = (z < 0) ? z + P.nz : (z >= P.nz ? z - P.nz : z);
-    const size_t s = ((size_t)X * P.ny + y) * P.nz + z;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(now.q[d] + 4 * s));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(now.th[d] + s));
-    }
-#pragma unroll
-    for (int k = 0; k < ND; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(now.ph[k] + 4 * s));
-}
-
-// Halo cells of plane X whose (y, z) leaves the lattice: load the wrapped
-// site from global memory into the staged plane.
-template <class S, int TY, int TZ, int ND>
-__device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const LevelPtrs<S>& now, unsigned char* buf,
-                                                   int X, int y0, int z0, int tid)
-{
-    using G = Geom<S, TY, TZ, ND>;
-    int ly, lz;
-    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
-    int y = y0 - 1 + ly, z = z0 - 1 + lz;
-    if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;  // delivered by the tensor copy
-    y = (y < 0) ? y + P.ny : (y >= P.ny ? y - P.ny : y);
-    z = (z < 0) ? z + P.nz : (z >= P.nz ? z - P.nz : z);
-    const int s = (X * P.ny + y) * P.nz + z;
-    const int cq = ly * G::QP + lz, ch = ly * G::HP + lz + G::TP - 1;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        const Q<S> v = ld4<S>(now.q[d], s);
-        st4(reinterpret_cast<S*>(buf + d * G::QB), cq, v.w, v.x, v.y, v.z);
-        reinterpret_cast<S*>(buf + G::OFF_TH + d * G::HB)[ch] = ld1<S>(now.th[d], s);
-    }
-#pragma unroll
-    for (int k = 0; k < ND; k++) {
-        const Q<S> v = ld4<S>(now.ph[k], s);
-        st4(reinterpret_cast<S*>(buf + G::OFF_PH + k * G::QB), cq, v.w, v.x, v.y, v.z);
-    }
-}
+using namespace tiled;
 
 // At least 512 threads per SM resident (two 8 x 32 tiles): caps registers at 128
 // per thread, which the logging-step variant would otherwise exceed.
@@ -268,18 +27,7 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::NBUF * G::BUF);
-
-    const int tz = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * TZ + tz;
-    const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
-    const int x0 = blockIdx.z * lx;
-    const int nloc = min(lx, P.nx - x0);
-    const int nplanes = nloc + 2;  // planes x0-1 .. x0+nloc
-    const bool wraps = (y0 == 0) || (y0 + TY == P.ny) || (z0 == 0) || (z0 + TZ == P.nz);
-    auto plane_x = [&](int p) {  // global x of relative plane p (p = 0 is x0 - 1)
-        int X = x0 - 1 + p;
-        return (X < 0) ? X + P.nx : (X >= P.nx ? X - P.nx : X);
-    };
+    const int tid = threadIdx.y * TZ + threadIdx.x;
 
     __shared__ int s_abort;
     if (tid == 0) {
@@ -288,68 +36,16 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0) {
-        for (int p = 0; p < min(G::NBUF, nplanes); p++)
-            issue_plane<S, TY, TZ, ND>(maps, smem + p * G::BUF, &bars[p], plane_x(p), y0, z0);
-    }
-    if (tid == 32 % (TY * TZ)) {
-        // past level of the first two planes computed (relative planes 1 and 2)
-        for (int p = 1; p <= 2 && p <= nloc; p++) prefetch_past<ND>(pmaps, plane_x(p), y0, z0);
-    }
 
     double obs[kObsCount];
 #pragma unroll
     for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
     unsigned warn = 0;
-
-    // own cells
-    const int cq0 = (ty + 1) * G::QP + (tz + 1);
-    const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
-    const int y = y0 + ty, z = z0 + tz;
-    XCarry<S, ND> carry;
-    carry.valid = false;
-
-    for (int i = 0; i < nloc; i++) {
-        // planes i (x-1), i+1 (x), i+2 (x+1) must be resident; i+2 is new except at i = 0
-        bool ok = true;
-        for (int p = (i == 0 ? 0 : i + 2); p <= i + 2; p++) {
-            ok = ok && mbar_wait_bounded(&bars[p % G::NBUF], (unsigned)((p / G::NBUF) & 1));
-            if (ok && wraps) patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + (p % G::NBUF) * G::BUF, plane_x(p), y0, z0, tid);
-        }
-        if (!ok) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
-
-        const unsigned char* bm = smem + (i % G::NBUF) * G::BUF;
-        const unsigned char* bc = smem + ((i + 1) % G::NBUF) * G::BUF;
-        const unsigned char* bp = smem + ((i + 2) % G::NBUF) * G::BUF;
-        Stencil<TRef> n;
-        n.c = {bc, cq0, ch0};
-        n.m[0] = {bm, cq0, ch0};
-        n.p[0] = {bp, cq0, ch0};
-        n.m[1] = {bc, cq0 - G::QP, ch0 - G::HP};
-        n.p[1] = {bc, cq0 + G::QP, ch0 + G::HP};
-        n.m[2] = {bc, cq0 - 1, ch0 - 1};
-        n.p[2] = {bc, cq0 + 1, ch0 + 1};
-        n.d01 = {bp, cq0 - G::QP, ch0 - G::HP};
-        n.d02 = {bp, cq0 - 1, ch0 - 1};
-        n.d10 = {bm, cq0 + G::QP, ch0 + G::HP};
-        n.d12 = {bc, cq0 + G::QP - 1, ch0 + G::HP - 1};
-        n.d20 = {bm, cq0 + 1, ch0 + 1};
-        n.d21 = {bc, cq0 - G::QP + 1, ch0 - G::HP + 1};
-        const int x = x0 + i;
-        const int s = (x * P.ny + y) * P.nz + z;
-        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn);
-
-        __syncthreads();  // every thread is done with plane i's buffer
-        if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
-        // plane i+3 is waited (and patched) in the next iteration
-        if (wraps && i + 3 < nplanes) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 3), y0, z0, tid);
-        if (tid == 0 && i + G::NBUF < nplanes)
-            issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
-                                       plane_x(i + G::NBUF), y0, z0);
-    }
-    if (s_abort && tid == 0) atomicOr(status, kErrTimeout);
+    RingPhase ring = {0u};
+    const int x0 = blockIdx.z * lx;
+    const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY>(maps, pmaps, P, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0,
+                                                       min(lx, P.nx - x0), smem, bars, ring, &s_abort, obs, warn);
+    if (!ok && tid == 0) atomicOr(status, kErrTimeout);
 
     if (ENERGY) {
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
@@ -465,7 +161,8 @@ cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepP
     switch (variant) {
     case 0: return launch_tiled_t<S, MODEL, 8, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
     case 1: return launch_tiled_t<S, MODEL, 4, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
-    default: return launch_tiled_t<S, MODEL, 4, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
+    case 2: return launch_tiled_t<S, MODEL, 4, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
+    default: return launch_tiled_t<S, MODEL, 16, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
     }
 }
 

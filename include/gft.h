@@ -189,7 +189,7 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
  * divides into a built tile, else the one-thread-per-site kernel), 1 = one
  * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
  * marching along x (mixed form).  tile = tile shape (0: 8 x 32, 1: 4 x 32,
- * 2: 4 x 16 sites in y x z); march = planes per CTA along x.  Returns
+ * 2: 4 x 16, 3: 16 x 16 sites in y x z); march = planes per CTA along x.  Returns
  * GFT_E_UNSUPPORTED when the lattice does not divide into the tile. */
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
@@ -199,6 +199,44 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
  * float sincos.cos, float sin, double sincos.sin, double sincos.cos, double sin;
  * max relative error of float asin, double asin. */
 int gft_selftest_math(int device, double* out);
+
+/* ---- ensembles ---------------------------------------------------------- */
+/* Many independent lattices (realisations: own seeds, couplings and sizes) in
+ * one object, evolved together by ONE persistent kernel launch per time step
+ * (no reference counterpart: the reference runs one lattice per process,
+ * Core/Source/Lattice.cpp:755-876).  All members share the model, the device,
+ * the analysers' cadence and the step counter; the form is GFT_FORM_MIXED; the
+ * members' (ny, nz) must share a tile shape (ny % 4 == 0 and nz % 16 == 0 at
+ * least).  Each member evolves exactly as a single handle would with the same
+ * tile shape and march depth (gft_set_kernel). */
+typedef struct gft_batch gft_batch;
+
+int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out);
+void gft_batch_destroy(gft_batch* b);
+int gft_batch_size(const gft_batch* b);
+/* Device initial data, one gft_ic per member. */
+int gft_batch_init_fields(gft_batch* b, const gft_ic* ics);
+/* Member transfer in the reference layout (float); an upload sets the shared step counter. */
+int gft_batch_upload_f32(gft_batch* b, int member, const float* scalars, const float* vectors, int time_iter);
+int gft_batch_download_f32(gft_batch* b, int member, float* scalars, float* vectors);
+/* Evolve every member n_steps.  rows[m * max_rows + r] receives member m's r-th
+ * logged row; *n_rows the rows written per member.  Whole logging periods run
+ * as one CUDA graph replay. */
+int gft_batch_evolve(gft_batch* b, int n_steps, gft_observables* rows, int max_rows, int* n_rows);
+/* Tile shape (0: 8 x 32, 1: 4 x 32, 2: 4 x 16, 3: 16 x 16), planes per tile along x, and
+ * whether whole logging periods are replayed from a CUDA graph. */
+int gft_batch_set_kernel(gft_batch* b, int tile, int march, int use_graphs);
+/* Times every tile shape the members admit with march depths 8..64 for
+ * trial_steps steps each on the ensemble itself (fields and step counter are
+ * restored afterwards) and keeps the fastest; reports the choice. */
+int gft_batch_autotune(gft_batch* b, int trial_steps, int* tile, int* march);
+/* Device time in milliseconds of the last gft_batch_evolve call (CUDA events on its stream). */
+double gft_batch_last_ms(const gft_batch* b);
+long long gft_batch_launch_count(const gft_batch* b);
+int gft_batch_time_iter(const gft_batch* b);
+void* gft_batch_stream(gft_batch* b);
+size_t gft_batch_device_bytes(const gft_batch* b);
+const char* gft_batch_last_error(const gft_batch* b);
 
 /* Message for the last error on this handle (or the last global error if h is NULL). */
 const char* gft_last_error(const gft_handle* h);

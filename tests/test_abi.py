@@ -76,3 +76,25 @@ def test_create_rejects_invalid_config_without_gpu(lib):
     cfg.nx = 0
     assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
     assert not h.value
+
+
+def test_batch_create_validates_members_without_gpu(lib):
+    """Ensemble members must share model, form (mixed), device and logging cadence; checked before any device call."""
+    from gftevolver_b200 import LatticeParams, _lib
+    from gftevolver_b200.evolver import make_config
+    a = LatticeParams(nx=8, ny=4, nz=16, energy_every=2)
+    b = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, model=_lib.GFT_MODEL_2HDM)
+    h = ctypes.c_void_p()
+    cfgs = (_lib.GftConfig * 2)(make_config(a), make_config(b))
+    assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_INVALID
+    assert b"model" in lib.gft_last_error(None)
+    c = LatticeParams(nx=8, ny=4, nz=16, energy_every=3)
+    cfgs = (_lib.GftConfig * 2)(make_config(a), make_config(c))
+    assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_INVALID
+    cfgs = (_lib.GftConfig * 1)(make_config(a, "fp64"))
+    assert lib.gft_batch_create(cfgs, 1, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
+    d = LatticeParams(nx=8, ny=6, nz=16, energy_every=2)  # ny % 4 != 0: no tile shape fits
+    cfgs = (_lib.GftConfig * 2)(make_config(a), make_config(d))
+    assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
+    assert lib.gft_batch_create(cfgs, 0, ctypes.byref(h)) == _lib.GFT_E_INVALID
+    assert not h.value

@@ -49,6 +49,8 @@ def _maxdiff(a, b):
     ((9, 12, 48), 2, 4),      # 4 x 16 tiles
     ((3, 4, 16), 2, 1),       # march 1
     ((20, 16, 32), 1, 64),    # march > nx
+    ((10, 32, 48), 3, 6),     # 16 x 16 tiles
+    ((4, 16, 16), 3, 32),     # 16 x 16, one tile per plane
 ])
 def test_tiled_matches_global_kernel(oracle_mod, model, shape, tile, march):
     op, p, sc, ve = _setup(oracle_mod, model, shape)
