@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 precision run (0: skip)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
+    ap.add_argument("--slab", action="store_true",
+                    help="N = 1: run the x-slab path (ghost planes refreshed by the exchange callback) on one GPU")
     ap.add_argument("--ensemble-steps", type=int, default=500,
                     help="steps of the 64-member ensemble run (0: skip)")
     return ap.parse_args()
@@ -378,13 +380,25 @@ def main():
 
     kind = {"auto": 0, "global": 1, "tiled": 2}[args.kernel]
 
+    def make_runner(form_):
+        """N = 1: the whole lattice.  N > 1: this rank's x-slab of an (N * n) x n x n lattice
+        (ghost planes exchanged over NCCL after every step; rows combined over ranks)."""
+        if world > 1 or args.slab:
+            import dataclasses
+
+            from gftevolver_b200.slab import SlabEvolver
+            s = SlabEvolver(dataclasses.replace(p, nx=p.nx * world), form=form_, device=local)
+            return s, s.local
+        e = Evolver(p, form=form_, device=local)
+        return e, e
+
     def timed_run(form_, steps, warmup, sampler=None):
-        ev = Evolver(p, form=form_, device=local)
+        runner, ev = make_runner(form_)
         if form_ == "mixed" and (kind != 0 or args.tile != 0 or args.march != 32):
             ev.set_kernel(kind, args.tile, args.march)
-        ev.init_fields(ic)
+        runner.init_fields(ic)
         if warmup:
-            ev.evolve(warmup)
+            runner.evolve(warmup)
         ev.step_kernel_ms()  # reset
         launches0 = ev.launch_count
         stream = torch.cuda.ExternalStream(ev.stream)
@@ -395,7 +409,7 @@ def main():
         if sampler:
             sampler.start()
         e0.record(stream)
-        rows = ev.evolve(steps)
+        rows = runner.evolve(steps)
         e1.record(stream)
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
@@ -403,6 +417,7 @@ def main():
         ms = e0.elapsed_time(e1)
         kms, nk = ev.step_kernel_ms()
         ev.timed_launches = ev.launch_count - launches0
+        ev.runner = runner
         return ev, ms, kms, nk, rows, clocks
 
     sampler = ClockSampler(local)
@@ -415,7 +430,7 @@ def main():
     # FP64 plain form for the mixed-vs-FP64 ratio
     fp64 = None
     if form == "mixed" and not args.no_fp64:
-        ev.close()
+        ev.runner.close()
         fsteps = args.fp64_steps or max(args.steps // 4, 10)
         ev64, ms64, kms64, nk64, _, _ = timed_run("fp64", fsteps, min(args.warmup, 3))
         ms64 = max_over_ranks(ms64)
@@ -423,9 +438,9 @@ def main():
         fp64 = {"value": v64, "steps": fsteps, "step_kernel_ms": kms64,
                 "roofline_frac": (B_ALG[(args.model, 8)] * p.nsite / (kms64 / 1e3)) / 1e9 / measured_peaks()[0],
                 "mixed_over_fp64": value / v64}
-        ev64.close()
+        ev64.runner.close()
     else:
-        ev.close()
+        ev.runner.close()
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
@@ -433,22 +448,25 @@ def main():
         dt = torch.float32 if sbytes == 4 else torch.float64
         sc_h = torch.empty((2, p.nx, p.ny, p.nz, p.nsc), dtype=dt).pin_memory()
         ve_h = torch.empty((2, p.nx, p.ny, p.nz, 15), dtype=dt).pin_memory()
-        ev = Evolver(p, form=form, device=local)
-        ev.init_fields(ic)
+        runner, ev = make_runner(form)
+        if world > 1 or args.slab:  # the slab with its ghost planes
+            sc_h = torch.empty((2, p.nx + 2, p.ny, p.nz, p.nsc), dtype=dt).pin_memory()
+            ve_h = torch.empty((2, p.nx + 2, p.ny, p.nz, 15), dtype=dt).pin_memory()
+        runner.init_fields(ic)
         ev.download_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8)
         ev.upload_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8, 0)  # warm the staging buffer
-        ev.evolve(min(args.warmup, 3))
+        runner.evolve(min(args.warmup, 3))
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         ev.upload_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8, 0)
-        rows_e2e = ev.evolve(args.steps)
+        rows_e2e = runner.evolve(args.steps)
         ev.download_ptr(sc_h.data_ptr(), ve_h.data_ptr(), sbytes == 8)
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
         barrier()
         secs = max_over_ranks(secs)
-        ev.close()
+        runner.close()
         nbytes = (sc_h.numel() + ve_h.numel()) * sc_h.element_size()
         e2e = {"value": world * p.nsite * args.steps / secs, "unit": "site-updates/s",
                "h2d_bytes_per_step": nbytes / args.steps,
@@ -461,11 +479,12 @@ def main():
             dist.destroy_process_group()
         return
 
+    # single-GPU properties: measured at N = 1 only
     precision = None
-    if args.precision_steps > 0 and form == "mixed":
+    if args.precision_steps > 0 and form == "mixed" and world == 1:
         precision = precision_report(p, ic, args.precision_steps, local)
     ensemble = None
-    if args.ensemble_steps > 0:
+    if args.ensemble_steps > 0 and world == 1:
         ensemble = ensemble_report(args.ensemble_steps, local)
 
     peak, peak_kind = measured_peaks()
@@ -482,12 +501,16 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if sbytes == 4 else "f64", "data": "synthetic",
-        "config": {"workload": f"{args.model.upper()} {args.size}^3 periodic leapfrog, form={form}, random SU(2) "
+        "config": {"workload": (f"{args.model.upper()} {world * args.size}x{args.size}x{args.size} periodic leapfrog "
+                                f"({args.size}^3 x-slab per GPU)" if world > 1 else
+                                f"{args.model.upper()} {args.size}^3 periodic leapfrog") + f", form={form}, random SU(2) "
                                f"links eps~N(0,0.1^2), theta_Y~N(0,0.1^2), Higgs N(1,0.1^2), dt=0.05, "
                                f"energy+Gauss analysers every {LOG_EVERY} steps",
                    "lattice": [p.nx, p.ny, p.nz], "form": form, "log_every": LOG_EVERY,
                    "l2": "inputs larger than L2 (state %.2f GB per level pair)" % (2 * p.nsite * (15 + p.nsc) * sbytes / 1e9),
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "parallelism": (f"x-slabs x{world}: lattice {world * p.nx}x{p.ny}x{p.nz}, one ghost plane per "
+                                   "side exchanged over NCCL send/recv after every step, FP64 all-reduce of "
+                                   "the analyser rows") if world > 1 else "single GPU",
                    "kernel": args.kernel, "tile": args.tile, "march": args.march},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": kernel_name,

@@ -72,6 +72,9 @@ class GftIC(ctypes.Structure):
     ]
 
 
+# int (*)(gft_handle*, int level, void* user)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p)
+
 _FP = ctypes.POINTER(ctypes.c_float)
 _DP = ctypes.POINTER(ctypes.c_double)
 _H = ctypes.c_void_p
@@ -104,6 +107,10 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "gft_last_error": (ctypes.c_char_p, [_H]),
     "gft_version": (ctypes.c_char_p, []),
+    "gft_set_slab": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gft_set_exchange": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p]),
+    "gft_level_planes": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.c_size_t), ctypes.c_int]),
     # ensembles
     "gft_batch_create": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_int, ctypes.POINTER(_H)]),
     "gft_batch_destroy": (None, [_H]),

@@ -71,6 +71,12 @@ struct gft_handle {
     bool tiled_ready = false;
     TMaps tm[2];   // staged "now" planes (with halo), per level
     TMaps tp[2];   // past-level L2 prefetch boxes (no halo), per level
+    // x-slab of a larger lattice (gft_set_slab): planes [x_begin, x_end) are
+    // this handle's own, the others are ghost copies of the neighbours' planes
+    int x_begin = 0, x_end = 0;  // x_end = 0: all planes
+    int x_offset = 0, nx_global = 0;
+    gft_exchange_fn exchange = nullptr;
+    void* exchange_user = nullptr;
 
     int fail(int code, const std::string& msg)
     {
@@ -139,6 +145,8 @@ StepParams gft::config_params(const gft_config& c, int nsite, bool f32ref, int t
     P.apply_norm = c.apply_norm;
     P.energy_offset = c.energy_offset;
     P.store_energy = energy ? 1 : 0;
+    P.obs_x0 = 0;
+    P.obs_x1 = c.nx;
     return P;
 }
 
@@ -157,7 +165,12 @@ namespace {
 
 StepParams make_params(const gft_handle* h, int time_iter, bool energy)
 {
-    return config_params(h->cfg, h->nsite, (h->cfg.form == GFT_FORM_REF) && h->sbytes == 4, time_iter, energy);
+    StepParams P = config_params(h->cfg, h->nsite, (h->cfg.form == GFT_FORM_REF) && h->sbytes == 4, time_iter, energy);
+    if (h->x_end > 0) {
+        P.obs_x0 = h->x_begin;
+        P.obs_x1 = h->x_end;
+    }
+    return P;
 }
 
 
@@ -578,6 +591,14 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         double* out = h->d_rows + (size_t)row * kRowSlots;
         if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->d_mid,
                                          h->stream);
+        if (h->exchange && err == cudaSuccess) {
+            // refresh the ghost planes of the level just written before anything reads them
+            const int xr = h->exchange(h, tp, h->exchange_user);
+            if (xr != 0) {
+                h->time_iter++;
+                return h->fail(GFT_E_STATE, "gft_evolve: the exchange callback failed (" + std::to_string(xr) + ")");
+            }
+        }
         if (g && err == cudaSuccess) {
             err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
             if (err == cudaSuccess)
@@ -648,6 +669,8 @@ int gft_init_fields(gft_handle* h, const gft_ic* ic)
     p.eps_sigma = ic->eps_sigma;
     p.wall_width = ic->wall_width;
     p.wall_value = ic->wall_value;
+    p.x_offset = h->x_offset;
+    p.nx_global = h->nx_global;
     const StepParams P = make_params(h, 0, false);
     cudaError_t e = is_f64_storage(h) ? launch_init_fields<double>(P, h->nsc, p, h->ld[0], h->ld[1], h->stream)
                                       : launch_init_fields<float>(P, h->nsc, p, h->lf[0], h->lf[1], h->stream);
@@ -779,6 +802,58 @@ double gft_step_kernel_ms(gft_handle* h, int* launches)
 }
 
 long long gft_launch_count(const gft_handle* h) { return h ? h->launches : 0; }
+
+int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_end)
+{
+    if (!h) return GFT_E_INVALID;
+    const int nx = h->cfg.nx;
+    if (nx_global < 1 || x_begin < 0 || x_end > nx || x_begin >= x_end)
+        return h->fail(GFT_E_INVALID, "gft_set_slab: need 0 <= x_begin < x_end <= nx and nx_global >= 1");
+    h->x_offset = x_offset;
+    h->nx_global = nx_global;
+    h->x_begin = x_begin;
+    h->x_end = x_end;
+    // means over this handle's own sites
+    gft_config c = h->cfg;
+    c.nx = x_end - x_begin;
+    double scale[kRowSlots];
+    row_scales(c, c.nx * c.ny * c.nz, scale);
+    cudaSetDevice(h->cfg.device);
+    cudaStreamSynchronize(h->stream);
+    cudaError_t e = cudaMemcpy(h->d_scale, scale, sizeof(scale), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_set_slab");
+    return GFT_OK;
+}
+
+int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user)
+{
+    if (!h) return GFT_E_INVALID;
+    h->exchange = fn;
+    h->exchange_user = user;
+    return GFT_OK;
+}
+
+int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes, int max)
+{
+    if (!h || level < 0 || level > 1 || x < 0 || x >= h->cfg.nx || !ptrs || !bytes) return GFT_E_INVALID;
+    const int n = 7 + (h->nsc == 8 ? 1 : 0);
+    if (max < n) return h->fail(GFT_E_INVALID, "gft_level_planes: need room for " + std::to_string(n) + " arrays");
+    const size_t plane = (size_t)h->cfg.ny * h->cfg.nz;
+    const size_t w = (size_t)h->sbytes;
+    int k = 0;
+    if (h->sbytes == 4) {
+        const LevelPtrs<float>& L = h->lf[level];
+        for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.q[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+        for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.th[d] + plane * x; bytes[k] = plane * w; }
+        for (int db = 0; db < h->nsc / 4; db++, k++) { ptrs[k] = L.ph[db] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+    } else {
+        const LevelPtrs<double>& L = h->ld[level];
+        for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.q[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+        for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.th[d] + plane * x; bytes[k] = plane * w; }
+        for (int db = 0; db < h->nsc / 4; db++, k++) { ptrs[k] = L.ph[db] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+    }
+    return n;
+}
 
 const char* gft_step_kernel_name(const gft_handle* h)
 {

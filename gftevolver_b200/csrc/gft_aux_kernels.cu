@@ -81,9 +81,14 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
     if (s >= P.nsite) return;
     const double two_pi = 6.283185307179586476925286766559;
     const int zc = s % P.nz;
+    // random-number key: the site's index in the whole lattice (differs from s only on an x-slab)
+    const int plane = P.ny * P.nz;
+    const int ng = ic.nx_global > 0 ? ic.nx_global : P.nx;
+    const int xg = ((s / plane + ic.x_offset) % ng + ng) % ng;
+    const unsigned long long key = (unsigned long long)xg * plane + (unsigned long long)(s % plane);
     double f[8];
     for (int c = 0; c < nsc; c++) {
-        double v = ic.mean[c] + ic.sigma[c] * gaussian(ic.seed, (unsigned long long)c, (unsigned long long)s);
+        double v = ic.mean[c] + ic.sigma[c] * gaussian(ic.seed, (unsigned long long)c, key);
         if (c == 0 && ic.wall_width > 0.0) {
             const double zz = (double)zc;
             v += ic.wall_value * 0.5 *
@@ -96,13 +101,13 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
         st4(b.ph[db], s, (S)f[4 * db], (S)f[4 * db + 1], (S)f[4 * db + 2], (S)f[4 * db + 3]);
     }
     for (int d = 0; d < 3; d++) {
-        const double th = ic.theta_sigma * gaussian(ic.seed, 16ULL + d, (unsigned long long)s);
+        const double th = ic.theta_sigma * gaussian(ic.seed, 16ULL + d, key);
         double q0 = 1.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
         if (ic.eps_sigma > 0.0) {
-            const double eps = ic.eps_sigma * gaussian(ic.seed, 32ULL + d, (unsigned long long)s);
-            const double ct = 2.0 * uniform01(ic.seed, 48ULL + d, (unsigned long long)s) - 1.0;
+            const double eps = ic.eps_sigma * gaussian(ic.seed, 32ULL + d, key);
+            const double ct = 2.0 * uniform01(ic.seed, 48ULL + d, key) - 1.0;
             const double st = sqrt(1.0 - ct * ct);
-            const double ph = two_pi * uniform01(ic.seed, 64ULL + d, (unsigned long long)s);
+            const double ph = two_pi * uniform01(ic.seed, 64ULL + d, key);
             const double se = sin(eps);
             q0 = cos(eps);
             q1 = se * st * cos(ph);

@@ -59,7 +59,11 @@ struct StepParams {
     int break_son, break_uhalfn, apply_norm;
     double energy_offset;
     int store_energy;       // logging step: renormalise as the reference does and accumulate energies
+    int obs_x0, obs_x1;     // planes whose sites count in observables, Gauss residuals and warnings
+                            // (all planes, except on an x-slab with ghost planes)
 };
+
+__device__ __forceinline__ bool counts(const StepParams& P, int x) { return x >= P.obs_x0 && x < P.obs_x1; }
 
 // ---------------------------------------------------------------------------
 // Quaternions: U = c0 + i c.sigma, product (a0 b0 - a.b, a0 b + b0 a - a x b)

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         n.d21 = o.c + o.p[2] + o.m[1];
         XCarry<S, (MODEL == kModelSM) ? 1 : 2> carry;
         carry.valid = false;
-        site_step<S, MODEL, ENERGY>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn);
+        site_step<S, MODEL, ENERGY>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn, counts(P, x));
     }
     if (ENERGY) {
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
     double v[kGaussSlots];
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
-    if (z < P.nz && y < P.ny) {
+    if (z < P.nz && y < P.ny && counts(P, x)) {
         const Offs o = offsets(P, x, y, z);
         gauss_site<S, MODEL>(P, now, fut, o.c, o.c + o.m[0], o.c + o.m[1], o.c + o.m[2], v);
     }

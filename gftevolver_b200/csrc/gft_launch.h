@@ -67,6 +67,9 @@ struct ICParams {
     unsigned long long seed;
     double mean[8], sigma[8];
     double theta_sigma, eps_sigma, wall_width, wall_value;
+    // x-slab: local plane x draws the random numbers of global plane
+    // (x + x_offset) mod nx_global, so slabs reproduce the whole lattice's data
+    int x_offset, nx_global;
 };
 template <class S>
 cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic, LevelPtrs<S> a, LevelPtrs<S> b,

@@ -429,6 +429,11 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                      && isfinite((double)q2) && isfinite((double)q3);
         }
         if (!finite) warn |= kWarnNonFinite;
+        if (!counts(P, x)) {  // ghost plane of an x-slab: no observables, no warnings
+            warn = 0;
+#pragma unroll
+            for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
+        }
     }
 
     if (ENERGY) {
@@ -451,7 +456,7 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
     double v[kGaussSlots];
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
-    if (z < P.nz && y < P.ny) {
+    if (z < P.nz && y < P.ny && counts(P, x)) {
         const Nbr n = neighbours(P, x, y, z);
         const RefView<S> Vn{now};
         const RefView<S> Vf{fut};

@@ -92,12 +92,14 @@ struct PastSite {
 };
 
 // The per-site update.  A provides q(d, R) -> Q<C>, th(d, R) -> C, ph(k, R) -> Q<C>
-// for the "now" level.  obs receives the energy-step observables.
+// for the "now" level.  obs receives the energy-step observables and warn the
+// warning bits, both only when `count` (the site is not on a ghost plane).
 template <class S, int MODEL, bool ENERGY, class A, class R>
 __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S> ps,
                                           XCarry<S, (MODEL == kModelSM) ? 1 : 2>& carry, double (&obs)[kObsCount],
-                                          unsigned& warn)
+                                          unsigned& warn, bool count = true)
 {
+    const unsigned warn_in = warn;
     using C = S;  // FP64 form -> double, mixed form -> float
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     const bool have = carry.valid;
@@ -372,6 +374,10 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     }
     if (!isfinite(check)) warn |= kWarnNonFinite;
     carry.valid = true;
+    if (!count) {
+        warn = warn_in;
+        return;
+    }
 
     if (ENERGY) {
         obs[kObsPotential] += pot_e;

@@ -338,7 +338,8 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         n.d21 = {bc, cq0 - G::QP + 1, ch0 - G::HP + 1};
         const int x = x0 + i;
         const int s = (x * P.ny + y) * P.nz + z;
-        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn);
+        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn,
+                                    counts(P, x));
 
         __syncthreads();  // every thread is done with plane i's buffer
         if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);

@@ -165,6 +165,30 @@ const char* gft_step_kernel_name(const gft_handle* h);
  * kernels, analyser reductions); a diagnostic with no reference counterpart. */
 long long gft_launch_count(const gft_handle* h);
 
+/* ---- x-slabs of a lattice split over ranks ------------------------------ */
+/* A handle can hold one x-slab of a larger periodic lattice (no reference
+ * counterpart; the reference only notes where an MPI halo exchange would go,
+ * Core/Source/Lattice.cpp:779).
+ * Its lattice is the slab plus one ghost plane on each side (nx = own planes +
+ * 2); the kernels run unchanged on it and the ghost planes' own updates are
+ * discarded: observables, Gauss residuals and warnings count only planes
+ * [x_begin, x_end), and the device initial data of local plane x is that of
+ * global plane (x + x_offset) mod nx_global.  Means in the rows are over the
+ * slab's own sites (a caller combines ranks by site-weighted sums). */
+int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_end);
+
+/* Called by gft_evolve after each step's kernels are enqueued on the handle's
+ * stream and before anything reads the level just written (`level`): the
+ * caller refreshes that level's ghost planes (e.g. NCCL send/recv of the
+ * boundary planes, ordered on gft_stream(h)).  Nonzero return aborts gft_evolve. */
+typedef int (*gft_exchange_fn)(gft_handle* h, int level, void* user);
+int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user);
+
+/* Device addresses and byte sizes of plane x of every field array of a level
+ * (3 quaternion arrays, 3 phase arrays, 1 or 2 doublet arrays, in that order);
+ * returns the number of arrays (7 or 8). */
+int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes, int max);
+
 /* Allocation-free observables (no counterpart in the reference).  For callers
  * that cannot allocate device memory where they need the numbers -- a fixed
  * memory budget, a region that must stay asynchronous (cudaMalloc/cudaFree
