@@ -102,6 +102,20 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     const unsigned warn_in = warn;
     using C = S;  // FP64 form -> double, mixed form -> float
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    // Own-site past level: on non-logging steps loaded here, so that the
+    // memory latency overlaps the force arithmetic below (the logging-step
+    // variant has no registers to spare and loads it where it is used).
+    Q<C> pst_f[ND], pst_u[3];
+    C pst_t[3];
+    if (!ENERGY) {
+#pragma unroll
+        for (int db = 0; db < ND; db++) pst_f[db] = ld4<C>(ps.L.ph[db], ps.s);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            pst_u[d] = ld4<C>(ps.L.q[d], ps.s);
+            pst_t[d] = ld1<C>(ps.L.th[d], ps.s);
+        }
+    }
     const bool have = carry.valid;
     const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
 
@@ -305,7 +319,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     const C keep = (C)(1.0 - P.damping_step);
 #pragma unroll
     for (int db = 0; db < ND; db++) {
-        const Q<C> fpast = ld4<C>(ps.L.ph[db], ps.s);
+        const Q<C> fpast = ENERGY ? ld4<C>(ps.L.ph[db], ps.s) : pst_f[db];
         const C fn[4] = {fc[db].w, fc[db].x, fc[db].y, fc[db].z};
         const C fo[4] = {fpast.w, fpast.x, fpast.y, fpast.z};
         const C dd[4] = {D[db].w, D[db].x, D[db].y, D[db].z};
@@ -329,8 +343,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const Q<C> Un = U[d];
-        const Q<C> Up = ld4<C>(ps.L.q[d], ps.s);
-        const C thp = ld1<C>(ps.L.th[d], ps.s);
+        const Q<C> Up = ENERGY ? ld4<C>(ps.L.q[d], ps.s) : pst_u[d];
+        const C thp = ENERGY ? ld1<C>(ps.L.th[d], ps.s) : pst_t[d];
         // link momentum vec(U_now U_past^dag) = vec((U_now - U_past) U_past^dag)
         const Q<C> dlt = {Un.w - Up.w, Un.x - Up.x, Un.y - Up.y, Un.z - Up.z};
         C E1, E2, E3;

@@ -285,16 +285,15 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
     };
     auto parity = [&](int p) { return ((ring.bits >> (p % G::NBUF)) ^ (unsigned)(p / G::NBUF)) & 1u; };
 
-    int issued = min(G::NBUF, nplanes);  // planes whose copy has been issued
-    int waited = 0;                      // planes whose copy every thread has waited for
     if (tid == 0) {
-        for (int p = 0; p < issued; p++)
+        for (int p = 0; p < min(G::NBUF, nplanes); p++)
             issue_plane<S, TY, TZ, ND>(maps, smem + p * G::BUF, &bars[p], plane_x(p), y0, z0);
     }
     if (tid == 32 % (TY * TZ)) {
         // past level of the first two planes computed (relative planes 1 and 2)
         for (int p = 1; p <= 2 && p <= nloc; p++) prefetch_past<ND>(pmaps, plane_x(p), y0, z0);
     }
+    if (wraps && nplanes > 3) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(3), y0, z0, tid);
 
     // own cells
     const int cq0 = (ty + 1) * G::QP + (tz + 1);
@@ -303,22 +302,23 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
     XCarry<S, ND> carry;
     carry.valid = false;
 
-    bool aborted = false;
-    for (int i = 0; i < nloc; i++) {
-        // planes i (x-1), i+1 (x), i+2 (x+1) must be resident; i+2 is new except at i = 0
-        bool ok = true;
-        for (int p = (i == 0 ? 0 : i + 2); p <= i + 2; p++) {
-            ok = ok && mbar_wait_bounded(&bars[p % G::NBUF], parity(p));
-            if (ok && wraps) patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + (p % G::NBUF) * G::BUF, plane_x(p), y0, z0, tid);
-        }
-        if (!ok) *s_abort = 1;
-        __syncthreads();
-        if (*s_abort) {
-            aborted = true;
-            break;
-        }
-        waited = i + 3;
+    // planes 0, 1, 2 (x0-1, x0, x0+1) resident and patched before the first site
+    bool ok = true;
+    for (int p = 0; p < 3; p++) {  // nplanes >= 3
+        ok = ok && mbar_wait_bounded(&bars[p], parity(p));
+        if (ok && wraps) patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + p * G::BUF, plane_x(p), y0, z0, tid);
+    }
+    if (!ok) *s_abort = 1;
+    __syncthreads();
+    // on a failed wait: the copies of planes [drain0, drain1) may still be in flight
+    int drain0 = 0, drain1 = min(G::NBUF, nplanes);
+    bool aborted = *s_abort != 0;
 
+    // One CTA barrier per plane: after computing plane i the threads wait for
+    // (and patch) plane i+3, which the next site needs, then synchronise once;
+    // that barrier both publishes the patches and frees plane i's buffer for
+    // the copy of plane i+4.
+    for (int i = 0; i < nloc && !aborted; i++) {
         const unsigned char* bm = smem + (i % G::NBUF) * G::BUF;
         const unsigned char* bc = smem + ((i + 1) % G::NBUF) * G::BUF;
         const unsigned char* bp = smem + ((i + 2) % G::NBUF) * G::BUF;
@@ -341,21 +341,32 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn,
                                     counts(P, x));
 
-        __syncthreads();  // every thread is done with plane i's buffer
-        if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
-        // plane i+3 is waited (and patched) in the next iteration
-        if (wraps && i + 3 < nplanes) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 3), y0, z0, tid);
-        if (i + G::NBUF < nplanes) {
-            if (tid == 0)
-                issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
-                                           plane_x(i + G::NBUF), y0, z0);
-            issued = i + G::NBUF + 1;
+        // plane i+3 (x+2) for the next site; its copy was issued one plane ago
+        bool okn = true;
+        if (i + 3 < nplanes) {
+            okn = mbar_wait_bounded(&bars[(i + 3) % G::NBUF], parity(i + 3));
+            if (okn && wraps)
+                patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + ((i + 3) % G::NBUF) * G::BUF, plane_x(i + 3), y0, z0,
+                                                  tid);
         }
+        if (!okn) *s_abort = 1;
+        __syncthreads();
+        if (*s_abort) {  // planes 0 .. i+2 were waited; the last copy issued was plane i+3
+            aborted = true;
+            drain0 = i + 3;
+            drain1 = min(nplanes, i + 4);
+            break;
+        }
+        if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
+        if (wraps && i + 4 < nplanes) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 4), y0, z0, tid);
+        if (tid == 0 && i + G::NBUF < nplanes)
+            issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
+                                       plane_x(i + G::NBUF), y0, z0);
     }
     if (aborted) {
         // drain: wait (bounded) for the copies still in flight into this CTA's buffers
         if (tid == 0)
-            for (int p = waited; p < issued; p++) mbar_wait_bounded(&bars[p % G::NBUF], parity(p));
+            for (int p = drain0; p < drain1; p++) mbar_wait_bounded(&bars[p % G::NBUF], parity(p));
         __syncthreads();
         return false;
     }
