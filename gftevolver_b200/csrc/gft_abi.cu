@@ -248,6 +248,12 @@ cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelP
     return launch_fast_step<S, kModel2HDM>(P, now, past, h->d_status, h->d_part_e, energy, 0, h->stream);
 }
 
+// Partial rows the Gauss kernel of this handle's form writes.
+int gauss_blocks(const gft_handle* h, const StepParams& P)
+{
+    return (h->cfg.form == GFT_FORM_REF) ? ref_launch_blocks(P) : fast_gauss_blocks(P);
+}
+
 template <class S>
 cudaError_t launch_gauss(gft_handle* h, const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut)
 {
@@ -582,7 +588,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
         err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e);
         h->launches += 1 + (e ? finalize_launches(step_blocks(h, P), true) : 0) +
-                       (g ? 1 + finalize_launches(fast_gauss_blocks(P), true) : 0);
+                       (g ? 1 + finalize_launches(gauss_blocks(h, P), true) : 0);
         if (prof) {
             cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
             h->ev_used++;
@@ -602,7 +608,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         if (g && err == cudaSuccess) {
             err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
             if (err == cudaSuccess)
-                err = launch_finalize(h->d_part_g, fast_gauss_blocks(P), kGaussSlots, 4, h->d_scale + kObsCount,
+                err = launch_finalize(h->d_part_g, gauss_blocks(h, P), kGaussSlots, 4, h->d_scale + kObsCount,
                                       out + kObsCount, h->d_mid, h->stream);
         }
         if (e || g) {

@@ -78,7 +78,10 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
     if (warn) atomicOr(status, warn);
 }
 
-// Gauss-law residual after a step (gauss_site in gft_step_body.cuh).
+// Gauss-law residual after a step (gauss_site in gft_step_body.cuh), one
+// thread per site: every load of a site is independent of the others, which
+// keeps the most loads in flight (a march along x that carries the x - 1 links
+// in registers serialises them and measured slower).
 template <class S, int MODEL>
 __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                          double* partials)

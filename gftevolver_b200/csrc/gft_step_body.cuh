@@ -137,7 +137,9 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         SA[a] = {(C)0, (C)0, (C)0, (C)0};
         SB[a] = {(C)0, (C)0, (C)0, (C)0};
     }
-    double mag_e = 0.0, plaq2 = 0.0, plaq1 = 0.0;
+    // logging-step terms: per-site partial sums in the form's arithmetic (a few
+    // cancellation-free terms each), added to the FP64 block sums once per site
+    C mag_e = (C)0, plaq2 = (C)0, plaq1 = (C)0;
 #pragma unroll
     for (int pl = 0; pl < 3; pl++) {
         const int i = (pl == 2) ? 1 : 0;
@@ -161,12 +163,12 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             // plaquette P1 = Aij U_i^dag: both orientations have the same trace;
             // 1 - cos F = 2 sin^2(F/2) (no cancellation for small F)
             const Q<C> P1 = qmul(Aij, qconj(U[i]));
-            const double omt = (double)one_minus_trace(P1);
+            const C omt = one_minus_trace(P1);
             const C hF = gsin((C)0.5 * F);
-            const double omc = 2.0 * (double)(hF * hF);
-            mag_e += 4.0 * P.lap[i] * P.lap[j] * (P.inv_g_sqr * omt + P.inv_gp_sqr * omc);
-            plaq2 += 1.0 - omt;
-            plaq1 += 1.0 - omc;
+            const C omc = (C)2 * hF * hF;
+            mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * ((C)P.inv_g_sqr * omt + (C)P.inv_gp_sqr * omc);
+            plaq2 += (C)1 - omt;
+            plaq1 += (C)1 - omc;
         }
     }
 #pragma unroll
@@ -211,7 +213,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         D[db] = {w * fc[db].w, w * fc[db].x, w * fc[db].y, w * fc[db].z};
     }
     C J[3][4];
-    double grad_e = 0.0;
+    C grad_e = (C)0;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         C sn, cs;
@@ -242,7 +244,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             j3 += t.w * fp.x - t.x * fp.w - t.y * fp.z + t.z * fp.y;
             if (ENERGY) {
                 const C e0 = fp.w - t.w, e1 = fp.x - t.x, e2 = fp.y - t.y, e3 = fp.z - t.z;
-                grad_e += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (double)(e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                grad_e += (C)(0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
             }
         }
         J[a][0] = (C)0.25 * j0;
@@ -313,7 +315,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
 
     // ---- scalar leapfrog (Model.cpp:347-356):
     //      phi(t+dt) = phi + [(phi - phi_past)(1 - damping) + dt^2 (D - dV)], one rounding at the end
-    double kin_e = 0.0, phisq = 0.0;
+    C kin_e = (C)0, phisq = (C)0;
     C check = (C)0;  // sum of every new value: non-finite iff one of them is
     const C dt2 = (C)P.dt2;
     const C keep = (C)(1.0 - P.damping_step);
@@ -330,15 +332,15 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             out[k] = fn[k] + (keep * vel + dt2 * (dd[k] - Pot[db][k]));
             check += out[k];
             if (ENERGY) {
-                kin_e += 0.5 * P.inv_sqr_dt * (double)(vel * vel);
-                phisq += (double)(fn[k] * fn[k]);
+                kin_e += vel * vel;  // x 0.5 / dt^2 below
+                phisq += fn[k] * fn[k];
             }
         }
         st4(ps.L.ph[db], ps.s, out[0], out[1], out[2], out[3]);
     }
 
     // ---- link update (WilsonLoops/Source/StandardModel.cpp:456-514) ----
-    double elec_e = 0.0;
+    C elec_e = (C)0;
     const C gY = (C)P.gsq[0], gI = (C)P.gsq[1];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -358,8 +360,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             // 1 - (U_now U_past^dag)_0 / |U_now U_past^dag| and 1 - cos(dtheta) = 2 sin^2(dtheta/2)
             const Q<C> Ed = {Un.w * Up.w + Un.x * Up.x + Un.y * Up.y + Un.z * Up.z, E1, E2, E3};
             const C h = gsin((C)0.5 * dth);
-            elec_e += 4.0 * P.lap[d] * P.inv_sqr_dt *
-                      (P.inv_g_sqr * (double)one_minus_trace(Ed) + P.inv_gp_sqr * 2.0 * (double)(h * h));
+            elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) *
+                      ((C)P.inv_g_sqr * one_minus_trace(Ed) + (C)P.inv_gp_sqr * (C)2 * h * h);
         }
         if (R0 * R0 > (C)1) warn |= kWarnAsin;
         if (fabs(th[d]) > (C)1e4) warn |= kWarnRange;
@@ -394,15 +396,17 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     }
 
     if (ENERGY) {
+        const double ge = (double)grad_e, ke = 0.5 * P.inv_sqr_dt * (double)kin_e;
+        const double me = (double)mag_e, ee = (double)elec_e;
         obs[kObsPotential] += pot_e;
-        obs[kObsGradient] += grad_e;
-        obs[kObsKinetic] += kin_e;
-        obs[kObsMagnetic] += mag_e;
-        obs[kObsElectric] += elec_e;
-        obs[kObsEnergy] += pot_e + grad_e + kin_e + mag_e + elec_e;
-        obs[kObsPlaqSU2] += plaq2;
-        obs[kObsPlaqU1] += plaq1;
-        obs[kObsPhiSq] += phisq;
+        obs[kObsGradient] += ge;
+        obs[kObsKinetic] += ke;
+        obs[kObsMagnetic] += me;
+        obs[kObsElectric] += ee;
+        obs[kObsEnergy] += pot_e + ge + ke + me + ee;
+        obs[kObsPlaqSU2] += (double)plaq2;
+        obs[kObsPlaqU1] += (double)plaq1;
+        obs[kObsPhiSq] += (double)phisq;
     }
 }
 
@@ -411,22 +415,36 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
 // the site x - e_a.  v[k] = v[4 + k] = |violation of constraint k| (the
 // integrated and the maximum slot of the analyser).  sin is the library's
 // double series.
+// One link direction at one site, both levels, as FP64 values.
+struct GLink {
+    Q<double> now, fut;
+    double tnow, tfut;
+};
+
+template <class S>
+__device__ __forceinline__ GLink gauss_link(const LevelPtrs<S>& now, const LevelPtrs<S>& fut, int d, int s)
+{
+    return {ld4<double>(now.q[d], s), ld4<double>(fut.q[d], s), ld1<double>(now.th[d], s), ld1<double>(fut.th[d], s)};
+}
+
+// The residuals from the links at x (own[d]) and at x - e_d (back[d]) and the
+// doublets at x (site c).
 template <class S, int MODEL>
-__device__ __forceinline__ void gauss_site(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut,
-                                           int c, int md0, int md1, int md2, double (&v)[kGaussSlots])
+__device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&own)[3], const GLink (&back)[3],
+                                           const LevelPtrs<S>& now, const LevelPtrs<S>& fut, int c,
+                                           double (&v)[kGaussSlots])
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
-    const int md[3] = {md0, md1, md2};
     double el[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        const double la = ld1<double>(fut.th[d], c) - ld1<double>(now.th[d], c);
-        const double na = ld1<double>(fut.th[d], md[d]) - ld1<double>(now.th[d], md[d]);
+        const double la = own[d].tfut - own[d].tnow;
+        const double na = back[d].tfut - back[d].tnow;
         el[0] += (gsin(la) - gsin(na)) * P.lap[d];
         // vec(U_now(x)^dag U_fut(x)) - vec(U_fut(x-d) U_now(x-d)^dag)
         double a1, a2, a3, b1, b2, b3;
-        qmul_vec(qconj(ld4<double>(now.q[d], c)), ld4<double>(fut.q[d], c), a1, a2, a3);
-        qmul_vec(ld4<double>(fut.q[d], md[d]), qconj(ld4<double>(now.q[d], md[d])), b1, b2, b3);
+        qmul_vec(qconj(own[d].now), own[d].fut, a1, a2, a3);
+        qmul_vec(back[d].fut, qconj(back[d].now), b1, b2, b3);
         el[1] += (a1 - b1) * P.lap[d];
         el[2] += (a2 - b2) * P.lap[d];
         el[3] += (a3 - b3) * P.lap[d];
@@ -447,6 +465,15 @@ __device__ __forceinline__ void gauss_site(const StepParams& P, const LevelPtrs<
         v[k] = av;
         v[4 + k] = av;
     }
+}
+
+template <class S, int MODEL>
+__device__ __forceinline__ void gauss_site(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut,
+                                           int c, int md0, int md1, int md2, double (&v)[kGaussSlots])
+{
+    const GLink own[3] = {gauss_link(now, fut, 0, c), gauss_link(now, fut, 1, c), gauss_link(now, fut, 2, c)};
+    const GLink back[3] = {gauss_link(now, fut, 0, md0), gauss_link(now, fut, 1, md1), gauss_link(now, fut, 2, md2)};
+    gauss_core<S, MODEL>(P, own, back, now, fut, c, v);
 }
 
 }  // namespace gft
