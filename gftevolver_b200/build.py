@@ -17,6 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgft_b200.so")
+HOST_RUN = os.path.join(HERE, "gft_run")  # GFTEvolver's main() over the C ABI (host/gft_run.cpp)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -43,7 +44,7 @@ def nvcc() -> str:
 
 def _deps_mtime() -> float:
     m = 0.0
-    for d in (CSRC, os.path.join(ROOT, "include")):
+    for d in (CSRC, os.path.join(ROOT, "include"), os.path.join(HERE, "host")):
         for f in os.listdir(d):
             m = max(m, os.path.getmtime(os.path.join(d, f)))
     return m
@@ -51,6 +52,8 @@ def _deps_mtime() -> float:
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime() and not ptxas_info:
+        if not os.path.exists(HOST_RUN) or os.path.getmtime(HOST_RUN) < _deps_mtime():
+            build_host()
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
@@ -80,7 +83,19 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if r.returncode != 0:
         raise RuntimeError(f"nvcc link failed:\n{r.stdout}")
     os.replace(tmp, LIB)
+    build_host()
     return LIB
+
+
+def build_host() -> str:
+    """The gft_run program (g++, linked against the in-tree library with an $ORIGIN rpath)."""
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), os.path.join(HERE, "host", "gft_run.cpp"),
+           "-L", HERE, "-lgft_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_RUN]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host program build failed:\n{r.stdout}")
+    return HOST_RUN
 
 
 if __name__ == "__main__":

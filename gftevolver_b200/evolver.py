@@ -139,6 +139,26 @@ class Evolver:
         self.h = h
         self.last_warnings = 0
 
+    # -- checkpoint / restart --------------------------------------------------
+    def save(self, path: str) -> None:
+        """Checkpoint: both time levels (reference layout, storage precision), the
+        step counter, the form and the parameters, in one .npz file.  Restarting
+        from it continues bit for bit (the step depends only on the two levels and
+        time_iter)."""
+        sc, ve = self.download()
+        np.savez(path, scalars=sc, vectors=ve, time_iter=self.time_iter, form=self.form,
+                 params=np.array(repr(asdict(self.params))))
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Evolver":
+        """Restart from a checkpoint written by save()."""
+        import ast
+        z = np.load(path, allow_pickle=False)
+        params = LatticeParams(**ast.literal_eval(str(z["params"])))
+        ev = cls(params, form=str(z["form"]), device=device)
+        ev.upload(z["scalars"], z["vectors"], int(z["time_iter"]))
+        return ev
+
     # -- lifetime ------------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "h", None):

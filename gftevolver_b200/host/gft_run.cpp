@@ -1,0 +1,397 @@
+// gft_run.cpp -- GFTEvolver's main(), with the time loop on the GPU.
+//
+// Reads a configuration tree laid out like the reference's
+// (<root>/Core/Config/Lattice.cfg, Model.cfg, Potentials/Config/*.cfg,
+// WilsonLoops/Config/*.cfg, Analysers/Config/*.cfg), evolves through the C ABI
+// of libgft_b200.so and writes what the reference's analysers write into
+// <root>/Data: the Energy and GaugeCondition global-quantity rows
+// (Analysers/Source/Energy.cpp:169-188, Analysers/Source/GaugeCondition.cpp:167-193)
+// and the OutputFields dumps (Analysers/Source/OutputFields.cpp:63-133).  The
+// reference's main() (main.cpp:10-60) constructs a Lattice, runs
+// initialAnalysis, evolve, finalAnalysis; this program does the same three
+// phases with Lattice::evolve (Core/Source/Lattice.cpp:755-876) replaced by
+// gft_evolve.
+//
+// The .cfg files are positional, as the reference's configure() functions read
+// them: a fixed number of description lines, then one entry per line whose
+// values follow the last ':' of the line.
+//
+// Initial data: --ic FILE (both time levels in the reference layout, float for
+// the ref32 / mixed forms, double for ref64 / fp64), or --device-ic SEED
+// (gft_init_fields: Higgs N(1, 0.1^2) per component, random links with
+// eps, theta_Y ~ N(0, 0.1^2)); the reference's own RandomUniform generator is
+// not restated.
+//
+// Usage: gft_run ROOT [--form ref32|ref64|fp64|mixed] [--ic FILE | --device-ic SEED]
+//                     [--device N] [--final-bin FILE] [--print-config]
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "gft.h"
+
+namespace {
+
+using Entries = std::vector<std::vector<std::string>>;
+
+// Entries of a positional .cfg file: after `header` description lines, the
+// whitespace-separated tokens after the last ':' of every line that has one.
+Entries read_cfg(const std::string& path, int header)
+{
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot open " + path);
+    Entries out;
+    std::string line;
+    for (int i = 0; i < header && std::getline(f, line); i++) {
+    }
+    while (std::getline(f, line)) {
+        const auto c = line.rfind(':');
+        if (c == std::string::npos) continue;
+        std::istringstream is(line.substr(c + 1));
+        std::vector<std::string> tok;
+        std::string t;
+        while (is >> t) tok.push_back(t);
+        out.push_back(tok);
+    }
+    return out;
+}
+
+const std::string& tok(const Entries& e, size_t i, size_t k, const std::string& file)
+{
+    if (i >= e.size() || k >= e[i].size())
+        throw std::runtime_error(file + ": entry " + std::to_string(i) + " value " + std::to_string(k) + " missing");
+    return e[i][k];
+}
+double num(const Entries& e, size_t i, size_t k, const std::string& file) { return std::stod(tok(e, i, k, file)); }
+int inum(const Entries& e, size_t i, size_t k, const std::string& file) { return std::stoi(tok(e, i, k, file)); }
+
+struct Analysers {
+    bool energy = false, gauss = false, fields = false;
+    std::string energy_path, gauss_path;
+    bool energy_opt[6] = {};
+    bool gauss_opt[2] = {};
+    int energy_freq = 1, gauss_freq = 1;
+    bool fields_both = false, fields_initial = false, fields_final = false, fields_continual = false;
+    int fields_freq = 1;
+    std::string fields_initial_path, fields_continual_path, fields_final_path;
+};
+
+struct Run {
+    gft_config cfg{};
+    int nt = 0;
+    Analysers an;
+};
+
+Run configure(const std::string& root)
+{
+    Run r;
+    gft_config& c = r.cfg;
+    // Core/Config/Lattice.cfg (Core/Source/Lattice.cpp:47-143)
+    const std::string lat = root + "/Core/Config/Lattice.cfg";
+    const Entries L = read_cfg(lat, 10);
+    c.nx = inum(L, 0, 0, lat);
+    c.ny = inum(L, 0, 1, lat);
+    c.nz = inum(L, 0, 2, lat);
+    c.dx = num(L, 1, 0, lat);
+    c.dy = num(L, 1, 1, lat);
+    c.dz = num(L, 1, 2, lat);
+    r.nt = inum(L, 2, 0, lat);
+    c.dt = num(L, 3, 0, lat);
+    const int nsc = inum(L, 4, 0, lat);
+    const int nvec = inum(L, 5, 0, lat);
+    if (inum(L, 6, 0, lat)) {  // nt from light-crossing times (Lattice.cpp:78-87)
+        const float crossings = (float)num(L, 7, 0, lat);
+        r.nt = static_cast<int>(crossings * static_cast<float>(c.nx) * c.dx / (2 * c.dt));
+    }
+    r.an.fields = inum(L, 9, 0, lat) != 0;
+    r.an.energy = inum(L, 10, 0, lat) != 0;
+    r.an.gauss = inum(L, 11, 0, lat) != 0;
+    for (int k = 0; k < 6; k++)
+        if (inum(L, 12, k, lat) != 3) throw std::runtime_error("only periodic faces (type 3) run on the GPU");
+    if (nvec != 5) throw std::runtime_error("only the quaternion link representation (5 components) runs on the GPU");
+
+    // Core/Config/Model.cfg (Core/Source/Model.cpp:173-221)
+    const std::string mod = root + "/Core/Config/Model.cfg";
+    const Entries M = read_cfg(mod, 11);
+    const int pot = inum(M, 0, 0, mod), grad = inum(M, 1, 0, mod), wl = inum(M, 2, 0, mod);
+    if (pot == 1 && grad == 2 && wl == 1 && nsc == 4)
+        c.model = GFT_MODEL_SM;
+    else if (pot == 2 && grad == 3 && wl == 2 && nsc == 8)
+        c.model = GFT_MODEL_2HDM;
+    else
+        throw std::runtime_error("model (potential " + std::to_string(pot) + ", gradient " + std::to_string(grad) +
+                                 ", wilson loop " + std::to_string(wl) + ", " + std::to_string(nsc) +
+                                 " scalars) is not built for the GPU");
+    c.damping = (float)num(M, 3, 0, mod);
+    c.nt_damped = inum(M, 4, 0, mod);
+    if (inum(M, 5, 0, mod)) c.nt_damped = static_cast<int>((float)num(M, 6, 0, mod) / c.dt);
+
+    if (c.model == GFT_MODEL_SM) {
+        // Potentials/Config/SO_N.cfg (Potentials/Source/SO_N.cpp:21-27)
+        const std::string so = root + "/Potentials/Config/SO_N.cfg";
+        const Entries S = read_cfg(so, 15);
+        c.lambda = num(S, 0, 0, so);
+        c.eta_sqr = num(S, 1, 0, so);
+        // WilsonLoops/Config/StandardModel.cfg
+        const std::string w = root + "/WilsonLoops/Config/StandardModel.cfg";
+        const Entries W = read_cfg(w, 12);
+        c.g = num(W, 0, 0, w);
+        c.gp = num(W, 1, 0, w);
+        c.div_tol = num(W, 2, 0, w);
+    } else {
+        // Potentials/Config/Double_SO_N.cfg (Potentials/Source/Double_SO_N.cpp:44-120)
+        const std::string ds = root + "/Potentials/Config/Double_SO_N.cfg";
+        const Entries D = read_cfg(ds, 40);
+        if (inum(D, 0, 0, ds) != 4) throw std::runtime_error("Double_SO_N: only 4 + 4 components run on the GPU");
+        c.apply_norm = inum(D, 1, 0, ds);
+        c.energy_offset = num(D, 2, 0, ds);
+        c.m1 = num(D, 3, 0, ds);
+        c.m2 = num(D, 3, 1, ds);
+        c.l1 = num(D, 4, 0, ds);
+        c.l2 = num(D, 4, 1, ds);
+        c.l3 = num(D, 5, 0, ds);
+        c.break_son = inum(D, 6, 0, ds);
+        c.m12r = num(D, 7, 0, ds);
+        c.l4p5 = num(D, 8, 0, ds);
+        c.l6r = num(D, 9, 0, ds);
+        c.l7r = num(D, 9, 1, ds);
+        c.break_uhalfn = inum(D, 10, 0, ds);
+        c.m12i = num(D, 11, 0, ds);
+        c.l4m5 = num(D, 12, 0, ds);
+        c.l5i = num(D, 12, 1, ds);
+        c.l6i = num(D, 13, 0, ds);
+        c.l7i = num(D, 13, 1, ds);
+        // WilsonLoops/Config/TwoHDM.cfg
+        const std::string w = root + "/WilsonLoops/Config/TwoHDM.cfg";
+        const Entries W = read_cfg(w, 12);
+        c.g = num(W, 0, 0, w);
+        c.gp = num(W, 1, 0, w);
+        if (inum(W, 3, 0, w)) throw std::runtime_error("the generator link representation does not run on the GPU");
+        c.div_tol = num(W, 4, 0, w);
+    }
+
+    // Analysers/Config/*.cfg (Analysers/Source/Energy.cpp:14-47, GaugeCondition.cpp:14-47, OutputFields.cpp:14-45)
+    if (r.an.energy) {
+        const std::string ef = root + "/Analysers/Config/Energy.cfg";
+        const Entries E = read_cfg(ef, 13);
+        r.an.energy_path = tok(E, 0, 0, ef);
+        bool any = false;
+        for (int k = 0; k < 6; k++) any |= (r.an.energy_opt[k] = inum(E, 1 + k, 0, ef) != 0);
+        r.an.energy_freq = inum(E, 7, 0, ef);
+        for (int k = 0; k < 6; k++)
+            if (inum(E, 9 + k, 0, ef)) std::cerr << "gft_run: local energy densities are not written by the GPU path\n";
+        c.energy_every = any ? r.an.energy_freq : 0;
+    }
+    if (r.an.gauss) {
+        const std::string gf = root + "/Analysers/Config/GaugeCondition.cfg";
+        const Entries G = read_cfg(gf, 13);
+        r.an.gauss_path = tok(G, 0, 0, gf);
+        r.an.gauss_opt[0] = inum(G, 1, 0, gf) != 0;
+        r.an.gauss_opt[1] = inum(G, 2, 0, gf) != 0;
+        r.an.gauss_freq = inum(G, 3, 0, gf);
+        if (inum(G, 5, 0, gf)) std::cerr << "gft_run: local Gauss violations are not written by the GPU path\n";
+        c.gauss_every = (r.an.gauss_opt[0] || r.an.gauss_opt[1]) ? r.an.gauss_freq : 0;
+    }
+    if (r.an.fields) {
+        const std::string of = root + "/Analysers/Config/OutputFields.cfg";
+        const Entries O = read_cfg(of, 13);
+        r.an.fields_both = inum(O, 0, 0, of) != 0;
+        r.an.fields_initial = inum(O, 1, 0, of) != 0;
+        r.an.fields_final = inum(O, 2, 0, of) != 0;
+        r.an.fields_continual = inum(O, 3, 0, of) != 0;
+        r.an.fields_freq = inum(O, 4, 0, of);
+        r.an.fields_initial_path = tok(O, 5, 0, of);
+        r.an.fields_continual_path = tok(O, 6, 0, of);
+        r.an.fields_final_path = tok(O, 7, 0, of);
+    }
+    return r;
+}
+
+void check(int rc, gft_handle* h, const char* what)
+{
+    if (rc < 0) throw std::runtime_error(std::string(what) + ": " + gft_last_error(h));
+    if (rc & GFT_W_ASIN_DOMAIN) std::cerr << "Panic: asin argument outside [-1, 1]\n";
+    if (rc & GFT_W_SQRT_DOMAIN) std::cerr << "Panic: sqrt of a negative number\n";
+    if (rc & GFT_W_NONFINITE) std::cerr << "Panic: non-finite field value\n";
+}
+
+// OutputFields::outputFields: one line per site, scalar then vector components.
+template <class T>
+void dump_fields(const std::string& path, const std::vector<T>& sc, const std::vector<T>& ve, int nsc, int time_step,
+                 bool both)
+{
+    std::ofstream ofs(path);
+    const size_t nsite2 = sc.size() / nsc;
+    const size_t n = both ? nsite2 : nsite2 / 2;
+    const size_t t0 = both ? 0 : (size_t)((time_step + 1) % 2) * n;
+    for (size_t s = t0; s < t0 + n; s++) {
+        for (int k = 0; k < nsc; k++) ofs << sc[s * nsc + k] << " ";
+        for (int k = 0; k < 15; k++) ofs << ve[s * 15 + k] << " ";
+        ofs << std::endl;
+    }
+}
+
+template <class T>
+int run(const std::string& root, Run& r, const std::string& ic_path, long long seed, const std::string& final_bin)
+{
+    gft_config& c = r.cfg;
+    const int nsc = (c.model == GFT_MODEL_SM) ? 4 : 8;
+    const size_t nsite = (size_t)c.nx * c.ny * c.nz;
+    const std::string data = root + "/Data";
+    mkdir(data.c_str(), 0755);
+    if (!r.an.fields_continual_path.empty()) {
+        const auto slash = r.an.fields_continual_path.rfind('/');
+        if (slash != std::string::npos) mkdir((data + "/" + r.an.fields_continual_path.substr(0, slash)).c_str(), 0755);
+    }
+
+    gft_handle* h = nullptr;
+    check(gft_create(&c, &h), nullptr, "gft_create");
+    std::vector<T> sc(2 * nsite * nsc), ve(2 * nsite * 15);
+    auto download = [&]() {
+        if constexpr (sizeof(T) == 4)
+            check(gft_download_f32(h, sc.data(), ve.data()), h, "gft_download");
+        else
+            check(gft_download_f64(h, sc.data(), ve.data()), h, "gft_download");
+    };
+    if (!ic_path.empty()) {
+        std::ifstream f(ic_path, std::ios::binary);
+        f.read(reinterpret_cast<char*>(sc.data()), sc.size() * sizeof(T));
+        f.read(reinterpret_cast<char*>(ve.data()), ve.size() * sizeof(T));
+        if (!f) throw std::runtime_error("short initial-data file " + ic_path);
+        if constexpr (sizeof(T) == 4)
+            check(gft_upload_f32(h, sc.data(), ve.data(), 0), h, "gft_upload");
+        else
+            check(gft_upload_f64(h, sc.data(), ve.data(), 0), h, "gft_upload");
+    } else {
+        gft_ic ic{};
+        ic.seed = (uint64_t)seed;
+        for (int k = 0; k < 8; k++) {
+            ic.mean[k] = 1.0;
+            ic.sigma[k] = 0.1;
+        }
+        ic.theta_sigma = 0.1;
+        ic.eps_sigma = 0.1;
+        check(gft_init_fields(h, &ic), h, "gft_init_fields");
+    }
+
+    // initialAnalysis
+    if (r.an.fields && r.an.fields_initial) {
+        download();
+        dump_fields(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
+    }
+
+    // evolve: chunks end where OutputFields writes a continual dump
+    const int chunk_max = (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0) ? r.an.fields_freq : 1000;
+    std::vector<gft_observables> rows(chunk_max + 1);
+    int done = 0;
+    while (done < r.nt) {
+        const int n = std::min(chunk_max - done % chunk_max, r.nt - done);
+        int got = 0;
+        check(gft_evolve(h, n, rows.data(), (int)rows.size(), &got), h, "gft_evolve");
+        done += n;
+        for (int i = 0; i < got; i++) {
+            const gft_observables& o = rows[i];
+            if (o.has_energy && !r.an.energy_path.empty()) {
+                std::ofstream ofs(data + "/" + r.an.energy_path, std::ios::app);
+                const double v[6] = {o.energy, o.potential, o.gradient, o.kinetic, o.magnetic, o.electric};
+                for (int k = 0; k < 6; k++)
+                    if (r.an.energy_opt[k]) ofs << v[k] << " ";
+                ofs << "\n";
+            }
+            if (o.has_gauss && !r.an.gauss_path.empty()) {
+                std::ofstream ofs(data + "/" + r.an.gauss_path, std::ios::app);
+                if (r.an.gauss_opt[0])
+                    for (int k = 0; k < 4; k++) ofs << o.gauss_int[k] << " ";
+                if (r.an.gauss_opt[1])
+                    for (int k = 0; k < 4; k++) ofs << o.gauss_max[k] << " ";
+                ofs << "\n";
+            }
+        }
+        if (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0 && done % r.an.fields_freq == 0) {
+            download();
+            dump_fields(data + "/" + r.an.fields_continual_path + "_" + std::to_string(done) + ".dat", sc, ve, nsc, done,
+                        r.an.fields_both);
+        }
+    }
+
+    // finalAnalysis
+    download();
+    if (r.an.fields && r.an.fields_final)
+        dump_fields(data + "/" + r.an.fields_final_path, sc, ve, nsc, r.nt, r.an.fields_both);
+    if (!final_bin.empty()) {
+        std::ofstream f(final_bin, std::ios::binary);
+        f.write(reinterpret_cast<const char*>(sc.data()), sc.size() * sizeof(T));
+        f.write(reinterpret_cast<const char*>(ve.data()), ve.size() * sizeof(T));
+    }
+    gft_destroy(h);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) {
+        std::cerr << "usage: gft_run ROOT [--form ref32|ref64|fp64|mixed] [--ic FILE | --device-ic SEED] "
+                     "[--device N] [--final-bin FILE] [--print-config]\n";
+        return 2;
+    }
+    try {
+        const std::string root = argv[1];
+        std::string form = "mixed", ic, final_bin;
+        long long seed = -1;
+        int device = 0;
+        bool print = false;
+        for (int i = 2; i < argc; i++) {
+            const std::string a = argv[i];
+            auto next = [&]() -> std::string {
+                if (i + 1 >= argc) throw std::runtime_error(a + " needs a value");
+                return argv[++i];
+            };
+            if (a == "--form") form = next();
+            else if (a == "--ic") ic = next();
+            else if (a == "--device-ic") seed = std::stoll(next());
+            else if (a == "--device") device = std::stoi(next());
+            else if (a == "--final-bin") final_bin = next();
+            else if (a == "--print-config") print = true;
+            else throw std::runtime_error("unknown option " + a);
+        }
+        Run r = configure(root);
+        r.cfg.device = device;
+        bool f64 = false;
+        if (form == "ref32") { r.cfg.form = GFT_FORM_REF; r.cfg.storage_bytes = 4; }
+        else if (form == "ref64") { r.cfg.form = GFT_FORM_REF; r.cfg.storage_bytes = 8; f64 = true; }
+        else if (form == "fp64") { r.cfg.form = GFT_FORM_FP64; f64 = true; }
+        else if (form == "mixed") { r.cfg.form = GFT_FORM_MIXED; }
+        else throw std::runtime_error("unknown form " + form);
+        if (print) {
+            const gft_config& c = r.cfg;
+            std::printf("model %d form %d storage %d nx %d ny %d nz %d dx %.17g dy %.17g dz %.17g dt %.17g nt %d\n",
+                        c.model, c.form, c.storage_bytes, c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, c.dt, r.nt);
+            std::printf("g %.17g gp %.17g div_tol %.17g damping %.17g nt_damped %d lambda %.17g eta_sqr %.17g\n", c.g,
+                        c.gp, c.div_tol, c.damping, c.nt_damped, c.lambda, c.eta_sqr);
+            std::printf("m1 %.17g m2 %.17g l1 %.17g l2 %.17g l3 %.17g m12r %.17g l4p5 %.17g l6r %.17g l7r %.17g\n", c.m1,
+                        c.m2, c.l1, c.l2, c.l3, c.m12r, c.l4p5, c.l6r, c.l7r);
+            std::printf("m12i %.17g l4m5 %.17g l5i %.17g l6i %.17g l7i %.17g break_son %d break_uhalfn %d "
+                        "apply_norm %d energy_offset %.17g\n",
+                        c.m12i, c.l4m5, c.l5i, c.l6i, c.l7i, c.break_son, c.break_uhalfn, c.apply_norm,
+                        c.energy_offset);
+            std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s\n", c.energy_every, c.gauss_every,
+                        r.an.energy_path.c_str(), r.an.gauss_path.c_str());
+            return 0;
+        }
+        if (ic.empty() && seed < 0) throw std::runtime_error("give --ic FILE or --device-ic SEED");
+        return f64 ? run<double>(root, r, ic, seed, final_bin) : run<float>(root, r, ic, seed, final_bin);
+    } catch (const std::exception& e) {
+        std::cerr << "Error in " << e.what() << std::endl;
+        return 1;
+    }
+}

@@ -234,3 +234,21 @@ def test_step_kernel_name_follows_form_and_shape(oracle_mod):
     odd = oracle_mod.Params(nx=5, ny=3, nz=7)
     with Evolver(_lp(odd.__dict__), form="mixed") as ev:
         assert ev.step_kernel_name == "fast_step_kernel"
+
+
+@pytest.mark.parametrize("form", ["mixed", "fp64", "ref32"])
+def test_checkpoint_restart_continues_bit_for_bit(tmp_path, oracle_mod, form):
+    from gftevolver_b200 import Evolver, InitialData
+    op = oracle_mod.Params(nx=8, ny=8, nz=32, energy_every=3, gauss_every=4)
+    with Evolver(_lp(op.__dict__), form=form) as ev:
+        ev.init_fields(InitialData(seed=8, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1))
+        ev.evolve(5)
+        ev.save(str(tmp_path / "ck.npz"))
+        rows_a = ev.evolve(6)
+        a = ev.download()
+    with Evolver.load(str(tmp_path / "ck.npz")) as ev:
+        assert ev.time_iter == 5 and ev.form == form
+        rows_b = ev.evolve(6)
+        b = ev.download()
+    assert rows_a == rows_b
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])

@@ -1,0 +1,99 @@
+"""gft_run -- GFTEvolver's main() over the C ABI: reads the reference's
+positional .cfg tree and writes the analysers' .dat files.
+
+CPU: the configuration a reference run would see is parsed into gft_config
+(no device call).  GPU: the same configuration tree and initial data run
+through the reference binary (oracle/_ref/ref32, its own analysers writing
+Data/*.dat) and through gft_run in the reference-arithmetic form; the .dat
+rows agree to the printed precision (6 significant digits; 2e-5 relative
+allows one unit in the last printed digit where the reference's float running
+sums and the FP64 sums round differently) and the final fields to the ref32
+bound (8 float ulps, at most 1 % of words different).
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GFT_RUN = os.path.join(ROOT, "gftevolver_b200", "gft_run")
+
+
+@pytest.fixture(scope="module")
+def gft_run():
+    if not os.path.exists(GFT_RUN):
+        from gftevolver_b200 import build
+        build.build()
+        build.build_host()
+    return GFT_RUN
+
+
+def _params(orc, model):
+    return orc.Params(model=model, nx=6, ny=5, nz=8, dt=0.05, damping=0.3, nt_damped=2, energy_every=2,
+                      gauss_every=3, g=0.61, gp=0.33)
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_config_tree_is_parsed_like_the_reference(tmp_path, oracle_mod, gft_run, model):
+    from oracle import refrun
+    p = _params(oracle_mod, model)
+    refrun.write_configs(str(tmp_path), p, 7)
+    out = subprocess.run([gft_run, str(tmp_path), "--print-config", "--form", "ref32"], capture_output=True,
+                         text=True, check=True).stdout.split()
+    kv = {out[i]: out[i + 1] for i in range(0, len(out) - 1, 2)}
+    assert int(kv["model"]) == model and int(kv["nt"]) == 7
+    assert (int(kv["nx"]), int(kv["ny"]), int(kv["nz"])) == (6, 5, 8)
+    assert float(kv["dt"]) == 0.05 and float(kv["g"]) == 0.61 and float(kv["gp"]) == 0.33
+    assert float(kv["damping"]) == float(np.float32(0.3)) and int(kv["nt_damped"]) == 2
+    assert int(kv["energy_every"]) == 2 and int(kv["gauss_every"]) == 3
+    if model == 1:
+        assert float(kv["lambda"]) == p.lam and float(kv["eta_sqr"]) == p.eta_sqr
+    else:
+        assert float(kv["m12r"]) == p.m12r and float(kv["l4p5"]) == p.l4p5 and int(kv["break_son"]) == 1
+
+
+def test_unsupported_reference_configuration_is_refused(tmp_path, oracle_mod, gft_run):
+    from oracle import refrun
+    p = _params(oracle_mod, 1)
+    refrun.write_configs(str(tmp_path), p, 7)
+    lat = tmp_path / "Core" / "Config" / "Lattice.cfg"
+    lat.write_text(lat.read_text().replace("faces                          : 3 3 3 3 3 3",
+                                           "faces                          : 1 1 3 3 3 3"))
+    r = subprocess.run([gft_run, str(tmp_path), "--print-config"], capture_output=True, text=True)
+    assert r.returncode == 1 and "periodic" in r.stderr
+
+
+def _numbers(path):
+    return [[float(v) for v in line.split()] for line in open(path) if line.strip()]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", [1, 2])
+def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_run, model):
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("oracle/_ref/ref32 not built")
+    p = _params(oracle_mod, model)
+    ic = oracle_mod.ICSpec(seed=5, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
+                           eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(p, ic, np.float32)
+    ref_dir, gpu_dir = tmp_path / "ref", tmp_path / "gpu"
+    ref_dir.mkdir()
+    r_sc, r_ve, _, _ = refrun.run(p, sc, ve, 7, workdir=str(ref_dir))
+    shutil.copytree(ref_dir, gpu_dir, ignore=shutil.ignore_patterns("Data", "final.bin", "rows.txt", "timing.txt"))
+    subprocess.run([gft_run, str(gpu_dir), "--form", "ref32", "--ic", str(gpu_dir / "ic.bin"), "--final-bin",
+                    str(gpu_dir / "final.bin")], check=True, capture_output=True, text=True)
+    for name in ("global_quantities.dat", "global_quantities_gauge.dat"):
+        a, b = _numbers(gpu_dir / "Data" / name), _numbers(ref_dir / "Data" / name)
+        assert len(a) == len(b) and len(a) > 0
+        for ra, rb in zip(a, b):
+            assert len(ra) == len(rb)
+            np.testing.assert_allclose(ra, rb, rtol=2e-5, atol=1e-12)
+    raw = np.fromfile(gpu_dir / "final.bin", dtype=np.float32)
+    g_sc, g_ve = raw[:sc.size].reshape(sc.shape), raw[sc.size:].reshape(ve.shape)
+    for g, r in ((g_sc, r_sc), (g_ve, r_ve)):
+        tol = 8 * np.spacing(np.maximum(np.abs(g), np.abs(r)))
+        assert np.all(np.abs(g.astype(np.float64) - r) <= tol + 1e-30)
+        assert np.mean(g != r) <= 0.01
