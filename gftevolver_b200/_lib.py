@@ -50,6 +50,7 @@ class GftConfig(ctypes.Structure):
         ("break_son", ctypes.c_int), ("break_uhalfn", ctypes.c_int), ("apply_norm", ctypes.c_int),
         ("energy_offset", ctypes.c_double),
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
+        ("fixed_axes", ctypes.c_int),
     ]
 
 

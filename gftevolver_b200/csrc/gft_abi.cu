@@ -147,11 +147,19 @@ StepParams gft::config_params(const gft_config& c, int nsite, bool f32ref, int t
     P.store_energy = energy ? 1 : 0;
     P.obs_x0 = 0;
     P.obs_x1 = c.nx;
+    P.fixed_axes = c.fixed_axes;
     return P;
 }
 
 void gft::row_scales(const gft_config& c, int nsite, double* scale)
 {
+    // means over the evolved sites (nsite = nx * ny * nz of c): a Fixed axis loses its two face planes
+    if (c.fixed_axes) {
+        const long long n[3] = {c.nx, c.ny, c.nz};
+        long long e = 1;
+        for (int a = 0; a < 3; a++) e *= ((c.fixed_axes >> a) & 1) ? (n[a] > 2 ? n[a] - 2 : 0) : n[a];
+        nsite = (int)(e > 0 ? e : 1);
+    }
     const double dv = c.dx * c.dy * c.dz;
     for (int k = 0; k < kRowSlots; k++) scale[k] = 1.0;
     for (int k = kObsEnergy; k <= kObsElectric; k++) scale[k] = dv;
@@ -303,6 +311,10 @@ int validate(const gft_config* c, std::string& why)
     }
     if (c->energy_every < 0 || c->gauss_every < 0) {
         why = "gft_create: analyser frequencies must be >= 0";
+        return GFT_E_INVALID;
+    }
+    if (c->fixed_axes < 0 || c->fixed_axes > 7) {
+        why = "gft_create: fixed_axes is a bitmask of the three axes (0..7)";
         return GFT_E_INVALID;
     }
     return GFT_OK;
@@ -815,6 +827,8 @@ int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_
     const int nx = h->cfg.nx;
     if (nx_global < 1 || x_begin < 0 || x_end > nx || x_begin >= x_end)
         return h->fail(GFT_E_INVALID, "gft_set_slab: need 0 <= x_begin < x_end <= nx and nx_global >= 1");
+    if (h->cfg.fixed_axes & 1)
+        return h->fail(GFT_E_UNSUPPORTED, "gft_set_slab: x-slabs need a periodic x axis (Fixed x faces given)");
     h->x_offset = x_offset;
     h->nx_global = nx_global;
     h->x_begin = x_begin;

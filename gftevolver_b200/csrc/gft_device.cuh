@@ -61,7 +61,17 @@ struct StepParams {
     int store_energy;       // logging step: renormalise as the reference does and accumulate energies
     int obs_x0, obs_x1;     // planes whose sites count in observables, Gauss residuals and warnings
                             // (all planes, except on an x-slab with ghost planes)
+    int fixed_axes;         // bit a: the two faces of axis a are Fixed (frozen, not evolved)
 };
+
+// A site on a Fixed face (BoundaryConditions/Source/Fixed.cpp:159-251): not
+// evolved, not part of the analysers' domain.
+__device__ __forceinline__ bool frozen(const StepParams& P, int x, int y, int z)
+{
+    const int f = P.fixed_axes;
+    return ((f & 1) && (x == 0 || x == P.nx - 1)) || ((f & 2) && (y == 0 || y == P.ny - 1)) ||
+           ((f & 4) && (z == 0 || z == P.nz - 1));
+}
 
 __device__ __forceinline__ bool counts(const StepParams& P, int x) { return x >= P.obs_x0 && x < P.obs_x1; }
 

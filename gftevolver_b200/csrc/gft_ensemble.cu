@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(TY * TZ) ensemble_gauss_kernel(const __grid_co
     const int nloc = min(lx, P.nx - w.w);
     for (int i = 0; i < nloc; i++) {
         const int x = w.w + i, xm = (x == 0) ? P.nx - 1 : x - 1;
-        if (!counts(P, x)) continue;
+        if (!counts(P, x) || frozen(P, x, y, z)) continue;
         double g[kGaussSlots];
         gauss_site<float, MODEL>(P, ep.lv[m][tn], ep.lv[m][1 - tn], (x * P.ny + y) * P.nz + z,
                                  (xm * P.ny + y) * P.nz + z, (x * P.ny + ym) * P.nz + z, (x * P.ny + y) * P.nz + zm,

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
 #pragma unroll
     for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
     unsigned warn = 0;
-    if ((z < P.nz) && (y < P.ny)) {
+    if ((z < P.nz) && (y < P.ny) && !frozen(P, x, y, z)) {  // Fixed faces: not evolved
         const Offs o = offsets(P, x, y, z);
         Stencil<int> n;
         n.c = o.c;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
     double v[kGaussSlots];
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
-    if (z < P.nz && y < P.ny && counts(P, x)) {
+    if (z < P.nz && y < P.ny && counts(P, x) && !frozen(P, x, y, z)) {
         const Offs o = offsets(P, x, y, z);
         gauss_site<S, MODEL>(P, now, fut, o.c, o.c + o.m[0], o.c + o.m[1], o.c + o.m[2], v);
     }

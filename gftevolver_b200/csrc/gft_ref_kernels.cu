@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.z;
-    const bool active = (z < P.nz) && (y < P.ny);
+    const bool active = (z < P.nz) && (y < P.ny) && !frozen(P, x, y, z);  // Fixed faces: not evolved
     double obs[kObsCount];
 #pragma unroll
     for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
     double v[kGaussSlots];
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
-    if (z < P.nz && y < P.ny && counts(P, x)) {
+    if (z < P.nz && y < P.ny && counts(P, x) && !frozen(P, x, y, z)) {
         const Nbr n = neighbours(P, x, y, z);
         const RefView<S> Vn{now};
         const RefView<S> Vf{fut};

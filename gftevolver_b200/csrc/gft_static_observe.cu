@@ -202,6 +202,10 @@ extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, c
     if (!c || !d_scalars || !d_vectors || !d_out || time_iter < 0) return GFT_E_INVALID;
     if (c->model != GFT_MODEL_SM && c->model != GFT_MODEL_2HDM) return GFT_E_UNSUPPORTED;
     if (c->nx < 1 || c->ny < 1 || c->nz < 1) return GFT_E_INVALID;
+    if (c->fixed_axes != 0) {
+        set_last_error("gft_observe_static: periodic lattices only (fixed_axes must be 0)");
+        return GFT_E_UNSUPPORTED;
+    }
     const long long n = (long long)c->nx * c->ny * c->nz;
     if (n > kStaticMaxSites) {
         set_last_error("gft_observe_static: lattice of " + std::to_string(n) +

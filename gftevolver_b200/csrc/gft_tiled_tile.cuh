@@ -338,8 +338,11 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         n.d21 = {bc, cq0 - G::QP + 1, ch0 - G::HP + 1};
         const int x = x0 + i;
         const int s = (x * P.ny + y) * P.nz + z;
-        site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn,
-                                    counts(P, x));
+        if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
+            carry.valid = false;
+        else
+            site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn,
+                                        counts(P, x));
 
         // plane i+3 (x+2) for the next site; its copy was issued one plane ago
         bool okn = true;

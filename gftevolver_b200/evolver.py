@@ -64,6 +64,7 @@ class LatticeParams:
     energy_offset: float = 0.0
     energy_every: int = 0
     gauss_every: int = 0
+    fixed_axes: int = 0        # bit a: both faces of axis a Fixed (frozen shell), else periodic
 
     @property
     def nsc(self) -> int:

@@ -114,8 +114,16 @@ Run configure(const std::string& root)
     r.an.fields = inum(L, 9, 0, lat) != 0;
     r.an.energy = inum(L, 10, 0, lat) != 0;
     r.an.gauss = inum(L, 11, 0, lat) != 0;
-    for (int k = 0; k < 6; k++)
-        if (inum(L, 12, k, lat) != 3) throw std::runtime_error("only periodic faces (type 3) run on the GPU");
+    // faces (-x) (+x) (-y) (+y) (-z) (+z): per axis both periodic (3) or both Fixed (1)
+    // (Core/Source/Lattice.cpp:217-258 requires periodic faces in pairs)
+    for (int a = 0; a < 3; a++) {
+        const int lo = inum(L, 12, 2 * a, lat), hi = inum(L, 12, 2 * a + 1, lat);
+        if (lo == 1 && hi == 1)
+            c.fixed_axes |= 1 << a;
+        else if (lo != 3 || hi != 3)
+            throw std::runtime_error("faces of axis " + std::to_string(a) +
+                                     ": only periodic (3 3) or Fixed (1 1) pairs run on the GPU");
+    }
     if (nvec != 5) throw std::runtime_error("only the quaternion link representation (5 components) runs on the GPU");
 
     // Core/Config/Model.cfg (Core/Source/Model.cpp:173-221)
@@ -384,8 +392,8 @@ int main(int argc, char** argv)
                         "apply_norm %d energy_offset %.17g\n",
                         c.m12i, c.l4m5, c.l5i, c.l6i, c.l7i, c.break_son, c.break_uhalfn, c.apply_norm,
                         c.energy_offset);
-            std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s\n", c.energy_every, c.gauss_every,
-                        r.an.energy_path.c_str(), r.an.gauss_path.c_str());
+            std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s fixed_axes %d\n", c.energy_every,
+                        c.gauss_every, r.an.energy_path.c_str(), r.an.gauss_path.c_str(), c.fixed_axes);
             return 0;
         }
         if (ic.empty() && seed < 0) throw std::runtime_error("give --ic FILE or --device-ic SEED");

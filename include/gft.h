@@ -81,6 +81,10 @@ typedef struct gft_config {
     double energy_offset;
     int energy_every;              /* Analysers/Config/Energy.cfg output frequency; 0 = no Energy analyser */
     int gauss_every;               /* Analysers/Config/GaugeCondition.cfg frequency; 0 = off */
+    int fixed_axes;                /* Core/Config/Lattice.cfg face types: bit a set = both faces of axis a
+                                      are Fixed (type 1), clear = periodic (type 3).  Sites on a Fixed
+                                      face are not evolved and not counted by the analysers
+                                      (BoundaryConditions/Source/Fixed.cpp:159-251, Core/Source/Lattice.cpp:217-306). */
 } gft_config;
 
 /* One row of global observables (Analysers/Source/Energy.cpp:169-220,
@@ -204,7 +208,8 @@ int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes
  * The first call on a device looks up that array's address (do it before any
  * stream capture); calls that overlap on the GPU share the array and race, so
  * the caller serialises them.  Only cfg's lattice, model and coupling fields
- * are read (form and storage_bytes are ignored). */
+ * are read (form and storage_bytes are ignored); periodic lattices only
+ * (fixed_axes != 0 returns GFT_E_UNSUPPORTED). */
 int gft_observe_static(const gft_config* cfg, const float* d_scalars, const float* d_vectors, int time_iter,
                        double* d_out, void* stream);
 

@@ -453,6 +453,16 @@ static void loop_constraint(const ctx_t* m, const S* x_now, const S* x_fut, cons
 
 static long long wrap(long long v, long long n) { return ((v % n) + n) % n; }
 
+/* A site on a Fixed face: Fixed::evolve does nothing there and no analyser
+ * visits it (BoundaryConditions/Source/Fixed.cpp:159-251; a region touching a
+ * Fixed face is Fixed, Core/Source/Lattice.cpp:292-306). */
+static int frozen(const ctx_t* m, long long x, long long y, long long z)
+{
+    const int f = m->cfg->fixed_axes;
+    return ((f & 1) && (x == 0 || x == m->nx - 1)) || ((f & 2) && (y == 0 || y == m->ny - 1)) ||
+           ((f & 4) && (z == 0 || z == m->nz - 1));
+}
+
 static long long site_index(const ctx_t* m, long long x, long long y, long long z)
 {
     return (x * m->ny + y) * m->nz + z;
@@ -608,9 +618,12 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
         double dsum[6] = {0, 0, 0, 0, 0, 0};
         double plaq2 = 0.0, plaq1 = 0.0, phisq = 0.0;
 
+        long long nevolved = 0;
         for (long long oi = 0; oi < N; oi++) {
             long long idx = order[oi];
             long long x = idx / (m.ny * m.nz), y = (idx / m.nz) % m.ny, z = idx % m.nz;
+            if (frozen(&m, x, y, z)) continue;
+            nevolved++;
             stencil_t st;
             build_stencil(&m, sc_now, ve_now, x, y, z, &st);
             S* s_now = sc_now + idx * nsc;
@@ -668,9 +681,10 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             row.magnetic = dsum[4] * dv;
             row.electric = dsum[5] * dv;
             for (int k = 0; k < 6; k++) row.ref_energy[k] = (double)ref_sum[k];
-            row.plaq_su2 = plaq2 / (3.0 * (double)N);
-            row.plaq_u1 = plaq1 / (3.0 * (double)N);
-            row.phi_sq = phisq / (double)N;
+            const double ne = nevolved > 0 ? (double)nevolved : 1.0;
+            row.plaq_su2 = plaq2 / (3.0 * ne);
+            row.plaq_u1 = plaq1 / (3.0 * ne);
+            row.phi_sq = phisq / ne;
         }
 
         if (do_gauss) {
@@ -680,6 +694,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             for (long long oi = 0; oi < N; oi++) {
                 long long idx = order[oi];
                 long long x = idx / (m.ny * m.nz), y = (idx / m.nz) % m.ny, z = idx % m.nz;
+                if (frozen(&m, x, y, z)) continue;
                 long long p[3] = {x, y, z}, n[3] = {m.nx, m.ny, m.nz};
                 const S* xm_now[3];
                 const S* xm_fut[3];

@@ -50,6 +50,11 @@ typedef struct orc_config {
     double energy_offset;
     /* Analysers/Config/Energy.cfg and GaugeCondition.cfg output frequencies; 0 = analyser off */
     int energy_every, gauss_every;
+    /* Core/Config/Lattice.cfg face types: bit a set = both faces of axis a are
+     * Fixed (type 1; Core/Source/Lattice.cpp:217-300 pairs faces per axis),
+     * clear = periodic.  Sites on a Fixed face are not evolved and are not part
+     * of the analysers' domain (BoundaryConditions/Source/Fixed.cpp:159-251). */
+    int fixed_axes;
 } orc_config;
 
 /* One row of global observables, written on every step where an analyser logs.

@@ -47,6 +47,7 @@ class OrcConfig(ctypes.Structure):
         ("break_son", ctypes.c_int), ("break_uhalfn", ctypes.c_int), ("apply_norm", ctypes.c_int),
         ("energy_offset", ctypes.c_double),
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
+        ("fixed_axes", ctypes.c_int),
     ]
 
 
@@ -103,6 +104,7 @@ class Params:
     energy_offset: float = 0.0
     energy_every: int = 0
     gauss_every: int = 0
+    fixed_axes: int = 0        # bit a: both faces of axis a Fixed (else periodic)
 
     @property
     def nsc(self) -> int:

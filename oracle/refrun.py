@@ -90,7 +90,8 @@ def write_configs(work: str, p: orc.Params, nt: int) -> None:
         "all faces periodic",
         "(-x) (+x) (-y) (+y) (-z) (+z)",
         "in this order",
-        "faces                          : 3 3 3 3 3 3",
+        "faces                          : " + " ".join("1 1" if (p.fixed_axes >> a) & 1 else "3 3"
+                                                         for a in range(3)),
         "",
         "progress reports               : 0",
         "report frequency               : 1000000",

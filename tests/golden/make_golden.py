@@ -46,6 +46,11 @@ CASES = {
                           dict(seed=17, mean=[0.0] * 8, sigma=[0.1] * 8), 10, ("f32", "f64")),
     "2hdm_wall_4x4x12": (dict(model=orc.MODEL_2HDM, nx=4, ny=4, nz=12, energy_every=4, gauss_every=4),
                          dict(seed=18, mean=[0.0] * 8, sigma=[0.05] * 8, wall_width=2.0, wall_value=1.0), 8, ("f64",)),
+    # Fixed faces on x and z (Lattice.cfg face types 1 1 3 3 1 1): a frozen shell, analysers over the rest
+    "sm_fixed_xz_6x5x7": (dict(model=orc.MODEL_SM, nx=6, ny=5, nz=7, energy_every=2, gauss_every=3, fixed_axes=5),
+                          dict(seed=19, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
+    "2hdm_fixed_y_5x6x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=6, nz=4, energy_every=2, gauss_every=2, fixed_axes=2),
+                           dict(seed=20, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 6, ("f32",)),
 }
 
 

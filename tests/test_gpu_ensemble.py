@@ -147,3 +147,26 @@ def test_device_initial_data_per_member_matches_evolver(oracle_mod):
             ev.init_fields(InitialData(**ic))
             sc, ve = ev.download()
         assert np.array_equal(got[m][0], sc) and np.array_equal(got[m][1], ve)
+
+
+def test_member_with_fixed_faces_evolves_like_a_single_handle(oracle_mod):
+    """A member with Fixed y faces (frozen shell) next to a periodic one."""
+    import dataclasses
+
+    from gftevolver_b200 import Ensemble, InitialData
+    ps, ics = _members(oracle_mod, 1, [(16, 16, 32), (8, 16, 16)])
+    ps[1] = dataclasses.replace(ps[1], fixed_axes=2)
+    with Ensemble(ps) as ens:
+        ens.set_kernel(3, 8)
+        ens.init_fields([InitialData(**ic) for ic in ics])
+        rows = ens.evolve(7)
+        out = [ens.download(m) for m in range(len(ps))]
+    for m, (p, ic) in enumerate(zip(ps, ics)):
+        sc, ve, r1 = _single(p, ic, 7, 3, 8)
+        assert np.max(np.abs(out[m][0] - sc)) <= 2e-6 and np.max(np.abs(out[m][1] - ve)) <= 2e-6
+        _compare_rows(rows[m], r1, p.nsite)
+    # the frozen shell kept its initial values
+    with Ensemble(ps[1:]) as one:
+        one.init_fields([InitialData(**ics[1])])
+        init = one.download(0)
+    assert np.array_equal(out[1][0][:, :, 0], init[0][:, :, 0]) and np.array_equal(out[1][1][:, :, -1], init[1][:, :, -1])

@@ -97,11 +97,13 @@ def test_fp64_forms_match_reference_golden(path, form, tol):
 
 
 @pytest.mark.parametrize("model", [1, 2], ids=["sm", "2hdm"])
-@pytest.mark.parametrize("shape", [(8, 8, 8), (5, 6, 7), (16, 12, 33)])
-def test_forms_vs_oracle_random(oracle_mod, model, shape):
-    """Random links and Gaussian scalars, 10 steps, all forms against the oracle."""
+@pytest.mark.parametrize("shape,fixed", [((8, 8, 8), 0), ((5, 6, 7), 0), ((16, 12, 33), 0), ((8, 8, 32), 5),
+                                         ((7, 8, 32), 7)])
+def test_forms_vs_oracle_random(oracle_mod, model, shape, fixed):
+    """Random links and Gaussian scalars, 10 steps, all forms against the oracle
+    (periodic, and with Fixed faces on x and z or on every axis: a frozen shell)."""
     nx, ny, nz = shape
-    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=5, gauss_every=5)
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=5, gauss_every=5, fixed_axes=fixed)
     ic = oracle_mod.ICSpec(seed=1234 + nx, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8,
                            theta_sigma=0.1, eps_sigma=0.1)
     p = _lp(op.__dict__)

@@ -17,10 +17,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _setup(oracle_mod, model, shape, seed=31):
+def _setup(oracle_mod, model, shape, seed=31, fixed_axes=0):
     from gftevolver_b200 import LatticeParams
     nx, ny, nz = shape
-    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=3, gauss_every=3)
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=3, gauss_every=3, fixed_axes=fixed_axes)
     ic = oracle_mod.ICSpec(seed=seed, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                            eps_sigma=0.1)
     sc, ve = oracle_mod.init_fields(op, ic, np.float32)
@@ -52,8 +52,9 @@ def _maxdiff(a, b):
     ((10, 32, 48), 3, 6),     # 16 x 16 tiles
     ((4, 16, 16), 3, 32),     # 16 x 16, one tile per plane
 ])
-def test_tiled_matches_global_kernel(oracle_mod, model, shape, tile, march):
-    op, p, sc, ve = _setup(oracle_mod, model, shape)
+@pytest.mark.parametrize("fixed_axes", [0, 3], ids=["periodic", "fixed_xy"])
+def test_tiled_matches_global_kernel(oracle_mod, model, shape, tile, march, fixed_axes):
+    op, p, sc, ve = _setup(oracle_mod, model, shape, fixed_axes=fixed_axes)
     g1 = _run(p, sc, ve, 1, kind=1)
     t1 = _run(p, sc, ve, 1, kind=2, tile=tile, march=march)
     assert _maxdiff(t1[0], g1[0]) <= 2.4e-7 and _maxdiff(t1[1], g1[1]) <= 2.4e-7

@@ -30,9 +30,9 @@ def gft_run():
     return GFT_RUN
 
 
-def _params(orc, model):
+def _params(orc, model, fixed_axes=0):
     return orc.Params(model=model, nx=6, ny=5, nz=8, dt=0.05, damping=0.3, nt_damped=2, energy_every=2,
-                      gauss_every=3, g=0.61, gp=0.33)
+                      gauss_every=3, g=0.61, gp=0.33, fixed_axes=fixed_axes)
 
 
 @pytest.mark.parametrize("model", [1, 2])
@@ -47,7 +47,7 @@ def test_config_tree_is_parsed_like_the_reference(tmp_path, oracle_mod, gft_run,
     assert (int(kv["nx"]), int(kv["ny"]), int(kv["nz"])) == (6, 5, 8)
     assert float(kv["dt"]) == 0.05 and float(kv["g"]) == 0.61 and float(kv["gp"]) == 0.33
     assert float(kv["damping"]) == float(np.float32(0.3)) and int(kv["nt_damped"]) == 2
-    assert int(kv["energy_every"]) == 2 and int(kv["gauss_every"]) == 3
+    assert int(kv["energy_every"]) == 2 and int(kv["gauss_every"]) == 3 and int(kv["fixed_axes"]) == 0
     if model == 1:
         assert float(kv["lambda"]) == p.lam and float(kv["eta_sqr"]) == p.eta_sqr
     else:
@@ -60,9 +60,17 @@ def test_unsupported_reference_configuration_is_refused(tmp_path, oracle_mod, gf
     refrun.write_configs(str(tmp_path), p, 7)
     lat = tmp_path / "Core" / "Config" / "Lattice.cfg"
     lat.write_text(lat.read_text().replace("faces                          : 3 3 3 3 3 3",
-                                           "faces                          : 1 1 3 3 3 3"))
+                                           "faces                          : 1 3 3 3 3 3"))
     r = subprocess.run([gft_run, str(tmp_path), "--print-config"], capture_output=True, text=True)
-    assert r.returncode == 1 and "periodic" in r.stderr
+    assert r.returncode == 1 and "pairs" in r.stderr
+
+
+def test_fixed_faces_are_parsed(tmp_path, oracle_mod, gft_run):
+    from oracle import refrun
+    refrun.write_configs(str(tmp_path), _params(oracle_mod, 1, fixed_axes=5), 7)
+    out = subprocess.run([gft_run, str(tmp_path), "--print-config"], capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert out[out.index("fixed_axes") + 1] == "5"
 
 
 def _numbers(path):
@@ -70,12 +78,12 @@ def _numbers(path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("model", [1, 2])
-def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_run, model):
+@pytest.mark.parametrize("model,fixed_axes", [(1, 0), (2, 0), (1, 5)])
+def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_run, model, fixed_axes):
     from oracle import refrun
     if not refrun.available(False):
         pytest.skip("oracle/_ref/ref32 not built")
-    p = _params(oracle_mod, model)
+    p = _params(oracle_mod, model, fixed_axes)
     ic = oracle_mod.ICSpec(seed=5, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                            eps_sigma=0.1)
     sc, ve = oracle_mod.init_fields(p, ic, np.float32)
