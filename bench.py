@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 precision run (0: skip)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other benchmark configurations (SM 32^3 FP64, 2HDM 192^3, 2HDM 448^3 wall)")
     ap.add_argument("--slab", action="store_true",
                     help="N = 1: run the x-slab path (ghost planes refreshed by the exchange callback) on one GPU")
     ap.add_argument("--ensemble-steps", type=int, default=500,
@@ -342,6 +344,73 @@ def ensemble_report(steps: int, device: int) -> dict:
 
 
 # ---------------------------------------------------------------------------
+# The other benchmark configurations, measured at their own sizes
+# ---------------------------------------------------------------------------
+def _timed_config(p, ic, form, steps, device):
+    import torch
+
+    from gftevolver_b200 import Evolver
+    ev = Evolver(p, form=form, device=device)
+    ev.init_fields(ic)
+    ev.evolve(3)
+    ev.step_kernel_ms()
+    st = torch.cuda.ExternalStream(ev.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    rows = ev.evolve(steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kms, _ = ev.step_kernel_ms()
+    name = ev.step_kernel_name
+    ev.close()
+    sbytes = 8 if form in ("fp64", "ref64") else 4
+    model = "sm" if p.model == 1 else "2hdm"
+    balg = B_ALG[(model, sbytes)]
+    peak = measured_peaks()[0]
+    e = [r for r in rows if r["has_energy"]]
+    g = [max(r["gauss_max"]) for r in rows if r["has_gauss"]]
+    return {
+        "form": form, "steps": steps, "value": p.nsite * steps / (ms / 1e3), "unit": "site-updates/s",
+        "ms_per_step": ms / steps, "kernel": name, "step_kernel_ms": kms,
+        "roofline_frac": balg * p.nsite / (kms / 1e3) / 1e9 / peak if kms > 0 else None,
+        "energy_first": e[0]["energy"] if e else None, "energy_last": e[-1]["energy"] if e else None,
+        "gauss_max": max(g) if g else None, "plaq_su2_last": e[-1]["plaq_su2"] if e else None,
+    }
+
+
+def configs_report(device: int) -> dict:
+    """SM 32^3 FP64 identity links (1000 steps); 2HDM 192^3 FP64 and mixed (100 of the 500
+    steps, which the timing does not depend on); 2HDM 448^3 mixed bubble wall (2000 steps,
+    analysers every 50).  Initial data are generated on the device from fixed seeds."""
+    import dataclasses
+
+    from gftevolver_b200 import InitialData
+    out = {}
+    p, _ = workload_params("sm", 32)
+    ic = InitialData(seed=7, mean=[0.0] * 8, sigma=[0.1] * 8)  # identity links, Higgs N(0, 0.1^2)
+    r = _timed_config(p, ic, "fp64", 1000, device)
+    r["workload"] = "SM 32^3 FP64, identity links, Higgs N(0,0.1^2), dt=0.05, analysers every 10"
+    out["sm_32_fp64"] = r
+    p, ic = workload_params("2hdm", 192)
+    for form in ("fp64", "mixed"):
+        r = _timed_config(p, ic, form, 100, device)
+        r["workload"] = ("2HDM 192^3, m11^2=m22^2=-0.5, m12^2=0.1, l1=l2=0.13, l3=0.2, l4=l5=-0.05, random links, "
+                         "doublets N(0.7,0.1^2), dt=0.05")
+        out[f"2hdm_192_{form}"] = r
+    out["2hdm_192_mixed"]["mixed_over_fp64"] = out["2hdm_192_mixed"]["value"] / out["2hdm_192_fp64"]["value"]
+    p, _ = workload_params("2hdm", 448)
+    p = dataclasses.replace(p, energy_every=50, gauss_every=50)
+    ic = InitialData(seed=5, mean=[0.0] * 8, sigma=[0.05] * 8, wall_width=5.0, wall_value=1.0)
+    r = _timed_config(p, ic, "mixed", 2000, device)
+    r["workload"] = ("2HDM 448^3 mixed, doublet 1 component 0 a periodic tanh double wall along z (width 5, "
+                     "value 1) + N(0,0.05^2), doublet 2 N(0,0.05^2), identity links, dt=0.05, analysers every 50")
+    out["2hdm_448_wall_mixed"] = r
+    return out
+
+
+# ---------------------------------------------------------------------------
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -486,6 +555,9 @@ def main():
     ensemble = None
     if args.ensemble_steps > 0 and world == 1:
         ensemble = ensemble_report(args.ensemble_steps, local)
+    configs = None
+    if not args.no_configs and world == 1 and args.size == 256 and args.model == "sm":
+        configs = configs_report(local)
 
     peak, peak_kind = measured_peaks()
     achieved = balg * p.nsite / (kms / 1e3) / 1e9
@@ -522,6 +594,7 @@ def main():
         "cpu_baseline": cpu,
         "precision": precision,
         "ensemble": ensemble,
+        "configs": configs,
         "analyser_rows": len(rows),
     }
     print(json.dumps(line), flush=True)

@@ -219,9 +219,14 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
     return true;
 }
 
+// Automatic choice (kernel_kind 0), from B200 measurements at 192^3-448^3: the
+// tiled kernel for SM (46 % of HBM against 42 % for one thread per site);
+// one thread per site for 2HDM, whose four staged plane buffers (two doublets)
+// need 130 KB of shared memory and leave one CTA per SM (30 % against 45 %).
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
     if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1) return false;
+    if (h->kernel_kind == 0 && h->cfg.model != GFT_MODEL_SM) return false;
     return tiled_supported(P, h->tile_variant);
 }
 

@@ -214,7 +214,7 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
                        double* d_out, void* stream);
 
 /* Step-kernel selection for the throughput forms (no reference counterpart):
- * kind 0 = automatic (the tiled kernel for the mixed form when the lattice
+ * kind 0 = automatic (the tiled kernel for the SM mixed form when the lattice
  * divides into a built tile, else the one-thread-per-site kernel), 1 = one
  * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
  * marching along x (mixed form).  tile = tile shape (0: 8 x 32, 1: 4 x 32,

@@ -236,6 +236,11 @@ def test_step_kernel_name_follows_form_and_shape(oracle_mod):
     odd = oracle_mod.Params(nx=5, ny=3, nz=7)
     with Evolver(_lp(odd.__dict__), form="mixed") as ev:
         assert ev.step_kernel_name == "fast_step_kernel"
+    two = oracle_mod.Params(model=2, nx=8, ny=8, nz=32)  # 2HDM: one thread per site unless asked
+    with Evolver(_lp(two.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
+        ev.set_kernel(2, 0, 32)
+        assert ev.step_kernel_name == "tiled_step_kernel"
 
 
 @pytest.mark.parametrize("form", ["mixed", "fp64", "ref32"])
