@@ -72,20 +72,25 @@ class DistTransport:
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
+        self._ops = {}  # the operation list per set of plane tensors (they are fixed views)
 
     def _global(self, r: int) -> int:
         return r if self.group is None else self.dist.get_global_rank(self.group, r)
 
     def exchange(self, send_lo, send_hi, recv_lo, recv_hi) -> None:
         dist = self.dist
-        left = self._global((self.rank - 1) % self.world)
-        right = self._global((self.rank + 1) % self.world)
-        ops = []
-        for k in range(len(send_lo)):
-            ops.append(dist.P2POp(dist.isend, send_lo[k], left, self.group))
-            ops.append(dist.P2POp(dist.irecv, recv_hi[k], right, self.group))
-            ops.append(dist.P2POp(dist.isend, send_hi[k], right, self.group))
-            ops.append(dist.P2POp(dist.irecv, recv_lo[k], left, self.group))
+        key = tuple(t.data_ptr() for t in (*send_lo, *recv_lo))
+        ops = self._ops.get(key)
+        if ops is None:
+            left = self._global((self.rank - 1) % self.world)
+            right = self._global((self.rank + 1) % self.world)
+            ops = []
+            for k in range(len(send_lo)):
+                ops.append(dist.P2POp(dist.isend, send_lo[k], left, self.group))
+                ops.append(dist.P2POp(dist.irecv, recv_hi[k], right, self.group))
+                ops.append(dist.P2POp(dist.isend, send_hi[k], right, self.group))
+                ops.append(dist.P2POp(dist.irecv, recv_lo[k], left, self.group))
+            self._ops[key] = ops
         for req in dist.batch_isend_irecv(ops):
             req.wait()
 
