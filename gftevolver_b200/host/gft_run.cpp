@@ -16,19 +16,25 @@
 // them: a fixed number of description lines, then one entry per line whose
 // values follow the last ':' of the line.
 //
-// Initial data: --ic FILE (both time levels in the reference layout, float for
-// the ref32 / mixed forms, double for ref64 / fp64), or --device-ic SEED
-// (gft_init_fields: Higgs N(1, 0.1^2) per component, random links with
-// eps, theta_Y ~ N(0, 0.1^2)); the reference's own RandomUniform generator is
-// not restated.
+// Initial data: by default the configured one, built as the reference builds it
+// (Lattice.cfg initial-condition types: 0 = zero scalars and identity links,
+// 1 = RandomUniform from InitialConditions/Config/RandomUniform.cfg, a
+// std::mt19937 stream per array); or --ic FILE (both time levels in the
+// reference layout, float for the ref32 / mixed forms, double for ref64 / fp64);
+// or --device-ic SEED (gft_init_fields: Higgs N(1, 0.1^2) per component, random
+// links with eps, theta_Y ~ N(0, 0.1^2)).
 //
 // Usage: gft_run ROOT [--form ref32|ref64|fp64|mixed] [--ic FILE | --device-ic SEED]
-//                     [--device N] [--final-bin FILE] [--print-config]
+//                     [--device N] [--initial-bin FILE [--initial-only]] [--final-bin FILE]
+//                     [--print-config]
+// --initial-only writes the host-built initial data to --initial-bin and exits
+// without opening a device.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <random>
 #include <iostream>
 #include <sstream>
 #include <stdexcept>
@@ -84,10 +90,21 @@ struct Analysers {
     std::string fields_initial_path, fields_continual_path, fields_final_path;
 };
 
+// The reference's configured initial condition (Core/Source/Lattice.cpp:172-215, 358-401):
+// type 0 = zero scalars / identity links, type 1 = RandomUniform
+// (InitialConditions/Source/RandomUniform.cpp:60-77).
+struct RefIC {
+    int type[2] = {0, 0};
+    unsigned seed = 0;
+    float lo = 0.f, hi = 0.f;  // parsed as float, as RandomUniform.cpp:28 reads them
+    bool equal = false;
+};
+
 struct Run {
     gft_config cfg{};
     int nt = 0;
     Analysers an;
+    RefIC ic;
 };
 
 Run configure(const std::string& root)
@@ -110,6 +127,16 @@ Run configure(const std::string& root)
     if (inum(L, 6, 0, lat)) {  // nt from light-crossing times (Lattice.cpp:78-87)
         const float crossings = (float)num(L, 7, 0, lat);
         r.nt = static_cast<int>(crossings * static_cast<float>(c.nx) * c.dx / (2 * c.dt));
+    }
+    r.ic.type[0] = inum(L, 8, 0, lat);
+    r.ic.type[1] = inum(L, 8, 1, lat);
+    if (r.ic.type[0] == 1 || r.ic.type[1] == 1) {
+        const std::string rf = root + "/InitialConditions/Config/RandomUniform.cfg";
+        const Entries R = read_cfg(rf, 12);
+        r.ic.seed = (unsigned)std::stoul(tok(R, 0, 0, rf));
+        r.ic.lo = std::stof(tok(R, 1, 0, rf));
+        r.ic.hi = std::stof(tok(R, 1, 1, rf));
+        r.ic.equal = inum(R, 2, 0, rf) != 0;
     }
     r.an.fields = inum(L, 9, 0, lat) != 0;
     r.an.energy = inum(L, 10, 0, lat) != 0;
@@ -247,12 +274,65 @@ void dump_fields(const std::string& path, const std::vector<T>& sc, const std::v
     }
 }
 
+// RandomUniform::setInitialFields: one std::mt19937 stream per field array from
+// the configured seed, float uniform in [lo, hi) as the reference stores it
+// (widened exactly for the FP64 forms), both time levels equal when asked.
 template <class T>
-int run(const std::string& root, Run& r, const std::string& ic_path, long long seed, const std::string& final_bin)
+void random_uniform(std::vector<T>& field, const RefIC& ic)
+{
+    std::mt19937 generator(ic.seed);
+    std::uniform_real_distribution<float> distribution(ic.lo, ic.hi);
+    size_t n = field.size();
+    if (ic.equal) n /= 2;
+    for (size_t i = 0; i < n; i++) {
+        field[i] = (T)distribution(generator);
+        if (ic.equal) field[i + n] = field[i];
+    }
+}
+
+template <class T>
+void write_bin(const std::string& path, const std::vector<T>& sc, const std::vector<T>& ve)
+{
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(sc.data()), sc.size() * sizeof(T));
+    f.write(reinterpret_cast<const char*>(ve.data()), ve.size() * sizeof(T));
+    if (!f) throw std::runtime_error("cannot write " + path);
+}
+
+// Host-side initial data: the --ic file, or the configured initial condition
+// built as the reference builds it.  Both time levels, reference layout.
+template <class T>
+void host_initial(const Run& r, const std::string& ic_path, std::vector<T>& sc, std::vector<T>& ve)
+{
+    if (!ic_path.empty()) {
+        std::ifstream f(ic_path, std::ios::binary);
+        f.read(reinterpret_cast<char*>(sc.data()), sc.size() * sizeof(T));
+        f.read(reinterpret_cast<char*>(ve.data()), ve.size() * sizeof(T));
+        if (!f) throw std::runtime_error("short initial-data file " + ic_path);
+        return;
+    }
+    std::fill(sc.begin(), sc.end(), (T)0);
+    std::fill(ve.begin(), ve.end(), (T)0);
+    for (size_t s = 0; s < ve.size() / 15; s++)
+        for (int d = 0; d < 3; d++) ve[s * 15 + d * 5 + 1] = (T)1;  // identity SU(2) links
+    if (r.ic.type[0] == 1) random_uniform(sc, r.ic);
+    if (r.ic.type[1] == 1) random_uniform(ve, r.ic);
+}
+
+template <class T>
+int run(const std::string& root, Run& r, const std::string& ic_path, long long seed, const std::string& final_bin,
+        const std::string& initial_bin, bool initial_only)
 {
     gft_config& c = r.cfg;
     const int nsc = (c.model == GFT_MODEL_SM) ? 4 : 8;
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
+    std::vector<T> sc(2 * nsite * nsc), ve(2 * nsite * 15);
+    if (initial_only) {  // the host-built initial data alone, no device
+        if (seed >= 0) throw std::runtime_error("--initial-only builds host initial data; drop --device-ic");
+        host_initial(r, ic_path, sc, ve);
+        write_bin(initial_bin, sc, ve);
+        return 0;
+    }
     const std::string data = root + "/Data";
     mkdir(data.c_str(), 0755);
     if (!r.an.fields_continual_path.empty()) {
@@ -262,18 +342,14 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
 
     gft_handle* h = nullptr;
     check(gft_create(&c, &h), nullptr, "gft_create");
-    std::vector<T> sc(2 * nsite * nsc), ve(2 * nsite * 15);
     auto download = [&]() {
         if constexpr (sizeof(T) == 4)
             check(gft_download_f32(h, sc.data(), ve.data()), h, "gft_download");
         else
             check(gft_download_f64(h, sc.data(), ve.data()), h, "gft_download");
     };
-    if (!ic_path.empty()) {
-        std::ifstream f(ic_path, std::ios::binary);
-        f.read(reinterpret_cast<char*>(sc.data()), sc.size() * sizeof(T));
-        f.read(reinterpret_cast<char*>(ve.data()), ve.size() * sizeof(T));
-        if (!f) throw std::runtime_error("short initial-data file " + ic_path);
+    if (seed < 0) {
+        host_initial(r, ic_path, sc, ve);
         if constexpr (sizeof(T) == 4)
             check(gft_upload_f32(h, sc.data(), ve.data(), 0), h, "gft_upload");
         else
@@ -291,10 +367,9 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
     }
 
     // initialAnalysis
-    if (r.an.fields && r.an.fields_initial) {
-        download();
-        dump_fields(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
-    }
+    if ((r.an.fields && r.an.fields_initial) || !initial_bin.empty()) download();
+    if (r.an.fields && r.an.fields_initial) dump_fields(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
+    if (!initial_bin.empty()) write_bin(initial_bin, sc, ve);
 
     // evolve: chunks end where OutputFields writes a continual dump
     const int chunk_max = (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0) ? r.an.fields_freq : 1000;
@@ -349,15 +424,15 @@ int main(int argc, char** argv)
 {
     if (argc < 2) {
         std::cerr << "usage: gft_run ROOT [--form ref32|ref64|fp64|mixed] [--ic FILE | --device-ic SEED] "
-                     "[--device N] [--final-bin FILE] [--print-config]\n";
+                     "[--device N] [--initial-bin FILE [--initial-only]] [--final-bin FILE] [--print-config]\n";
         return 2;
     }
     try {
         const std::string root = argv[1];
-        std::string form = "mixed", ic, final_bin;
+        std::string form = "mixed", ic, final_bin, initial_bin;
         long long seed = -1;
         int device = 0;
-        bool print = false;
+        bool print = false, initial_only = false;
         for (int i = 2; i < argc; i++) {
             const std::string a = argv[i];
             auto next = [&]() -> std::string {
@@ -369,6 +444,8 @@ int main(int argc, char** argv)
             else if (a == "--device-ic") seed = std::stoll(next());
             else if (a == "--device") device = std::stoi(next());
             else if (a == "--final-bin") final_bin = next();
+            else if (a == "--initial-bin") initial_bin = next();
+            else if (a == "--initial-only") initial_only = true;
             else if (a == "--print-config") print = true;
             else throw std::runtime_error("unknown option " + a);
         }
@@ -394,10 +471,13 @@ int main(int argc, char** argv)
                         c.energy_offset);
             std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s fixed_axes %d\n", c.energy_every,
                         c.gauss_every, r.an.energy_path.c_str(), r.an.gauss_path.c_str(), c.fixed_axes);
+            std::printf("ic_scalar %d ic_gauge %d ic_seed %u ic_min %.9g ic_max %.9g ic_equal %d\n", r.ic.type[0],
+                        r.ic.type[1], r.ic.seed, r.ic.lo, r.ic.hi, (int)r.ic.equal);
             return 0;
         }
-        if (ic.empty() && seed < 0) throw std::runtime_error("give --ic FILE or --device-ic SEED");
-        return f64 ? run<double>(root, r, ic, seed, final_bin) : run<float>(root, r, ic, seed, final_bin);
+        if (initial_only && initial_bin.empty()) throw std::runtime_error("--initial-only needs --initial-bin FILE");
+        return f64 ? run<double>(root, r, ic, seed, final_bin, initial_bin, initial_only)
+                   : run<float>(root, r, ic, seed, final_bin, initial_bin, initial_only);
     } catch (const std::exception& e) {
         std::cerr << "Error in " << e.what() << std::endl;
         return 1;

@@ -75,15 +75,22 @@ int main()
 
         Lattice lattice;
 
-        // Initial data from ic.bin replaces the (zero) configured initial condition.
+        // Initial data from ic.bin, when given, replaces the configured initial
+        // condition; without it the configured one (Lattice.cfg types) stands.
         {
             std::ifstream ic(work + "/ic.bin", std::ios::binary);
-            if (!ic) throw std::runtime_error("ref_harness: cannot open ic.bin");
-            ic.read(reinterpret_cast<char*>(lattice.scalarFields.data()),
-                    (std::streamsize)(lattice.scalarFields.size() * sizeof(word_t)));
-            ic.read(reinterpret_cast<char*>(lattice.vectorFields.data()),
-                    (std::streamsize)(lattice.vectorFields.size() * sizeof(word_t)));
-            if (!ic) throw std::runtime_error("ref_harness: ic.bin is shorter than the configured lattice");
+            if (ic) {
+                ic.read(reinterpret_cast<char*>(lattice.scalarFields.data()),
+                        (std::streamsize)(lattice.scalarFields.size() * sizeof(word_t)));
+                ic.read(reinterpret_cast<char*>(lattice.vectorFields.data()),
+                        (std::streamsize)(lattice.vectorFields.size() * sizeof(word_t)));
+                if (!ic) throw std::runtime_error("ref_harness: ic.bin is shorter than the configured lattice");
+            }
+            std::ofstream fi(work + "/initial.bin", std::ios::binary);
+            fi.write(reinterpret_cast<const char*>(lattice.scalarFields.data()),
+                     (std::streamsize)(lattice.scalarFields.size() * sizeof(word_t)));
+            fi.write(reinterpret_cast<const char*>(lattice.vectorFields.data()),
+                     (std::streamsize)(lattice.vectorFields.size() * sizeof(word_t)));
         }
 
         CaptureAnalyser* cap = new CaptureAnalyser();

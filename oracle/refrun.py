@@ -57,7 +57,9 @@ def _write(path: str, lines: list[str]) -> None:
         f.write("\n".join(lines) + "\n")
 
 
-def write_configs(work: str, p: orc.Params, nt: int) -> None:
+def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1)) -> None:
+    """ic_types: Lattice.cfg initial-condition types (0 zero / identity links, 1 RandomUniform);
+    random_uniform: InitialConditions/Config/RandomUniform.cfg (seed, min, max, equal time levels)."""
     sm = p.model == orc.MODEL_SM
     # Core/Config/Lattice.cfg -- Lattice::configure (Lattice.cpp:47-143)
     lat = _header(10, "Lattice")
@@ -77,7 +79,7 @@ def write_configs(work: str, p: orc.Params, nt: int) -> None:
         "initial condition types for",
         "scalar fields and gauge fields",
         "(zero, loaded by the harness)",
-        "types                          : 0 0",
+        f"types                          : {ic_types[0]} {ic_types[1]}",
         "",
         "analysis options",
         "output fields                  : 0",
@@ -97,6 +99,13 @@ def write_configs(work: str, p: orc.Params, nt: int) -> None:
         "report frequency               : 1000000",
     ]
     _write(os.path.join(work, "Core", "Config", "Lattice.cfg"), lat)
+
+    # InitialConditions/Config/RandomUniform.cfg -- RandomUniform::configure (RandomUniform.cpp:14-34)
+    ru = _header(12, "RandomUniform")
+    ru += [f"seed                           : {int(random_uniform[0])}",
+           f"range (min max)                : {_num(random_uniform[1])} {_num(random_uniform[2])}",
+           f"equal time levels              : {int(random_uniform[3])}"]
+    _write(os.path.join(work, "InitialConditions", "Config", "RandomUniform.cfg"), ru)
 
     # Core/Config/Model.cfg -- Model::configure (Model.cpp:173-221)
     mod = _header(11, "Model")
@@ -191,23 +200,33 @@ def write_configs(work: str, p: orc.Params, nt: int) -> None:
     _write(os.path.join(work, "Analysers", "Config", "GaugeCondition.cfg"), ga)
 
 
-def run(p: orc.Params, scalars: np.ndarray, vectors: np.ndarray, nt: int, fp64: bool = False,
-        workdir: str | None = None, timeout: float = 600.0):
-    """Run the reference binary from the given two-level initial data.
+def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, nt: int, fp64: bool = False,
+        workdir: str | None = None, timeout: float = 600.0, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1)):
+    """Run the reference binary from the given two-level initial data, or (scalars
+    None) from its own configured initial condition (ic_types, random_uniform).
 
     Returns (final_scalars, final_vectors, rows, seconds) where rows lists the
     analysers' raw sums per logged step (float in ref32) and seconds is the
-    wall time of Lattice::evolve.
+    wall time of Lattice::evolve.  The initial fields the run started from are
+    left in <workdir>/initial.bin.
     """
     dtype = np.float64 if fp64 else np.float32
     own = workdir is None
     tmp = tempfile.TemporaryDirectory(prefix="gftref_") if own else None
     work = tmp.name if own else workdir
+    given = scalars is not None
+    if not given:
+        scalars = np.zeros((2, p.nx, p.ny, p.nz, p.nsc), dtype)
+        vectors = np.zeros((2, p.nx, p.ny, p.nz, 15), dtype)
     try:
-        write_configs(work, p, nt)
-        with open(os.path.join(work, "ic.bin"), "wb") as f:
-            f.write(np.ascontiguousarray(scalars, dtype=dtype).tobytes())
-            f.write(np.ascontiguousarray(vectors, dtype=dtype).tobytes())
+        write_configs(work, p, nt, ic_types, random_uniform)
+        icp = os.path.join(work, "ic.bin")
+        if given:
+            with open(icp, "wb") as f:
+                f.write(np.ascontiguousarray(scalars, dtype=dtype).tobytes())
+                f.write(np.ascontiguousarray(vectors, dtype=dtype).tobytes())
+        elif os.path.exists(icp):
+            os.remove(icp)
         env = dict(os.environ, GFT_REF_WORKDIR=work)
         t0 = time.perf_counter()
         res = subprocess.run([binary(fp64)], env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,

@@ -105,3 +105,70 @@ def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_r
         tol = 8 * np.spacing(np.maximum(np.abs(g), np.abs(r)))
         assert np.all(np.abs(g.astype(np.float64) - r) <= tol + 1e-30)
         assert np.mean(g != r) <= 0.01
+
+
+@pytest.mark.parametrize("ic_types,random_uniform", [((1, 0), (42, -1.0, 1.0, 1)), ((0, 1), (7, -0.5, 0.25, 0)),
+                                                     ((1, 1), (-3, 0.0, 2.0, 1)), ((0, 0), (42, -1.0, 1.0, 1))])
+@pytest.mark.parametrize("model", [1, 2])
+def test_configured_initial_condition_matches_the_reference(tmp_path, oracle_mod, gft_run, model, ic_types,
+                                                            random_uniform):
+    """Zero scalars / identity links and RandomUniform (Core/Source/Lattice.cpp:358-401,
+    InitialConditions/Source/RandomUniform.cpp:60-77), bit for bit against the
+    initial fields the reference binary built from the same configuration tree."""
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("oracle/_ref/ref32 not built")
+    p = _params(oracle_mod, model)
+    ref_dir = tmp_path / "ref"
+    ref_dir.mkdir()
+    refrun.run(p, None, None, 1, workdir=str(ref_dir), ic_types=ic_types, random_uniform=random_uniform)
+    want = np.fromfile(ref_dir / "initial.bin", dtype=np.float32)
+    out = subprocess.run([gft_run, str(ref_dir), "--print-config"], capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert (int(out[out.index("ic_scalar") + 1]), int(out[out.index("ic_gauge") + 1])) == ic_types
+    for form, dtype in (("ref32", np.float32), ("fp64", np.float64)):
+        path = tmp_path / f"initial_{form}.bin"
+        subprocess.run([gft_run, str(ref_dir), "--form", form, "--initial-bin", str(path), "--initial-only"],
+                       check=True, capture_output=True, text=True)
+        got = np.fromfile(path, dtype=dtype)
+        assert got.size == want.size
+        np.testing.assert_array_equal(got, want.astype(dtype))
+
+
+def test_initial_only_refuses_device_initial_data(tmp_path, oracle_mod, gft_run):
+    from oracle import refrun
+    refrun.write_configs(str(tmp_path), _params(oracle_mod, 1), 7)
+    r = subprocess.run([gft_run, str(tmp_path), "--device-ic", "3", "--initial-bin", str(tmp_path / "x.bin"),
+                        "--initial-only"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--device-ic" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", [1, 2])
+def test_configured_initial_condition_run_matches_the_reference(tmp_path, oracle_mod, gft_run, model):
+    """The whole job from the configured initial condition (RandomUniform scalars,
+    identity links): no initial-data file on either side."""
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("oracle/_ref/ref32 not built")
+    p = _params(oracle_mod, model)
+    ref_dir, gpu_dir = tmp_path / "ref", tmp_path / "gpu"
+    ref_dir.mkdir()
+    r_sc, r_ve, _, _ = refrun.run(p, None, None, 7, workdir=str(ref_dir), ic_types=(1, 0),
+                                  random_uniform=(42, -0.5, 0.5, 1))
+    shutil.copytree(ref_dir, gpu_dir, ignore=shutil.ignore_patterns("Data", "*.bin", "rows.txt", "timing.txt"))
+    subprocess.run([gft_run, str(gpu_dir), "--form", "ref32", "--initial-bin", str(gpu_dir / "initial.bin"),
+                    "--final-bin", str(gpu_dir / "final.bin")], check=True, capture_output=True, text=True)
+    np.testing.assert_array_equal(np.fromfile(gpu_dir / "initial.bin", dtype=np.float32),
+                                  np.fromfile(ref_dir / "initial.bin", dtype=np.float32))
+    for name in ("global_quantities.dat", "global_quantities_gauge.dat"):
+        a, b = _numbers(gpu_dir / "Data" / name), _numbers(ref_dir / "Data" / name)
+        assert len(a) == len(b) and len(a) > 0
+        for ra, rb in zip(a, b):
+            np.testing.assert_allclose(ra, rb, rtol=2e-5, atol=1e-12)
+    raw = np.fromfile(gpu_dir / "final.bin", dtype=np.float32)
+    g_sc, g_ve = raw[:r_sc.size].reshape(r_sc.shape), raw[r_sc.size:].reshape(r_ve.shape)
+    for g, r in ((g_sc, r_sc), (g_ve, r_ve)):
+        tol = 8 * np.spacing(np.maximum(np.abs(g), np.abs(r)))
+        assert np.all(np.abs(g.astype(np.float64) - r) <= tol + 1e-30)
+        assert np.mean(g != r) <= 0.01
