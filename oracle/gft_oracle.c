@@ -13,7 +13,9 @@
  *
  * Layout (Core/Source/Lattice.cpp:358-367, 658-671): two time levels,
  *     scalars[((t*nx + x)*ny + y)*nz + z][nsc]     nsc = 4 (SM) or 8 (2HDM)
- *     vectors[((t*nx + x)*ny + y)*nz + z][15]      per direction d: [theta_Y, c0, c1, c2, c3]
+ *     vectors[((t*nx + x)*ny + y)*nz + z][3*dw]    per direction d: [theta_Y, c0, c1, c2, c3]
+ *                                                  (+ theta_H, or + d0..d3, for the 2HDM
+ *                                                  Higgs-family gauge field: dw = 5, 6 or 9)
  * At step time_iter the "now" level is (time_iter + 1) % 2 and the update is
  * written in place into the other ("past") level (Lattice.cpp:773-774).
  */
@@ -37,14 +39,12 @@ typedef ORC_S S;
 #define ORC_CAT(a, b) ORC_CAT2(a, b)
 #define FN(name) ORC_CAT(ORC_PREFIX, name)
 
-#define NV 15                /* vector components per site: 3 directions x 5 (quaternion representation) */
-#define DW 5                 /* direction width */
-
 /* ----------------------------------------------------------------------------
  * Model context: the plugin parameters the reference keeps as members.
  * ------------------------------------------------------------------------- */
 typedef struct {
     int model, nsc;
+    int hf, dw, nv, neq;         /* Higgs family, words per direction, per site, gauge equations per direction */
     long long nx, ny, nz, nsite;
     double dt;
     double stencil[3][3];        /* Gradients/Source/StandardModel.cpp:14-24 */
@@ -52,7 +52,8 @@ typedef struct {
     double inv_sqr[3];           /* WilsonLoops/Source/StandardModel.cpp:51-53 */
     double inv_sqr_dt;           /* :55 */
     double g_sqr, gp_sqr, inv_g_sqr, inv_gp_sqr;
-    double gsq_coupling[4];      /* getSqrCouplings(k) (returns float: :224-230) */
+    double gpp_sqr, inv_gpp_sqr; /* WilsonLoops/Source/TwoHDM.cpp:17-39, 62-86 */
+    double gsq_coupling[ORC_MAX_EQ]; /* getSqrCouplings(k) (returns float: :224-230; TwoHDM.cpp:258-267) */
     int store_energy;            /* WilsonLoops storeEnergy flag (:243-248) */
     double damping_step;         /* Core/Source/Model.cpp:345 */
     const orc_config* cfg;
@@ -70,15 +71,22 @@ typedef struct {
  * SU(2) helpers (WilsonLoops/Source/StandardModel.cpp:76-112, 160-191)
  * ------------------------------------------------------------------------- */
 
-/* getSU2Representation, quaternion branch: c0 = v[d+1], c_a = conj*v[d+1+a]. */
-static void su2_rep(const S* v, int d, int conj, double c[4])
+/* getSU2Representation, quaternion branch: c0 = v[d+off], c_a = conj*v[d+off+a]
+ * (off = 1: the isospin link; off = 5: the Higgs-family SU(2) link). */
+static void su2_rep_at(const S* v, int d, int off, int conj, double c[4])
 {
-    c[0] = (double)v[d + 1];
-    for (int k = 2; k < 5; k++) {
-        S comp = conj ? (S)(-v[d + k]) : v[d + k];
-        c[k - 1] = (double)comp;
+    c[0] = (double)v[d + off];
+    for (int k = 1; k < 4; k++) {
+        S comp = conj ? (S)(-v[d + off + k]) : v[d + off + k];
+        c[k] = (double)comp;
     }
 }
+
+static void su2_rep(const S* v, int d, int conj, double c[4]) { su2_rep_at(v, d, 1, conj, c); }
+
+/* offset of the Higgs-family field in a direction block (TwoHDM.cpp:362-368: 5 in the
+ * quaternion representation) */
+#define HF_OFF 5
 
 /* SU2Product(U1, U2, calc_trace): vector part always, scalar part and
  * renormalisation only when calc_trace (component 0 stays 0 otherwise). */
@@ -104,8 +112,42 @@ static void su2_product(const double a[4], const double b[4], int calc_trace, do
  * ------------------------------------------------------------------------- */
 
 /* transform(phi, link, conj): U(1) phase on each complex pair, then the SU(2)
- * quaternion as a real 4x4 matrix, doublet by doublet. */
-static void transform(int nsc, const double* in, const S* v, int d, int conj, double* out)
+ * quaternion as a real 4x4 matrix, doublet by doublet; for the 2HDM with a
+ * Higgs-family field, then its U(1) phase (+theta_H on doublet 1, -theta_H on
+ * doublet 2) or its SU(2) acting on (doublet 1, doublet 2) component pairs
+ * (Gradients/Source/TwoHDM.cpp:72-149). */
+static void transform_sm(int nsc, const double* in, const S* v, int d, int conj, double* out);
+
+static void transform(const ctx_t* m, const double* in, const S* v, int d, int conj, double* out)
+{
+    if (m->hf == ORC_HF_NONE) {
+        transform_sm(m->nsc, in, v, d, conj, out);
+        return;
+    }
+    double sm[8];
+    transform_sm(8, in, v, d, conj, sm);
+    const int conj_fac = conj ? -1 : 1;
+    if (m->hf == ORC_HF_U1) {
+        const double th = (double)v[d + HF_OFF];
+        for (int c = 0; c < 8; c++) {
+            int pm = -1 + 2 * (c % 2);
+            int pm4 = 1 - 2 * (c / 4);
+            out[c] = cos(th) * sm[c] + (double)pm * sin((double)(pm4 * conj_fac) * th) * sm[c - pm];
+        }
+    } else {
+        double u[4];
+        su2_rep_at(v, d, HF_OFF, conj, u);
+        for (int inner = 0; inner < 2; inner++) {
+            const int i = inner * 2;
+            out[i]     =  u[0] * sm[i] - u[3] * sm[i + 1] + u[2] * sm[i + 4] - u[1] * sm[i + 5];
+            out[i + 1] =  u[3] * sm[i] + u[0] * sm[i + 1] + u[1] * sm[i + 4] + u[2] * sm[i + 5];
+            out[i + 4] = -u[2] * sm[i] - u[1] * sm[i + 1] + u[0] * sm[i + 4] + u[3] * sm[i + 5];
+            out[i + 5] =  u[1] * sm[i] - u[2] * sm[i + 1] - u[3] * sm[i + 4] + u[0] * sm[i + 5];
+        }
+    }
+}
+
+static void transform_sm(int nsc, const double* in, const S* v, int d, int conj, double* out)
 {
     double hyper[8];
     double th = (double)v[d];
@@ -137,14 +179,14 @@ static void calc_derivatives(const ctx_t* m, const stencil_t* st, double* D)
     for (int c = 0; c < nsc; c++) D[c] = 0.0;
     for (int s = 0; s < 3; s++) {
         for (int a = 0; a < 3; a++) {
-            int d = a * DW;
+            int d = a * m->dw;
             double f[8], t[8];
             load_scalar(nsc, st->sp[a][s], f);
             if (s == 0) {
-                transform(nsc, f, st->vp[a][0], d, 0, t);
+                transform(m, f, st->vp[a][0], d, 0, t);
                 memcpy(f, t, sizeof(double) * (size_t)nsc);
             } else if (s == 2) {
-                transform(nsc, f, st->vp[a][1], d, 1, t);
+                transform(m, f, st->vp[a][1], d, 1, t);
                 memcpy(f, t, sizeof(double) * (size_t)nsc);
             }
             for (int c = 0; c < nsc; c++) D[c] += m->stencil[a][s] * f[c];
@@ -152,16 +194,17 @@ static void calc_derivatives(const ctx_t* m, const stencil_t* st, double* D)
     }
 }
 
-/* calcCurrents: J[4a + k] (hypercharge k = 0, isospin k = 1..3), summed over doublets. */
-static void calc_currents(const ctx_t* m, const stencil_t* st, double J[12])
+/* calcCurrents: J[neq*a + k] (hypercharge k = 0, isospin k = 1..3, Higgs family
+ * k = 4 (U(1)) or 4..6 (SU(2))), summed over doublets (TwoHDM.cpp:424-489). */
+static void calc_currents(const ctx_t* m, const stencil_t* st, double J[3 * ORC_MAX_EQ])
 {
     int nsc = m->nsc;
-    for (int k = 0; k < 12; k++) J[k] = 0.0;
+    for (int k = 0; k < 3 * m->neq; k++) J[k] = 0.0;
     for (int a = 0; a < 3; a++) {
-        int e = a * 4, d = a * DW;
+        int e = a * m->neq, d = a * m->dw;
         double f[8], t[8], n[8];
         load_scalar(nsc, st->sp[a][1], f);
-        transform(nsc, f, st->vp[a][1], d, 0, t);
+        transform(m, f, st->vp[a][1], d, 0, t);
         load_scalar(nsc, st->sp[a][2], n);
         for (int db = 0; db < nsc; db += 4) {
             const double* p = t + db;
@@ -170,6 +213,14 @@ static void calc_currents(const ctx_t* m, const stencil_t* st, double J[12])
             J[e + 1] += 0.25 * ( p[0] * q[3] - p[1] * q[2] + p[2] * q[1] - p[3] * q[0]);
             J[e + 2] += 0.25 * (-p[0] * q[2] - p[1] * q[3] + p[2] * q[0] + p[3] * q[1]);
             J[e + 3] += 0.25 * ( p[0] * q[1] - p[1] * q[0] - p[2] * q[3] + p[3] * q[2]);
+            const int i = db / 2;  /* upper (0) or lower (2) component pair of both doublets */
+            if (m->hf == ORC_HF_U1) {
+                J[e + 4] += 0.25 * (t[i] * n[i + 1] - t[i + 1] * n[i] - t[i + 4] * n[i + 5] + t[i + 5] * n[i + 4]);
+            } else if (m->hf == ORC_HF_SU2) {
+                J[e + 4] += 0.25 * ( t[i] * n[i + 5] - t[i + 1] * n[i + 4] + t[i + 4] * n[i + 1] - t[i + 5] * n[i]);
+                J[e + 5] += 0.25 * (-t[i] * n[i + 4] - t[i + 1] * n[i + 5] + t[i + 4] * n[i] + t[i + 5] * n[i + 1]);
+                J[e + 6] += 0.25 * ( t[i] * n[i + 1] - t[i + 1] * n[i] - t[i + 4] * n[i + 5] + t[i + 5] * n[i + 4]);
+            }
         }
     }
 }
@@ -185,7 +236,7 @@ static S gradient_energy(const ctx_t* m, const stencil_t* st)
             double f[8], t[8];
             load_scalar(nsc, st->sp[a][s], f);
             if (s == 1) {
-                transform(nsc, f, st->vp[a][1], a * DW, 0, t);
+                transform(m, f, st->vp[a][1], a * m->dw, 0, t);
                 memcpy(f, t, sizeof(double) * (size_t)nsc);
             }
             for (int c = 0; c < nsc; c++)
@@ -210,9 +261,9 @@ static S kinetic_energy(const ctx_t* m, const S* now, const S* past)
 }
 
 /* Gradients::*::calcConstraintContributions (charge density of phi_future, phi_now). */
-static void gradient_constraint(const ctx_t* m, const S* fut, const S* now, S out[4])
+static void gradient_constraint(const ctx_t* m, const S* fut, const S* now, S out[ORC_MAX_EQ])
 {
-    for (int k = 0; k < 4; k++) out[k] = (S)0;
+    for (int k = 0; k < m->neq; k++) out[k] = (S)0;
     for (int db = 0; db < m->nsc; db += 4) {
         const S* a = now + db;
         const S* b = fut + db;
@@ -232,6 +283,21 @@ static void gradient_constraint(const ctx_t* m, const S* fut, const S* now, S ou
             out[1] = (S)((double)out[1] + 0.25 * (double)t1);
             out[2] = (S)((double)out[2] + 0.25 * (double)t2);
             out[3] = (S)((double)out[3] + 0.25 * (double)t3);
+            /* Higgs-family charges (TwoHDM.cpp:355-372), over the full 8-vectors */
+            const int i = db / 2;
+            const S* A = now;
+            const S* B = fut;
+            if (m->hf == ORC_HF_U1) {
+                S h = A[i] * B[i + 1] - A[i + 1] * B[i] - A[i + 4] * B[i + 5] + A[i + 5] * B[i + 4];
+                out[4] = (S)((double)out[4] + 0.25 * (double)h);
+            } else if (m->hf == ORC_HF_SU2) {
+                S h4 = A[i] * B[i + 5] - A[i + 1] * B[i + 4] + A[i + 4] * B[i + 1] - A[i + 5] * B[i];
+                S h5 = -A[i] * B[i + 4] - A[i + 1] * B[i + 5] + A[i + 4] * B[i] + A[i + 5] * B[i + 1];
+                S h6 = A[i] * B[i + 1] - A[i + 1] * B[i] - A[i + 4] * B[i + 5] + A[i + 5] * B[i + 4];
+                out[4] = (S)((double)out[4] + 0.25 * (double)h4);
+                out[5] = (S)((double)out[5] + 0.25 * (double)h5);
+                out[6] = (S)((double)out[6] + 0.25 * (double)h6);
+            }
         }
     }
 }
@@ -337,16 +403,16 @@ static S potential_energy(const ctx_t* m, const S* f)
 /* calcMagneticContributions: U(1) sines and SU(2) staples per (i, j != i).
  * *mag_energy is the reference's storedMagneticEnergy (accumulated in S);
  * plaq (if non-null) receives P1_0 and cos(local) for i < j. */
-static void calc_magnetic(const ctx_t* m, const stencil_t* st, double Mg[12], S* mag_energy,
+static void calc_magnetic(const ctx_t* m, const stencil_t* st, double Mg[3 * ORC_MAX_EQ], S* mag_energy,
                           double* plaq_su2, double* plaq_u1)
 {
-    for (int k = 0; k < 12; k++) Mg[k] = 0.0;
+    for (int k = 0; k < 3 * m->neq; k++) Mg[k] = 0.0;
     for (int i = 0; i < 3; i++) {
-        int e = i * 4, di = i * DW;
+        int e = i * m->neq, di = i * m->dw;
         int diag = 2;
         for (int j = 0; j < 3; j++) {
             if (j == i) continue;
-            int dj = j * DW;
+            int dj = j * m->dw;
             diag += 1;
             double local = -(double)st->vp[i][2][dj] + (double)st->vp[j][2][di]
                            + (double)st->vp[i][1][dj] - (double)st->vp[j][1][di];
@@ -383,15 +449,49 @@ static void calc_magnetic(const ctx_t* m, const stencil_t* st, double Mg[12], S*
                     *plaq_u1 += cos(local);
                 }
             }
+
+            /* Higgs family (WilsonLoops/Source/TwoHDM.cpp:484-551): the same loops on
+             * the family U(1) phase or SU(2) quaternion, coupling g'' */
+            if (m->hf == ORC_HF_U1) {
+                const int o = HF_OFF;
+                double hl = -(double)st->vp[i][2][dj + o] + (double)st->vp[j][2][di + o]
+                            + (double)st->vp[i][1][dj + o] - (double)st->vp[j][1][di + o];
+                double hn = -(double)st->vp[i][diag][dj + o] - (double)st->vp[j][0][di + o]
+                            + (double)st->vp[j][0][dj + o] + (double)st->vp[i][1][di + o];
+                Mg[e + 4] += (sin(hl) - sin(hn)) * m->inv_sqr[j];
+                if (m->store_energy)
+                    *mag_energy = (S)((double)*mag_energy
+                        + 2.0 * m->inv_sqr[i] * m->inv_sqr[j] * m->inv_gpp_sqr * (1.0 - cos(hl)));
+            } else if (m->hf == ORC_HF_SU2) {
+                double q1[4], q2[4], mq[4];
+                su2_rep_at(st->vp[j][1], di, HF_OFF, 1, q1);
+                su2_rep_at(st->vp[i][1], dj, HF_OFF, 0, mq);
+                su2_product(mq, q1, 1, q1);
+                su2_rep_at(st->vp[j][2], di, HF_OFF, 0, mq);
+                su2_product(mq, q1, 1, q1);
+                su2_rep_at(st->vp[i][2], dj, HF_OFF, 1, mq);
+                su2_product(mq, q1, m->store_energy, q1);
+                su2_rep_at(st->vp[i][diag], dj, HF_OFF, 1, q2);
+                su2_rep_at(st->vp[j][0], di, HF_OFF, 1, mq);
+                su2_product(mq, q2, 1, q2);
+                su2_rep_at(st->vp[j][0], dj, HF_OFF, 0, mq);
+                su2_product(mq, q2, 1, q2);
+                su2_rep_at(st->vp[i][1], di, HF_OFF, 0, mq);
+                su2_product(mq, q2, 0, q2);
+                for (int k = 4; k < 7; k++) Mg[e + k] += (q1[k - 3] - q2[k - 3]) * m->inv_sqr[j];
+                if (m->store_energy)
+                    *mag_energy = (S)((double)*mag_energy
+                        + 2.0 * m->inv_sqr[i] * m->inv_sqr[j] * m->inv_gpp_sqr * (1.0 - q1[0]));
+            }
         }
     }
 }
 
 /* calcElectricContributions: sin(theta_now - theta_past), vec(U_now U_past^dag). */
-static void calc_electric(const ctx_t* m, const S* now, const S* past, double El[12], S* elec_energy)
+static void calc_electric(const ctx_t* m, const S* now, const S* past, double El[3 * ORC_MAX_EQ], S* elec_energy)
 {
     for (int d = 0; d < 3; d++) {
-        int e = d * 4, dd = d * DW;
+        int e = d * m->neq, dd = d * m->dw;
         double ang = (double)now[dd] - (double)past[dd];
         El[e] = sin(ang);
         double up[4], mul[4];
@@ -402,16 +502,31 @@ static void calc_electric(const ctx_t* m, const S* now, const S* past, double El
         if (m->store_energy)
             *elec_energy = (S)((double)*elec_energy
                 + 4.0 * m->inv_sqr[d] * (m->inv_g_sqr * (1.0 - up[0]) + m->inv_gp_sqr * (1.0 - cos(ang))));
+        /* Higgs family (TwoHDM.cpp:601-633) */
+        if (m->hf == ORC_HF_U1) {
+            double ha = (double)now[dd + HF_OFF] - (double)past[dd + HF_OFF];
+            El[e + 4] = sin(ha);
+            if (m->store_energy)
+                *elec_energy = (S)((double)*elec_energy + 4.0 * m->inv_sqr[d] * m->inv_gpp_sqr * (1.0 - cos(ha)));
+        } else if (m->hf == ORC_HF_SU2) {
+            double hp[4], hm[4];
+            su2_rep_at(past, dd, HF_OFF, 1, hp);
+            su2_rep_at(now, dd, HF_OFF, 0, hm);
+            su2_product(hm, hp, m->store_energy, hp);
+            for (int k = 4; k < 7; k++) El[e + k] = hp[k - 3];
+            if (m->store_energy)
+                *elec_energy = (S)((double)*elec_energy + 4.0 * m->inv_sqr[d] * m->inv_gpp_sqr * (1.0 - hp[0]));
+        }
     }
 }
 
 /* WilsonLoops::StandardModel::evolve: theta <- asin(RHS) + theta_now;
  * U <- normalise((sqrt(1 - |c|^2), c) x U_now).  Returns domain-warning bits. */
-static int evolve_links(S* past, const S* now, const double R[12])
+static int evolve_links(const ctx_t* m, S* past, const S* now, const double R[3 * ORC_MAX_EQ])
 {
     int warn = 0;
     for (int d = 0; d < 3; d++) {
-        int e = d * 4, dd = d * DW;
+        int e = d * m->neq, dd = d * m->dw;
         past[dd] = (S)(asin(R[e]) + (double)now[dd]);
         if (R[e] * R[e] > 1) warn |= 1;
         double cm = 0.0;
@@ -422,17 +537,31 @@ static int evolve_links(S* past, const S* now, const double R[12])
         su2_rep(now, dd, 0, up);
         su2_product(u, up, 1, up);
         for (int k = 0; k < 4; k++) past[dd + 1 + k] = (S)up[k];
+        /* Higgs family (TwoHDM.cpp:702-745) */
+        if (m->hf == ORC_HF_U1) {
+            past[dd + HF_OFF] = (S)(asin(R[e + 4]) + (double)now[dd + HF_OFF]);
+            if (R[e + 4] * R[e + 4] > 1) warn |= 1;
+        } else if (m->hf == ORC_HF_SU2) {
+            double hm = 0.0;
+            for (int k = 4; k < 7; k++) hm += R[e + k] * R[e + k];
+            if (hm > 1) warn |= 2;
+            double hu[4] = {sqrt(1.0 - hm), R[e + 4], R[e + 5], R[e + 6]};
+            double hq[4];
+            su2_rep_at(now, dd, HF_OFF, 0, hq);
+            su2_product(hu, hq, 1, hq);
+            for (int k = 0; k < 4; k++) past[dd + HF_OFF + k] = (S)hq[k];
+        }
     }
     return warn;
 }
 
 /* WilsonLoops::*::calcConstraintContributions over both levels (now, future). */
 static void loop_constraint(const ctx_t* m, const S* x_now, const S* x_fut, const S* const xm_now[3],
-                            const S* const xm_fut[3], S out[4])
+                            const S* const xm_fut[3], S out[ORC_MAX_EQ])
 {
-    for (int k = 0; k < 4; k++) out[k] = (S)0;
+    for (int k = 0; k < m->neq; k++) out[k] = (S)0;
     for (int d = 0; d < 3; d++) {
-        int dd = d * DW;
+        int dd = d * m->dw;
         double la = (double)x_fut[dd] - (double)x_now[dd];
         double na = (double)xm_fut[d][dd] - (double)xm_now[d][dd];
         out[0] = (S)((double)out[0] + (sin(la) - sin(na)) * m->inv_sqr[d]);
@@ -444,6 +573,21 @@ static void loop_constraint(const ctx_t* m, const S* x_now, const S* x_fut, cons
         su2_rep(xm_fut[d], dd, 0, mul);
         su2_product(mul, p2, 0, p2);
         for (int k = 1; k < 4; k++) out[k] = out[k] + (S)((p1[k] - p2[k]) * m->inv_sqr[d]);
+        /* Higgs family (TwoHDM.cpp:357-392) */
+        if (m->hf == ORC_HF_U1) {
+            double hl = (double)x_fut[dd + HF_OFF] - (double)x_now[dd + HF_OFF];
+            double hn = (double)xm_fut[d][dd + HF_OFF] - (double)xm_now[d][dd + HF_OFF];
+            out[4] = (S)((double)out[4] + (sin(hl) - sin(hn)) * m->inv_sqr[d]);
+        } else if (m->hf == ORC_HF_SU2) {
+            double q1[4], q2[4], mq[4];
+            su2_rep_at(x_fut, dd, HF_OFF, 0, q1);
+            su2_rep_at(x_now, dd, HF_OFF, 1, mq);
+            su2_product(mq, q1, 0, q1);
+            su2_rep_at(xm_now[d], dd, HF_OFF, 1, q2);
+            su2_rep_at(xm_fut[d], dd, HF_OFF, 0, mq);
+            su2_product(mq, q2, 0, q2);
+            for (int k = 4; k < 7; k++) out[k] = out[k] + (S)((q1[k - 3] - q2[k - 3]) * m->inv_sqr[d]);
+        }
     }
 }
 
@@ -478,7 +622,7 @@ static void build_stencil(const ctx_t* m, const S* sc_now, const S* ve_now, long
             long long q[3] = {p[0], p[1], p[2]};
             q[a] = wrap(q[a] + s - 1, n[a]);
             long long idx = site_index(m, q[0], q[1], q[2]);
-            st->vp[a][s] = ve_now + idx * NV;
+            st->vp[a][s] = ve_now + idx * m->nv;
             st->sp[a][s] = sc_now + idx * m->nsc;
         }
         int k = 3;
@@ -487,7 +631,7 @@ static void build_stencil(const ctx_t* m, const S* sc_now, const S* ve_now, long
             long long q[3] = {p[0], p[1], p[2]};
             q[a] = wrap(q[a] + 1, n[a]);
             q[j] = wrap(q[j] - 1, n[j]);
-            st->vp[a][k++] = ve_now + site_index(m, q[0], q[1], q[2]) * NV;
+            st->vp[a][k++] = ve_now + site_index(m, q[0], q[1], q[2]) * m->nv;
         }
     }
 }
@@ -544,9 +688,14 @@ static int ctx_init(ctx_t* m, const orc_config* c)
     memset(m, 0, sizeof(*m));
     if (c->model != ORC_MODEL_SM && c->model != ORC_MODEL_2HDM) return -1;
     if (c->nx < 1 || c->ny < 1 || c->nz < 1) return -1;
+    if (c->hf < ORC_HF_NONE || c->hf > ORC_HF_SU2 || (c->hf != ORC_HF_NONE && c->model != ORC_MODEL_2HDM)) return -1;
     m->cfg = c;
     m->model = c->model;
     m->nsc = (c->model == ORC_MODEL_SM) ? 4 : 8;
+    m->hf = c->hf;
+    m->dw = (c->hf == ORC_HF_U1) ? 6 : (c->hf == ORC_HF_SU2) ? 9 : 5;
+    m->nv = 3 * m->dw;
+    m->neq = (c->hf == ORC_HF_U1) ? 5 : (c->hf == ORC_HF_SU2) ? 7 : 4;
     m->nx = c->nx; m->ny = c->ny; m->nz = c->nz;
     m->nsite = m->nx * m->ny * m->nz;
     m->dt = c->dt;
@@ -566,8 +715,11 @@ static int ctx_init(ctx_t* m, const orc_config* c)
     m->inv_g_sqr = (m->g_sqr > c->div_tol) ? 1.0 / m->g_sqr : 0.0;
     m->inv_gp_sqr = (m->gp_sqr > c->div_tol) ? 1.0 / m->gp_sqr : 0.0;
     /* getSqrCouplings returns float in the shipped build: the coupling enters as S */
+    m->gpp_sqr = c->gpp * c->gpp;
+    m->inv_gpp_sqr = (m->gpp_sqr > c->div_tol) ? 1.0 / m->gpp_sqr : 0.0;
     m->gsq_coupling[0] = (double)(S)m->gp_sqr;
     for (int k = 1; k < 4; k++) m->gsq_coupling[k] = (double)(S)m->g_sqr;
+    for (int k = 4; k < ORC_MAX_EQ; k++) m->gsq_coupling[k] = (double)(S)m->gpp_sqr;
     return 0;
 }
 
@@ -595,7 +747,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
     long long* order = reference_site_order(&m);
     if (!order) return -2;
     const long long N = m.nsite;
-    const int nsc = m.nsc;
+    const int nsc = m.nsc, NV = m.nv, neq = m.neq;
     int nrows = 0, w = 0;
 
     for (int step = 0; step < nsteps; step++) {
@@ -631,7 +783,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             S* v_now = ve_now + idx * NV;
             S* v_past = ve_past + idx * NV;
 
-            double P[8], D[8], J[12], Mg[12], El[12];
+            double P[8], D[8], J[3 * ORC_MAX_EQ], Mg[3 * ORC_MAX_EQ], El[3 * ORC_MAX_EQ];
             potential_derivatives(&m, s_now, P);
             calc_derivatives(&m, &st, D);
             calc_currents(&m, &st, J);
@@ -665,10 +817,10 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
                            - m.damping_step * ((double)s_now[c] - (double)s_past[c]);
                 s_past[c] = (S)(2 * (double)s_now[c] - (double)s_past[c] + rhs);
             }
-            double R[12];
-            for (int k = 0; k < 12; k++)
-                R[k] = (1.0 - m.damping_step) * El[k] + m.dt * m.dt * (Mg[k] + m.gsq_coupling[k % 4] * J[k]);
-            w |= evolve_links(v_past, v_now, R);
+            double R[3 * ORC_MAX_EQ];
+            for (int k = 0; k < 3 * neq; k++)
+                R[k] = (1.0 - m.damping_step) * El[k] + m.dt * m.dt * (Mg[k] + m.gsq_coupling[k % neq] * J[k]);
+            w |= evolve_links(&m, v_past, v_now, R);
         }
 
         if (do_energy) {
@@ -689,8 +841,8 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
 
         if (do_gauss) {
             /* post-evolve: the past slot now holds t + dt (Lattice.cpp:441-541) */
-            S ref_int[4] = {0, 0, 0, 0};
-            double gint[4] = {0, 0, 0, 0}, gmax[4] = {0, 0, 0, 0};
+            S ref_int[ORC_MAX_EQ] = {0};
+            double gint[ORC_MAX_EQ] = {0}, gmax[ORC_MAX_EQ] = {0};
             for (long long oi = 0; oi < N; oi++) {
                 long long idx = order[oi];
                 long long x = idx / (m.ny * m.nz), y = (idx / m.nz) % m.ny, z = idx % m.nz;
@@ -705,10 +857,10 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
                     xm_now[d] = ve_now + j * NV;
                     xm_fut[d] = ve_past + j * NV;
                 }
-                S el[4], gr[4];
+                S el[ORC_MAX_EQ], gr[ORC_MAX_EQ];
                 loop_constraint(&m, ve_now + idx * NV, ve_past + idx * NV, xm_now, xm_fut, el);
                 gradient_constraint(&m, sc_past + idx * nsc, sc_now + idx * nsc, gr);
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < neq; k++) {
                     S viol = el[k] - (S)m.gsq_coupling[k] * gr[k];
                     S v = viol < (S)0 ? -viol : viol;
                     ref_int[k] = ref_int[k] + v;
@@ -718,7 +870,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             }
             double dv = cfg->dx * cfg->dy * cfg->dz;
             row.has_gauss = 1;
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < neq; k++) {
                 row.gauss_int[k] = gint[k] * dv;
                 row.gauss_max[k] = gmax[k];
                 row.ref_gauss_int[k] = (double)ref_int[k];
@@ -765,25 +917,51 @@ static double gaussian(uint64_t seed, uint64_t stream, uint64_t i)
 }
 
 /* Stream ids: scalars 0..7 (component c), theta_Y of direction d: 16 + d,
- * SU(2) angle eps: 32 + d, axis cos(polar): 48 + d, axis azimuth: 64 + d. */
+ * SU(2) angle eps: 32 + d, axis cos(polar): 48 + d, axis azimuth: 64 + d;
+ * Higgs-family U(1) phase: 80 + d; Higgs-family SU(2): 96 + d, 112 + d, 128 + d
+ * (eps, cos polar, azimuth). */
 #define ORC_STREAM_SCALAR(c) (0 + (c))
 #define ORC_STREAM_THETA(d) (16 + (d))
 #define ORC_STREAM_EPS(d) (32 + (d))
 #define ORC_STREAM_COSPOLAR(d) (48 + (d))
 #define ORC_STREAM_AZIMUTH(d) (64 + (d))
+#define ORC_STREAM_HF_THETA(d) (80 + (d))
+#define ORC_STREAM_HF_EPS(d) (96 + (d))
+#define ORC_STREAM_HF_COSPOLAR(d) (112 + (d))
+#define ORC_STREAM_HF_AZIMUTH(d) (128 + (d))
+
+/* Random unit quaternion (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform on S^2. */
+static void random_link(uint64_t seed, int s_eps, int s_cos, int s_az, uint64_t i, double eps_sigma, double q[4])
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    q[0] = 1.0;
+    q[1] = q[2] = q[3] = 0.0;
+    if (eps_sigma > 0.0) {
+        double eps = eps_sigma * gaussian(seed, (uint64_t)s_eps, i);
+        double ct = 2.0 * uniform01(seed, (uint64_t)s_cos, i) - 1.0;
+        double st = sqrt(1.0 - ct * ct);
+        double ph = two_pi * uniform01(seed, (uint64_t)s_az, i);
+        double se = sin(eps);
+        q[0] = cos(eps);
+        q[1] = se * st * cos(ph);
+        q[2] = se * st * sin(ph);
+        q[3] = se * ct;
+    }
+}
 
 /*
  * Fill both time levels (E = 0, pi = 0).  Scalars: component c ~ N(mean[c], sigma[c]^2)
  * (+ wall profile on component 0 when wall_width > 0).  Links: theta_Y ~ N(0, theta_sigma^2);
  * SU(2) = (cos eps, sin eps n) with eps ~ N(0, eps_sigma^2), n uniform on S^2; identity when
- * eps_sigma == 0 and theta_sigma == 0.
+ * eps_sigma == 0 and theta_sigma == 0.  dw = words per direction (5, or 6 / 9 with a
+ * Higgs-family phase ~ N(0, theta_sigma^2) / quaternion drawn like the SU(2) link).
  */
-void FN(init_fields)(int nx, int ny, int nz, int nsc, S* scalars, S* vectors, unsigned long long seed,
+void FN(init_fields)(int nx, int ny, int nz, int nsc, int dw, S* scalars, S* vectors, unsigned long long seed,
                      const double* mean, const double* sigma, double theta_sigma, double eps_sigma,
                      double wall_width, double wall_value)
 {
-    const double two_pi = 6.283185307179586476925286766559;
     long long N = (long long)nx * ny * nz;
+    const int NV = 3 * dw;
     for (long long i = 0; i < N; i++) {
         long long z = i % nz;
         for (int c = 0; c < nsc; c++) {
@@ -797,22 +975,21 @@ void FN(init_fields)(int nx, int ny, int nz, int nsc, S* scalars, S* vectors, un
         }
         for (int d = 0; d < 3; d++) {
             double th = theta_sigma * gaussian(seed, ORC_STREAM_THETA(d), (uint64_t)i);
-            double q[4] = {1.0, 0.0, 0.0, 0.0};
-            if (eps_sigma > 0.0) {
-                double eps = eps_sigma * gaussian(seed, ORC_STREAM_EPS(d), (uint64_t)i);
-                double ct = 2.0 * uniform01(seed, ORC_STREAM_COSPOLAR(d), (uint64_t)i) - 1.0;
-                double st = sqrt(1.0 - ct * ct);
-                double ph = two_pi * uniform01(seed, ORC_STREAM_AZIMUTH(d), (uint64_t)i);
-                double se = sin(eps);
-                q[0] = cos(eps);
-                q[1] = se * st * cos(ph);
-                q[2] = se * st * sin(ph);
-                q[3] = se * ct;
-            }
-            S* v0 = vectors + i * NV + d * DW;
-            S* v1 = vectors + (N + i) * NV + d * DW;
+            double q[4];
+            random_link(seed, ORC_STREAM_EPS(d), ORC_STREAM_COSPOLAR(d), ORC_STREAM_AZIMUTH(d), (uint64_t)i, eps_sigma, q);
+            S* v0 = vectors + i * NV + d * dw;
+            S* v1 = vectors + (N + i) * NV + d * dw;
             v0[0] = v1[0] = (S)th;
             for (int k = 0; k < 4; k++) v0[1 + k] = v1[1 + k] = (S)q[k];
+            if (dw == 6) {
+                double hth = theta_sigma * gaussian(seed, ORC_STREAM_HF_THETA(d), (uint64_t)i);
+                v0[5] = v1[5] = (S)hth;
+            } else if (dw == 9) {
+                double hq[4];
+                random_link(seed, ORC_STREAM_HF_EPS(d), ORC_STREAM_HF_COSPOLAR(d), ORC_STREAM_HF_AZIMUTH(d),
+                            (uint64_t)i, eps_sigma, hq);
+                for (int k = 0; k < 4; k++) v0[5 + k] = v1[5 + k] = (S)hq[k];
+            }
         }
     }
 }

@@ -28,7 +28,16 @@ extern "C" {
  * (Core/Header/Model.hpp:19-21).  Only the quaternion link representation and
  * periodic faces are restated (the paths the benchmark configurations use). */
 #define ORC_MODEL_SM    1   /* SO_N potential, Gradients::StandardModel, WilsonLoops::StandardModel */
-#define ORC_MODEL_2HDM  2   /* Double_SO_N, Gradients::TwoHDM, WilsonLoops::TwoHDM with gaugeNum = 4 */
+#define ORC_MODEL_2HDM  2   /* Double_SO_N, Gradients::TwoHDM, WilsonLoops::TwoHDM (gaugeNum 4, 5 or 7) */
+
+/* Higgs-family gauge field of the 2HDM (WilsonLoops/Source/TwoHDM.cpp:210-242):
+ * none (gaugeNum 4, 5 link words per direction), a U(1) phase theta_H (gaugeNum 5,
+ * 6 words: [theta_Y, c0..c3, theta_H]) or an SU(2) quaternion d (gaugeNum 7,
+ * 9 words: [theta_Y, c0..c3, d0..d3]). */
+#define ORC_HF_NONE 0
+#define ORC_HF_U1   1
+#define ORC_HF_SU2  2
+#define ORC_MAX_EQ  7
 
 typedef struct orc_config {
     int model;
@@ -55,6 +64,9 @@ typedef struct orc_config {
      * clear = periodic.  Sites on a Fixed face are not evolved and are not part
      * of the analysers' domain (BoundaryConditions/Source/Fixed.cpp:159-251). */
     int fixed_axes;
+    /* 2HDM Higgs-family gauge group (ORC_HF_*) and its coupling g'' (WilsonLoops/Config/TwoHDM.cfg) */
+    int hf;
+    double gpp;
 } orc_config;
 
 /* One row of global observables, written on every step where an analyser logs.
@@ -65,12 +77,12 @@ typedef struct orc_row {
     int time_iter;
     int has_energy, has_gauss;
     double energy, potential, gradient, kinetic, magnetic, electric;
-    double gauss_int[4], gauss_max[4];
+    double gauss_int[ORC_MAX_EQ], gauss_max[ORC_MAX_EQ];  /* gaugeNum entries used */
     double plaq_su2, plaq_u1, phi_sq;
     /* reference-precision running sums (float in the shipped build), as the
      * reference accumulates them site by site in its own region order */
     double ref_energy[6];
-    double ref_gauss_int[4];
+    double ref_gauss_int[ORC_MAX_EQ];
 } orc_row;
 
 #ifdef __cplusplus

@@ -10,7 +10,9 @@ its Energy and GaugeCondition analysers.  Only ``tests/``,
 checker; the product never imports it.
 
 Arrays use the reference layout: ``scalars[2, nx, ny, nz, nsc]`` and
-``vectors[2, nx, ny, nz, 15]`` (per direction ``[theta_Y, c0, c1, c2, c3]``).
+``vectors[2, nx, ny, nz, 3 * dw]`` (per direction ``[theta_Y, c0, c1, c2, c3]``,
+plus the 2HDM Higgs-family phase ``theta_H`` (dw = 6) or quaternion ``d0..d3``
+(dw = 9), ``WilsonLoops/Source/TwoHDM.cpp:210-242``).
 """
 from __future__ import annotations
 
@@ -28,6 +30,8 @@ LIB_PATH = os.path.join(BUILD_DIR, "liborc.so")
 
 MODEL_SM = 1
 MODEL_2HDM = 2
+HF_NONE, HF_U1, HF_SU2 = 0, 1, 2   # 2HDM Higgs-family gauge group (gaugeNum 4, 5, 7)
+MAX_EQ = 7
 
 
 class OrcConfig(ctypes.Structure):
@@ -48,6 +52,7 @@ class OrcConfig(ctypes.Structure):
         ("energy_offset", ctypes.c_double),
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
         ("fixed_axes", ctypes.c_int),
+        ("hf", ctypes.c_int), ("gpp", ctypes.c_double),
     ]
 
 
@@ -57,10 +62,10 @@ class OrcRow(ctypes.Structure):
         ("has_energy", ctypes.c_int), ("has_gauss", ctypes.c_int),
         ("energy", ctypes.c_double), ("potential", ctypes.c_double), ("gradient", ctypes.c_double),
         ("kinetic", ctypes.c_double), ("magnetic", ctypes.c_double), ("electric", ctypes.c_double),
-        ("gauss_int", ctypes.c_double * 4), ("gauss_max", ctypes.c_double * 4),
+        ("gauss_int", ctypes.c_double * MAX_EQ), ("gauss_max", ctypes.c_double * MAX_EQ),
         ("plaq_su2", ctypes.c_double), ("plaq_u1", ctypes.c_double), ("phi_sq", ctypes.c_double),
         ("ref_energy", ctypes.c_double * 6),
-        ("ref_gauss_int", ctypes.c_double * 4),
+        ("ref_gauss_int", ctypes.c_double * MAX_EQ),
     ]
 
 
@@ -105,10 +110,25 @@ class Params:
     energy_every: int = 0
     gauss_every: int = 0
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (else periodic)
+    hf: int = HF_NONE          # 2HDM Higgs-family gauge field (HF_*)
 
     @property
     def nsc(self) -> int:
         return 4 if self.model == MODEL_SM else 8
+
+    @property
+    def dw(self) -> int:
+        """Link words per direction."""
+        return {HF_NONE: 5, HF_U1: 6, HF_SU2: 9}[self.hf]
+
+    @property
+    def nve(self) -> int:
+        return 3 * self.dw
+
+    @property
+    def neq(self) -> int:
+        """Gauge equations per direction = Gauss constraints (gaugeNum)."""
+        return {HF_NONE: 4, HF_U1: 5, HF_SU2: 7}[self.hf]
 
     @property
     def nsite(self) -> int:
@@ -160,7 +180,8 @@ def _load():
                               ctypes.POINTER(OrcRow), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
                 f = getattr(lib, p + "init_fields")
                 f.restype = None
-                f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, fp, ctypes.c_ulonglong,
+                f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, fp,
+                              ctypes.c_ulonglong,
                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
             _lib = lib
@@ -198,11 +219,11 @@ def init_fields(p: Params, ic: ICSpec, dtype=np.float32):
     """Both time levels of the initial data (E = 0, pi = 0) in the reference layout."""
     lib = _load()
     sc = np.zeros((2, p.nx, p.ny, p.nz, p.nsc), dtype=dtype)
-    ve = np.zeros((2, p.nx, p.ny, p.nz, 15), dtype=dtype)
+    ve = np.zeros((2, p.nx, p.ny, p.nz, p.nve), dtype=dtype)
     mean = (ctypes.c_double * 8)(*[float(v) for v in (list(ic.mean) + [0.0] * 8)[:8]])
     sig = (ctypes.c_double * 8)(*[float(v) for v in (list(ic.sigma) + [0.0] * 8)[:8]])
     getattr(lib, _prefix(dtype) + "init_fields")(
-        p.nx, p.ny, p.nz, p.nsc, _ptr(sc), _ptr(ve), ctypes.c_ulonglong(ic.seed), mean, sig,
+        p.nx, p.ny, p.nz, p.nsc, p.dw, _ptr(sc), _ptr(ve), ctypes.c_ulonglong(ic.seed), mean, sig,
         float(ic.theta_sigma), float(ic.eps_sigma), float(ic.wall_width), float(ic.wall_value))
     return sc, ve
 
@@ -216,7 +237,7 @@ def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, tim
     assert scalars.flags.c_contiguous and vectors.flags.c_contiguous
     assert scalars.dtype == vectors.dtype
     assert scalars.shape == (2, p.nx, p.ny, p.nz, p.nsc), scalars.shape
-    assert vectors.shape == (2, p.nx, p.ny, p.nz, 15), vectors.shape
+    assert vectors.shape == (2, p.nx, p.ny, p.nz, p.nve), vectors.shape
     max_rows = nsteps + 1
     rows = (OrcRow * max_rows)()
     warn = ctypes.c_int(0)
@@ -230,10 +251,10 @@ def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, tim
         d = {"time_iter": r.time_iter, "has_energy": bool(r.has_energy), "has_gauss": bool(r.has_gauss)}
         for k in ROW_KEYS:
             d[k] = getattr(r, k)
-        d["gauss_int"] = list(r.gauss_int)
-        d["gauss_max"] = list(r.gauss_max)
+        d["gauss_int"] = list(r.gauss_int)[: p.neq]
+        d["gauss_max"] = list(r.gauss_max)[: p.neq]
         d["plaq_su2"], d["plaq_u1"], d["phi_sq"] = r.plaq_su2, r.plaq_u1, r.phi_sq
         d["ref_energy"] = list(r.ref_energy)
-        d["ref_gauss_int"] = list(r.ref_gauss_int)
+        d["ref_gauss_int"] = list(r.ref_gauss_int)[: p.neq]
         out.append(d)
     return out, warn.value

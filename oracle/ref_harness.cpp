@@ -5,13 +5,16 @@
  *
  * Usage:  GFT_REF_WORKDIR=<dir> ref32|ref64
  *   <dir>/<Module>/Config/*.cfg   configuration (written by oracle/refrun.py)
- *   <dir>/ic.bin                  both time levels: scalars then vectors, raw
- *                                 storage words in the reference layout
+ *   <dir>/ic.bin                  optional: both time levels, scalars then vectors,
+ *                                 raw storage words in the reference layout (without
+ *                                 it the configured initial condition stands)
  * Output:
+ *   <dir>/initial.bin             the initial fields the run started from
  *   <dir>/final.bin               both time levels after nt steps (same layout)
  *   <dir>/rows.txt                per logged step: the Energy analyser's running
- *                                 sums and the GaugeCondition sums and maxima,
- *                                 read before the analysers write and reset them
+ *                                 sums and the GaugeCondition sums and maxima (7
+ *                                 each, zero beyond gaugeNum), read before the
+ *                                 analysers write and reset them
  *   <dir>/timing.txt              wall seconds of Lattice::evolve
  *
  * The analysers' sums are private members of the reference classes; this file
@@ -56,9 +59,10 @@ public:
         out << time_step << " " << (e ? 1 : 0) << " " << (g ? 1 : 0);
         out << std::setprecision(17);
         for (unsigned k = 0; k < 6; k++) out << " " << (e ? (double)*energy->energyPointers[k] : 0.0);
-        for (unsigned k = 0; k < 4; k++)
+        // up to gaugeNum = 7 constraint equations (WilsonLoops/Source/TwoHDM.cpp:276-279), zero-padded
+        for (unsigned k = 0; k < 7; k++)
             out << " " << (g && k < gauge->integratedAbsViolation.size() ? (double)gauge->integratedAbsViolation[k] : 0.0);
-        for (unsigned k = 0; k < 4; k++)
+        for (unsigned k = 0; k < 7; k++)
             out << " " << (g && k < gauge->maxAbsViolation.size() ? (double)gauge->maxAbsViolation[k] : 0.0);
         out << "\n";
     }

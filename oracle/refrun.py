@@ -70,7 +70,7 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
         f"timestep size                  : {_num(p.dt)}",
         "",
         f"scalar components              : {p.nsc}",
-        "vector components per direction: 5",
+        f"vector components per direction: {p.dw}",
         "",
         "override nt by light crossings",
         "flag                           : 0",
@@ -217,7 +217,7 @@ def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, n
     given = scalars is not None
     if not given:
         scalars = np.zeros((2, p.nx, p.ny, p.nz, p.nsc), dtype)
-        vectors = np.zeros((2, p.nx, p.ny, p.nz, 15), dtype)
+        vectors = np.zeros((2, p.nx, p.ny, p.nz, p.nve), dtype)
     try:
         write_configs(work, p, nt, ic_types, random_uniform)
         icp = os.path.join(work, "ic.bin")
@@ -245,8 +245,10 @@ def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, n
                 if not t:
                     continue
                 vals = [float(v) for v in t[3:]]
+                k = orc.MAX_EQ
                 rows.append({"time_iter": int(t[0]), "has_energy": t[1] == "1", "has_gauss": t[2] == "1",
-                             "ref_energy": vals[0:6], "ref_gauss_int": vals[6:10], "gauss_max": vals[10:14]})
+                             "ref_energy": vals[0:6], "ref_gauss_int": vals[6:6 + p.neq],
+                             "gauss_max": vals[6 + k:6 + k + p.neq]})
         with open(os.path.join(work, "timing.txt")) as f:
             secs = float(f.read().split()[0])
         return sc, ve, rows, secs if secs > 0 else wall

@@ -51,6 +51,13 @@ CASES = {
                           dict(seed=19, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
     "2hdm_fixed_y_5x6x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=6, nz=4, energy_every=2, gauss_every=2, fixed_axes=2),
                            dict(seed=20, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 6, ("f32",)),
+    # 2HDM with a Higgs-family gauge field: U(1) (gaugeNum 5) and SU(2) (gaugeNum 7), coupling g''
+    "2hdm_hf_u1_4x5x3": (dict(model=orc.MODEL_2HDM, nx=4, ny=5, nz=3, energy_every=2, gauss_every=3, hf=orc.HF_U1,
+                              gpp=0.47),
+                         dict(seed=21, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
+    "2hdm_hf_su2_5x3x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=3, nz=4, energy_every=3, gauss_every=2, hf=orc.HF_SU2,
+                               gpp=0.52),
+                          dict(seed=22, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
 }
 
 
@@ -72,8 +79,8 @@ def make(name: str) -> None:
             row_has_energy=np.array([r["has_energy"] for r in rows], dtype=bool),
             row_has_gauss=np.array([r["has_gauss"] for r in rows], dtype=bool),
             row_ref_energy=np.array([r["ref_energy"] for r in rows], dtype=np.float64).reshape(-1, 6),
-            row_ref_gauss_int=np.array([r["ref_gauss_int"] for r in rows], dtype=np.float64).reshape(-1, 4),
-            row_gauss_max=np.array([r["gauss_max"] for r in rows], dtype=np.float64).reshape(-1, 4),
+            row_ref_gauss_int=np.array([r["ref_gauss_int"] for r in rows], dtype=np.float64).reshape(-1, p.neq),
+            row_gauss_max=np.array([r["gauss_max"] for r in rows], dtype=np.float64).reshape(-1, p.neq),
             meta=np.array(json.dumps(meta)))
         print("wrote", os.path.relpath(out, ROOT), os.path.getsize(out), "bytes")
 
