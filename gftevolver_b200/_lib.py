@@ -29,6 +29,11 @@ GFT_W_RANGE = 16
 GFT_MODEL_SM = 1
 GFT_MODEL_2HDM = 2
 
+GFT_HF_NONE = 0   # 2HDM Higgs-family gauge field: none (gaugeNum 4), U(1) (5), SU(2) (7)
+GFT_HF_U1 = 1
+GFT_HF_SU2 = 2
+GFT_MAX_GAUSS = 7
+
 GFT_FORM_REF = 0
 GFT_FORM_FP64 = 1
 GFT_FORM_MIXED = 2
@@ -51,6 +56,7 @@ class GftConfig(ctypes.Structure):
         ("energy_offset", ctypes.c_double),
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
         ("fixed_axes", ctypes.c_int),
+        ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
     ]
 
 
@@ -59,7 +65,7 @@ class GftObservables(ctypes.Structure):
         ("time_iter", ctypes.c_int), ("has_energy", ctypes.c_int), ("has_gauss", ctypes.c_int),
         ("energy", ctypes.c_double), ("potential", ctypes.c_double), ("gradient", ctypes.c_double),
         ("kinetic", ctypes.c_double), ("magnetic", ctypes.c_double), ("electric", ctypes.c_double),
-        ("gauss_int", ctypes.c_double * 4), ("gauss_max", ctypes.c_double * 4),
+        ("gauss_int", ctypes.c_double * GFT_MAX_GAUSS), ("gauss_max", ctypes.c_double * GFT_MAX_GAUSS),
         ("plaq_su2", ctypes.c_double), ("plaq_u1", ctypes.c_double), ("phi_sq", ctypes.c_double),
     ]
 

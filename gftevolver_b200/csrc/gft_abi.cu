@@ -27,8 +27,9 @@ void set_global_error(const std::string& s)
     g_err = s;
 }
 
-// Slots of one device row: kObsCount energy slots, then kGaussSlots.
-constexpr int kRowSlots = kObsCount + kGaussSlots;
+// Slots of one device row: kObsCount energy slots, then gaugeNum integrated and
+// gaugeNum maximum Gauss slots (room for gaugeNum = 7).
+constexpr int kRowSlots = kRowSlotCount;
 constexpr int kMaxProfiled = 8192;
 
 }  // namespace
@@ -40,6 +41,9 @@ void set_last_error(const std::string& msg) { set_global_error(msg); }
 struct gft_handle {
     gft_config cfg{};
     int nsc = 4;
+    int hf = 0;             // Higgs-family field (kHf*)
+    int nve = 15;           // link words per site in the reference layout (15, 18 or 27)
+    int neq = 4;            // gauge equations per direction = Gauss constraints (gaugeNum)
     int nsite = 0;
     int sbytes = 4;         // storage bytes per word (4 or 8)
     void* level_mem[2] = {nullptr, nullptr};
@@ -121,6 +125,10 @@ StepParams gft::config_params(const gft_config& c, int nsite, bool f32ref, int t
     for (int k = 1; k < 4; k++) P.gsq[k] = f32ref ? (double)(float)g2 : g2;
     P.inv_g_sqr = (g2 > c.div_tol) ? 1.0 / g2 : 0.0;
     P.inv_gp_sqr = (gp2 > c.div_tol) ? 1.0 / gp2 : 0.0;
+    P.hf = (c.model == GFT_MODEL_2HDM) ? c.higgs_family : kHfNone;
+    const double gpp2 = c.gpp * c.gpp;
+    P.gsq_hf = f32ref ? (double)(float)gpp2 : gpp2;
+    P.inv_gpp_sqr = (gpp2 > c.div_tol) ? 1.0 / gpp2 : 0.0;
     double damp = (time_iter < c.nt_damped) ? c.damping : 0.0;
     if (f32ref) damp = (double)(float)damp;
     P.damping_step = 0.5 * damp * c.dt;
@@ -166,7 +174,7 @@ void gft::row_scales(const gft_config& c, int nsite, double* scale)
     scale[kObsPlaqSU2] = 1.0 / (3.0 * nsite);
     scale[kObsPlaqU1] = 1.0 / (3.0 * nsite);
     scale[kObsPhiSq] = 1.0 / (double)nsite;
-    for (int k = 0; k < 4; k++) scale[kObsCount + k] = dv;
+    for (int k = 0; k < config_neq(c); k++) scale[kObsCount + k] = dv;  // integrated |violation|; maxima unscaled
 }
 
 namespace {
@@ -187,8 +195,9 @@ StepParams make_params(const gft_handle* h, int time_iter, bool energy)
 // aligned for any lattice size.
 size_t padded_sites(int nsite) { return ((size_t)nsite + 63) / 64 * 64; }
 
+// hf: Higgs-family arrays after the doublets (3 phase arrays or 3 quaternion arrays).
 template <class S>
-void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
+void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L, int hf = kHfNone)
 {
     const size_t np = padded_sites(nsite);
     S* p = static_cast<S*>(mem);
@@ -203,9 +212,17 @@ void carve(void* mem, int nsite, int nsc, LevelPtrs<S>& L)
     L.ph[0] = p;
     p += 4 * np;
     L.ph[1] = (nsc == 8) ? p : nullptr;
+    p += (nsc == 8) ? 4 * np : 0;
+    for (int d = 0; d < 3; d++) {
+        L.hth[d] = (hf == kHfU1) ? p + d * np : nullptr;
+        L.hq[d] = (hf == kHfSU2) ? p + 4 * d * np : nullptr;
+    }
 }
 
-size_t level_words(int nsite, int nsc) { return padded_sites(nsite) * (15 + (size_t)nsc); }
+size_t level_words(int nsite, int nsc, int hf = kHfNone)
+{
+    return padded_sites(nsite) * (15 + (size_t)nsc + (hf == kHfU1 ? 3 : (hf == kHfSU2 ? 12 : 0)));
+}
 
 // Tensor maps of both levels for a tile shape: staged planes and past prefetch.
 bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm, TMaps* tp)
@@ -225,7 +242,7 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
 // need 130 KB of shared memory and leave one CTA per SM (30 % against 45 %).
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
-    if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1) return false;
+    if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1 || h->hf != kHfNone) return false;
     if (h->kernel_kind == 0 && h->cfg.model != GFT_MODEL_SM) return false;
     return tiled_supported(P, h->tile_variant);
 }
@@ -322,6 +339,14 @@ int validate(const gft_config* c, std::string& why)
         why = "gft_create: fixed_axes is a bitmask of the three axes (0..7)";
         return GFT_E_INVALID;
     }
+    if (c->higgs_family < GFT_HF_NONE || c->higgs_family > GFT_HF_SU2) {
+        why = "gft_create: higgs_family must be GFT_HF_NONE, GFT_HF_U1 or GFT_HF_SU2";
+        return GFT_E_INVALID;
+    }
+    if (c->higgs_family != GFT_HF_NONE && c->model != GFT_MODEL_2HDM) {
+        why = "gft_create: a Higgs-family gauge field needs the 2HDM (WilsonLoops::TwoHDM)";
+        return GFT_E_INVALID;
+    }
     return GFT_OK;
 }
 
@@ -353,6 +378,9 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     gft_handle* h = new gft_handle();
     h->cfg = *cfg;
     h->nsc = (cfg->model == GFT_MODEL_SM) ? 4 : 8;
+    h->hf = (cfg->model == GFT_MODEL_2HDM) ? cfg->higgs_family : kHfNone;
+    h->nve = 3 * (h->hf == kHfU1 ? 6 : (h->hf == kHfSU2 ? 9 : 5));
+    h->neq = config_neq(*cfg);
     h->nsite = cfg->nx * cfg->ny * cfg->nz;
     h->sbytes = (cfg->form == GFT_FORM_REF) ? cfg->storage_bytes : (cfg->form == GFT_FORM_FP64 ? 8 : 4);
     cudaError_t e = cudaSetDevice(cfg->device);
@@ -367,7 +395,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
         delete h;
         return r;
     }
-    const size_t lbytes = level_words(h->nsite, h->nsc) * (size_t)h->sbytes;
+    const size_t lbytes = level_words(h->nsite, h->nsc, h->hf) * (size_t)h->sbytes;
     for (int t = 0; t < 2; t++) {
         e = cudaMalloc(&h->level_mem[t], lbytes);
         if (e != cudaSuccess) {
@@ -377,9 +405,9 @@ int gft_create(const gft_config* cfg, gft_handle** out)
         }
         h->dev_bytes += lbytes;
         if (h->sbytes == 4)
-            carve<float>(h->level_mem[t], h->nsite, h->nsc, h->lf[t]);
+            carve<float>(h->level_mem[t], h->nsite, h->nsc, h->lf[t], h->hf);
         else
-            carve<double>(h->level_mem[t], h->nsite, h->nsc, h->ld[t]);
+            carve<double>(h->level_mem[t], h->nsite, h->nsc, h->ld[t], h->hf);
     }
     const StepParams P = make_params(h, 0, false);
     if (cfg->form == GFT_FORM_MIXED) {
@@ -390,7 +418,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     }
     int nb = std::max(fast_launch_blocks(P, 0), fast_gauss_blocks(P));
     nb = std::max(nb, ref_launch_blocks(P));
-    const size_t pe = (size_t)nb * kObsCount * sizeof(double), pg = (size_t)nb * kGaussSlots * sizeof(double);
+    const size_t pe = (size_t)nb * kObsCount * sizeof(double), pg = (size_t)nb * 2 * h->neq * sizeof(double);
     h->rows_cap = 64;
     if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMalloc(&h->d_part_e, pe)) != cudaSuccess || (e = cudaMalloc(&h->d_part_g, pg)) != cudaSuccess ||
@@ -479,7 +507,7 @@ int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter, bool on_
     if (!h || !sc || !ve) return GFT_E_INVALID;
     if (time_iter < 0) return h->fail(GFT_E_INVALID, "gft_upload: time_iter must be >= 0");
     cudaSetDevice(h->cfg.device);
-    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
+    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * h->nve;
     const H* dsc = sc;
     const H* dve = ve;
     cudaError_t e = cudaSuccess;
@@ -494,7 +522,7 @@ int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter, bool on_
     }
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         const H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
-        const H* v_t = dve + (size_t)t * h->nsite * 15;
+        const H* v_t = dve + (size_t)t * h->nsite * h->nve;
         e = is_f64_storage(h) ? launch_aos_to_soa<double, H>(s_t, v_t, h->nsite, h->nsc, h->ld[t], h->stream)
                               : launch_aos_to_soa<float, H>(s_t, v_t, h->nsite, h->nsc, h->lf[t], h->stream);
     }
@@ -511,7 +539,7 @@ int download_impl(gft_handle* h, H* sc, H* ve, bool on_device = false)
     if (!h || !sc || !ve) return GFT_E_INVALID;
     if (!h->has_data) return h->fail(GFT_E_STATE, "gft_download: no field data on the device");
     cudaSetDevice(h->cfg.device);
-    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * 15;
+    const size_t nsc_w = 2 * (size_t)h->nsite * h->nsc, nve_w = 2 * (size_t)h->nsite * h->nve;
     H* dsc = sc;
     H* dve = ve;
     if (!on_device) {
@@ -523,7 +551,7 @@ int download_impl(gft_handle* h, H* sc, H* ve, bool on_device = false)
     cudaError_t e = cudaSuccess;
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
-        H* v_t = dve + (size_t)t * h->nsite * 15;
+        H* v_t = dve + (size_t)t * h->nsite * h->nve;
         e = is_f64_storage(h) ? launch_soa_to_aos<double, H>(h->ld[t], h->nsite, h->nsc, s_t, v_t, h->stream)
                               : launch_soa_to_aos<float, H>(h->lf[t], h->nsite, h->nsc, s_t, v_t, h->stream);
     }
@@ -550,7 +578,7 @@ int ensure_rows(gft_handle* h, int n)
     return GFT_OK;
 }
 
-void fill_row(gft_observables* r, int time_iter, bool e, bool g, const double* v)
+void fill_row(gft_observables* r, int time_iter, bool e, bool g, const double* v, int neq)
 {
     std::memset(r, 0, sizeof(*r));
     r->time_iter = time_iter;
@@ -568,9 +596,9 @@ void fill_row(gft_observables* r, int time_iter, bool e, bool g, const double* v
         r->phi_sq = v[kObsPhiSq];
     }
     if (g) {
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < neq; k++) {
             r->gauss_int[k] = v[kObsCount + k];
-            r->gauss_max[k] = v[kObsCount + 4 + k];
+            r->gauss_max[k] = v[kObsCount + neq + k];
         }
     }
 }
@@ -625,7 +653,7 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         if (g && err == cudaSuccess) {
             err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
             if (err == cudaSuccess)
-                err = launch_finalize(h->d_part_g, gauss_blocks(h, P), kGaussSlots, 4, h->d_scale + kObsCount,
+                err = launch_finalize(h->d_part_g, gauss_blocks(h, P), 2 * h->neq, h->neq, h->d_scale + kObsCount,
                                       out + kObsCount, h->d_mid, h->stream);
         }
         if (e || g) {
@@ -645,7 +673,8 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
     if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve");
     if (status & 8u) return h->fail(GFT_E_TIMEOUT, "gft_evolve: a device wait timed out (tensor-copy barrier)");
     const int nw = rows ? std::min(row, std::max(max_rows, 0)) : 0;
-    for (int r = 0; r < nw; r++) fill_row(&rows[r], meta[r].ti, meta[r].e, meta[r].g, host.data() + (size_t)r * kRowSlots);
+    for (int r = 0; r < nw; r++)
+        fill_row(&rows[r], meta[r].ti, meta[r].e, meta[r].g, host.data() + (size_t)r * kRowSlots, h->neq);
     if (n_rows) *n_rows = nw;
     return (int)(status & (GFT_W_ASIN_DOMAIN | GFT_W_SQRT_DOMAIN | GFT_W_NONFINITE | GFT_W_RANGE));
 }
@@ -653,9 +682,9 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
 }  // namespace
 
 int gft::validate_config(const gft_config* c, std::string& why) { return validate(c, why); }
-void gft::fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v)
+void gft::fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v, int neq)
 {
-    fill_row(r, time_iter, e, g, v);
+    fill_row(r, time_iter, e, g, v, neq);
 }
 size_t gft::level_bytes_f32(int nsite, int nsc) { return level_words(nsite, nsc) * sizeof(float); }
 void gft::carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L) { carve<float>(mem, nsite, nsc, L); }
@@ -724,7 +753,7 @@ int gft_observe(gft_handle* h, gft_observables* row)
     cudaSetDevice(h->cfg.device);
     const int ti = h->time_iter;
     const int tn = (ti + 1) % 2, tp = 1 - tn;
-    const size_t lbytes = level_words(h->nsite, h->nsc) * (size_t)h->sbytes;
+    const size_t lbytes = level_words(h->nsite, h->nsc, h->hf) * (size_t)h->sbytes;
     int rc = ensure_stage(h, lbytes);
     if (rc != GFT_OK) return rc;
     cudaError_t e = cudaMemcpyAsync(h->d_stage, h->level_mem[tp], lbytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -732,11 +761,11 @@ int gft_observe(gft_handle* h, gft_observables* row)
     if (e == cudaSuccess) {
         if (is_f64_storage(h)) {
             LevelPtrs<double> tmp;
-            carve<double>(h->d_stage, h->nsite, h->nsc, tmp);
+            carve<double>(h->d_stage, h->nsite, h->nsc, tmp, h->hf);
             e = launch_step<double>(h, P, tn, h->ld[tn], tmp, true);
         } else {
             LevelPtrs<float> tmp;
-            carve<float>(h->d_stage, h->nsite, h->nsc, tmp);
+            carve<float>(h->d_stage, h->nsite, h->nsc, tmp, h->hf);
             e = launch_step<float>(h, P, tn, h->lf[tn], tmp, true);
         }
     }
@@ -748,7 +777,7 @@ int gft_observe(gft_handle* h, gft_observables* row)
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "gft_observe");
-    fill_row(row, ti, true, false, host.data());
+    fill_row(row, ti, true, false, host.data(), h->neq);
     return GFT_OK;
 }
 
@@ -760,6 +789,8 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
         h->kernel_kind = 1;
         return GFT_OK;
     }
+    if (kind == 2 && h->hf != kHfNone)
+        return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel has no Higgs-family field");
     if (h->cfg.form != GFT_FORM_MIXED) {
         if (kind == 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
         h->kernel_kind = 0;
@@ -861,7 +892,7 @@ int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user)
 int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes, int max)
 {
     if (!h || level < 0 || level > 1 || x < 0 || x >= h->cfg.nx || !ptrs || !bytes) return GFT_E_INVALID;
-    const int n = 7 + (h->nsc == 8 ? 1 : 0);
+    const int n = 7 + (h->nsc == 8 ? 1 : 0) + (h->hf != kHfNone ? 3 : 0);
     if (max < n) return h->fail(GFT_E_INVALID, "gft_level_planes: need room for " + std::to_string(n) + " arrays");
     const size_t plane = (size_t)h->cfg.ny * h->cfg.nz;
     const size_t w = (size_t)h->sbytes;
@@ -871,11 +902,15 @@ int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes
         for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.q[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
         for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.th[d] + plane * x; bytes[k] = plane * w; }
         for (int db = 0; db < h->nsc / 4; db++, k++) { ptrs[k] = L.ph[db] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+        for (int d = 0; d < 3 && h->hf == kHfU1; d++, k++) { ptrs[k] = L.hth[d] + plane * x; bytes[k] = plane * w; }
+        for (int d = 0; d < 3 && h->hf == kHfSU2; d++, k++) { ptrs[k] = L.hq[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
     } else {
         const LevelPtrs<double>& L = h->ld[level];
         for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.q[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
         for (int d = 0; d < 3; d++, k++) { ptrs[k] = L.th[d] + plane * x; bytes[k] = plane * w; }
         for (int db = 0; db < h->nsc / 4; db++, k++) { ptrs[k] = L.ph[db] + 4 * plane * x; bytes[k] = 4 * plane * w; }
+        for (int d = 0; d < 3 && h->hf == kHfU1; d++, k++) { ptrs[k] = L.hth[d] + plane * x; bytes[k] = plane * w; }
+        for (int d = 0; d < 3 && h->hf == kHfSU2; d++, k++) { ptrs[k] = L.hq[d] + 4 * plane * x; bytes[k] = 4 * plane * w; }
     }
     return n;
 }

@@ -16,11 +16,15 @@ __global__ void aos_to_soa_kernel(const H* __restrict__ sc, const H* __restrict_
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsite) return;
-    const H* v = ve + (size_t)s * 15;
+    const int dw = lv.hq[0] ? 9 : (lv.hth[0] ? 6 : 5);  // link words per direction
+    const H* v = ve + (size_t)s * 3 * dw;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        lv.th[d][s] = (S)v[5 * d];
-        st4(lv.q[d], s, (S)v[5 * d + 1], (S)v[5 * d + 2], (S)v[5 * d + 3], (S)v[5 * d + 4]);
+        const H* w = v + dw * d;
+        lv.th[d][s] = (S)w[0];
+        st4(lv.q[d], s, (S)w[1], (S)w[2], (S)w[3], (S)w[4]);
+        if (dw == 6) lv.hth[d][s] = (S)w[5];
+        if (dw == 9) st4(lv.hq[d], s, (S)w[5], (S)w[6], (S)w[7], (S)w[8]);
     }
     const H* f = sc + (size_t)s * nsc;
     for (int db = 0; db < nsc / 4; db++)
@@ -32,13 +36,21 @@ __global__ void soa_to_aos_kernel(LevelPtrs<S> lv, int nsite, int nsc, H* __rest
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsite) return;
-    H* v = ve + (size_t)s * 15;
+    const int dw = lv.hq[0] ? 9 : (lv.hth[0] ? 6 : 5);  // link words per direction
+    H* v = ve + (size_t)s * 3 * dw;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        v[5 * d] = (H)lv.th[d][s];
+        H* w = v + dw * d;
+        w[0] = (H)lv.th[d][s];
         const S* q = lv.q[d] + 4 * (size_t)s;
 #pragma unroll
-        for (int k = 0; k < 4; k++) v[5 * d + 1 + k] = (H)q[k];
+        for (int k = 0; k < 4; k++) w[1 + k] = (H)q[k];
+        if (dw == 6) w[5] = (H)lv.hth[d][s];
+        if (dw == 9) {
+            const S* h = lv.hq[d] + 4 * (size_t)s;
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[5 + k] = (H)h[k];
+        }
     }
     H* f = sc + (size_t)s * nsc;
     for (int db = 0; db < nsc / 4; db++) {
@@ -52,7 +64,8 @@ __global__ void soa_to_aos_kernel(LevelPtrs<S> lv, int nsite, int nsc, H* __rest
 // (seed, stream, index); uniforms from the top 53 bits; normals by the cosine
 // branch of Box-Muller.  Stream ids: scalar component c -> c, theta_Y of
 // direction d -> 16 + d, SU(2) angle -> 32 + d, axis cos(polar) -> 48 + d,
-// axis azimuth -> 64 + d.
+// axis azimuth -> 64 + d; Higgs-family phase -> 80 + d, Higgs-family SU(2)
+// angle / cos(polar) / azimuth -> 96 / 112 / 128 + d.
 __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
 {
     z += 0x9E3779B97F4A7C15ULL;
@@ -74,12 +87,32 @@ __device__ __forceinline__ double gaussian(unsigned long long seed, unsigned lon
     return sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
 }
 
+// Unit quaternion (cos eps, sin eps n): eps ~ N(0, eps_sigma^2) from stream s0,
+// n uniform on S^2 from streams s0 + 16 (cos polar) and s0 + 32 (azimuth).
+__device__ __forceinline__ void random_link(const ICParams& ic, unsigned long long s0, unsigned long long key,
+                                            double (&q)[4])
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    q[0] = 1.0;
+    q[1] = q[2] = q[3] = 0.0;
+    if (ic.eps_sigma > 0.0) {
+        const double eps = ic.eps_sigma * gaussian(ic.seed, s0, key);
+        const double ct = 2.0 * uniform01(ic.seed, s0 + 16ULL, key) - 1.0;
+        const double st = sqrt(1.0 - ct * ct);
+        const double ph = two_pi * uniform01(ic.seed, s0 + 32ULL, key);
+        const double se = sin(eps);
+        q[0] = cos(eps);
+        q[1] = se * st * cos(ph);
+        q[2] = se * st * sin(ph);
+        q[3] = se * ct;
+    }
+}
+
 template <class S>
 __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs<S> a, LevelPtrs<S> b)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.nsite) return;
-    const double two_pi = 6.283185307179586476925286766559;
     const int zc = s % P.nz;
     // random-number key: the site's index in the whole lattice (differs from s only on an x-slab)
     const int plane = P.ny * P.nz;
@@ -102,22 +135,22 @@ __global__ void init_fields_kernel(StepParams P, int nsc, ICParams ic, LevelPtrs
     }
     for (int d = 0; d < 3; d++) {
         const double th = ic.theta_sigma * gaussian(ic.seed, 16ULL + d, key);
-        double q0 = 1.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
-        if (ic.eps_sigma > 0.0) {
-            const double eps = ic.eps_sigma * gaussian(ic.seed, 32ULL + d, key);
-            const double ct = 2.0 * uniform01(ic.seed, 48ULL + d, key) - 1.0;
-            const double st = sqrt(1.0 - ct * ct);
-            const double ph = two_pi * uniform01(ic.seed, 64ULL + d, key);
-            const double se = sin(eps);
-            q0 = cos(eps);
-            q1 = se * st * cos(ph);
-            q2 = se * st * sin(ph);
-            q3 = se * ct;
-        }
+        double q[4];
+        random_link(ic, 32ULL + d, key, q);
         a.th[d][s] = (S)th;
         b.th[d][s] = (S)th;
-        st4(a.q[d], s, (S)q0, (S)q1, (S)q2, (S)q3);
-        st4(b.q[d], s, (S)q0, (S)q1, (S)q2, (S)q3);
+        st4(a.q[d], s, (S)q[0], (S)q[1], (S)q[2], (S)q[3]);
+        st4(b.q[d], s, (S)q[0], (S)q[1], (S)q[2], (S)q[3]);
+        if (a.hth[0]) {
+            const double h = ic.theta_sigma * gaussian(ic.seed, 80ULL + d, key);
+            a.hth[d][s] = (S)h;
+            b.hth[d][s] = (S)h;
+        }
+        if (a.hq[0]) {
+            random_link(ic, 96ULL + d, key, q);
+            st4(a.hq[d], s, (S)q[0], (S)q[1], (S)q[2], (S)q[3]);
+            st4(b.hq[d], s, (S)q[0], (S)q[1], (S)q[2], (S)q[3]);
+        }
     }
 }
 

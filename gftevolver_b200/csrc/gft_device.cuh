@@ -5,6 +5,8 @@
 //   q[d]  : [N][4] storage words, SU(2) quaternion (c0, c1, c2, c3) of the link in direction d
 //   th[d] : [N]    storage words, U(1) hypercharge phase theta_Y of the link in direction d
 //   ph[k] : [N][4] storage words, Higgs doublet k (k = 0 for SM, 0..1 for 2HDM)
+//   hth[d]: [N]    2HDM Higgs-family U(1) phase theta_H (gaugeNum 5 only)
+//   hq[d] : [N][4] 2HDM Higgs-family SU(2) quaternion (gaugeNum 7 only)
 // Site index s = (x*ny + y)*nz + z as in the reference (Core/Source/Lattice.cpp:658-671).
 // The reference's AoS record per site ([theta, c0..c3] x 3 directions, then the
 // scalar components) is split so that a warp reads 16- or 32-byte vectors of
@@ -34,11 +36,22 @@ enum ObsSlot : int {
 };
 constexpr int kGaussSlots = 8;  // integrated |viol| (4) then max |viol| (4)
 
+// 2HDM Higgs-family gauge field (WilsonLoops/Source/TwoHDM.cpp:210-242): none
+// (gaugeNum 4), a U(1) phase (gaugeNum 5) or an SU(2) quaternion (gaugeNum 7).
+constexpr int kHfNone = 0;
+constexpr int kHfU1 = 1;
+constexpr int kHfSU2 = 2;
+constexpr int kEqMax = 7;                     // gauge equations per direction (gaugeNum) at most
+constexpr int kGaussSlotsMax = 2 * kEqMax;    // integrated then max |viol| per constraint
+__host__ __device__ constexpr int hf_neq(int hf) { return hf == kHfU1 ? 5 : (hf == kHfSU2 ? 7 : 4); }
+
 template <class S>
 struct LevelPtrs {
     S* q[3];
     S* th[3];
     S* ph[2];
+    S* hth[3];   // Higgs-family U(1) phase (null unless gaugeNum 5)
+    S* hq[3];    // Higgs-family SU(2) quaternion (null unless gaugeNum 7)
 };
 
 // Per-launch parameters (POD, passed by value).
@@ -51,6 +64,9 @@ struct StepParams {
     double inv_sqr_dt;      // 1/dt^2
     double gsq[4];          // coupling^2 per equation k % 4 (as the reference's getSqrCouplings returns it)
     double inv_g_sqr, inv_gp_sqr;
+    int hf;                 // 2HDM Higgs-family gauge field (kHf*)
+    double gsq_hf;          // g''^2 of the Higgs-family equations (TwoHDM.cpp:258-267)
+    double inv_gpp_sqr;     // 1/g''^2 (0 below the division tolerance)
     double damping_step;    // 0.5 * damping * dt for this step
     // SO_N
     double lambda, eta_sqr;

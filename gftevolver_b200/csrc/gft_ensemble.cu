@@ -35,9 +35,28 @@ using namespace tiled;
 
 constexpr int kGroup = 64;  // members per launch: their parameters are kernel parameters
 
+// A member's level arrays (the ensemble runs gaugeNum-4 models: no Higgs-family
+// arrays, so the kernel-parameter copy omits those pointers).  The step and
+// Gauss bodies read them from the parameter space in place.
+struct EnsLevel {
+    float* q[3];
+    float* th[3];
+    float* ph[2];
+    EnsLevel& operator=(const LevelPtrs<float>& L)
+    {
+        for (int d = 0; d < 3; d++) {
+            q[d] = L.q[d];
+            th[d] = L.th[d];
+        }
+        ph[0] = L.ph[0];
+        ph[1] = L.ph[1];
+        return *this;
+    }
+};
+
 struct EnsParams {
     StepParams P[kGroup];
-    LevelPtrs<float> lv[kGroup][2];
+    EnsLevel lv[kGroup][2];
 };
 static_assert(sizeof(EnsParams) <= 31 * 1024, "ensemble parameters exceed the kernel parameter space");
 
@@ -550,6 +569,10 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
         }
         if (cfgs[m].form != GFT_FORM_MIXED) {
             set_error("gft_batch_create: the ensemble evolves the mixed form only");
+            return GFT_E_UNSUPPORTED;
+        }
+        if (cfgs[m].higgs_family != GFT_HF_NONE) {
+            set_error("gft_batch_create: the ensemble has no Higgs-family gauge field (gaugeNum 4 only)");
             return GFT_E_UNSUPPORTED;
         }
         if (cfgs[m].model != cfgs[0].model || cfgs[m].device != cfgs[0].device) {

@@ -39,9 +39,11 @@ struct GlobalAcc {
     __device__ __forceinline__ Q<S> q(int d, int s) const { return ld4<S>(L.q[d], s); }
     __device__ __forceinline__ S th(int d, int s) const { return ld1<S>(L.th[d], s); }
     __device__ __forceinline__ Q<S> ph(int k, int s) const { return ld4<S>(L.ph[k], s); }
+    __device__ __forceinline__ S hth(int d, int s) const { return ld1<S>(L.hth[d], s); }
+    __device__ __forceinline__ Q<S> hq(int d, int s) const { return ld4<S>(L.hq[d], s); }
 };
 
-template <class S, int MODEL, bool ENERGY>
+template <class S, int MODEL, int HF, bool ENERGY>
 __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> past,
                                                         unsigned* status, double* partials)
 {
@@ -69,7 +71,8 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         n.d21 = o.c + o.p[2] + o.m[1];
         XCarry<S, (MODEL == kModelSM) ? 1 : 2> carry;
         carry.valid = false;
-        site_step<S, MODEL, ENERGY>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn, counts(P, x));
+        site_step<S, MODEL, ENERGY, HF>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn,
+                                        counts(P, x));
     }
     if (ENERGY) {
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
@@ -82,22 +85,44 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
 // thread per site: every load of a site is independent of the others, which
 // keeps the most loads in flight (a march along x that carries the x - 1 links
 // in registers serialises them and measured slower).
-template <class S, int MODEL>
+template <class S, int MODEL, int HF>
 __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                          double* partials)
 {
+    constexpr int NG = 2 * hf_neq(HF);
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.z;
-    double v[kGaussSlots];
+    double v[NG];
 #pragma unroll
-    for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
+    for (int k = 0; k < NG; k++) v[k] = 0.0;
     if (z < P.nz && y < P.ny && counts(P, x) && !frozen(P, x, y, z)) {
         const Offs o = offsets(P, x, y, z);
-        gauss_site<S, MODEL>(P, now, fut, o.c, o.c + o.m[0], o.c + o.m[1], o.c + o.m[2], v);
+        gauss_site<S, MODEL, HF>(P, now, fut, o.c, o.c + o.m[0], o.c + o.m[1], o.c + o.m[2], v);
     }
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    block_reduce_store<kGaussSlots>(v, partials + (size_t)blk * kGaussSlots, 4);
+    block_reduce_store<NG>(v, partials + (size_t)blk * NG, NG / 2);
+}
+
+template <class S, int MODEL, int HF>
+void fast_step_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                      double* partials, bool energy, cudaStream_t stream)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    if (energy)
+        fast_step_kernel<S, MODEL, HF, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+    else
+        fast_step_kernel<S, MODEL, HF, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+}
+
+template <class S, int MODEL, int HF>
+void fast_gauss_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
+                       cudaStream_t stream)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    fast_gauss_kernel<S, MODEL, HF><<<grid, block, 0, stream>>>(P, now, fut, partials);
 }
 
 }  // namespace
@@ -105,16 +130,22 @@ __global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs
 int fast_launch_blocks(const StepParams& P, int /*variant*/) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
 int fast_gauss_blocks(const StepParams& P) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
 
+// P.hf selects the Higgs-family variant (2HDM only); the Gauss kernel writes
+// 2 * gaugeNum partial slots per block.
 template <class S, int MODEL>
 cudaError_t launch_fast_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
                              double* partials, bool energy, int /*variant*/, cudaStream_t stream)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
-    if (energy)
-        fast_step_kernel<S, MODEL, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
-    else
-        fast_step_kernel<S, MODEL, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+    if constexpr (MODEL == kModel2HDM) {
+        if (P.hf == kHfU1)
+            fast_step_launch<S, MODEL, kHfU1>(P, now, past, status, partials, energy, stream);
+        else if (P.hf == kHfSU2)
+            fast_step_launch<S, MODEL, kHfSU2>(P, now, past, status, partials, energy, stream);
+        else
+            fast_step_launch<S, MODEL, kHfNone>(P, now, past, status, partials, energy, stream);
+    } else {
+        fast_step_launch<S, MODEL, kHfNone>(P, now, past, status, partials, energy, stream);
+    }
     return cudaGetLastError();
 }
 
@@ -122,9 +153,16 @@ template <class S, int MODEL>
 cudaError_t launch_fast_gauss(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
                               cudaStream_t stream)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
-    fast_gauss_kernel<S, MODEL><<<grid, block, 0, stream>>>(P, now, fut, partials);
+    if constexpr (MODEL == kModel2HDM) {
+        if (P.hf == kHfU1)
+            fast_gauss_launch<S, MODEL, kHfU1>(P, now, fut, partials, stream);
+        else if (P.hf == kHfSU2)
+            fast_gauss_launch<S, MODEL, kHfSU2>(P, now, fut, partials, stream);
+        else
+            fast_gauss_launch<S, MODEL, kHfNone>(P, now, fut, partials, stream);
+    } else {
+        fast_gauss_launch<S, MODEL, kHfNone>(P, now, fut, partials, stream);
+    }
     return cudaGetLastError();
 }
 

@@ -58,6 +58,8 @@ inline void tiled_tile(int variant, int& ty, int& tz)
 }
 
 // Auxiliary kernels (gft_aux_kernels.cu).
+// The reference record has 3 x 5 link words per site, 3 x 6 with a Higgs-family
+// phase (lv.hth set) or 3 x 9 with a Higgs-family quaternion (lv.hq set).
 template <class S, class H>
 cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s);
 template <class S, class H>
@@ -95,13 +97,18 @@ void set_error(const std::string& msg);
 // arithmetic form with float storage, whose couplings are rounded to float).
 StepParams config_params(const gft_config& c, int nsite, bool f32ref, int time_iter, bool energy);
 // Per-slot scale of an observables row: energies and Gauss integrals x dV, means / N.
+// (kRowSlotCount slots: kObsCount energy slots, then gaugeNum integrated and
+// gaugeNum maximum Gauss slots.)
 void row_scales(const gft_config& c, int nsite, double* scale);
 int validate_config(const gft_config* c, std::string& why);
-void fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v);
-// One time level of float storage: bytes, and the array pointers within it.
+// neq = gaugeNum (Gauss constraints per row).
+void fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v, int neq = 4);
+// One time level of float storage (no Higgs-family arrays): bytes, and the array pointers within it.
 size_t level_bytes_f32(int nsite, int nsc);
 void carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L);
-constexpr int kRowSlotCount = kObsCount + kGaussSlots;
+constexpr int kRowSlotCount = kObsCount + kGaussSlotsMax;
+// Gauge equations per direction (gaugeNum) of a configuration.
+inline int config_neq(const gft_config& c) { return c.model == GFT_MODEL_2HDM ? hf_neq(c.higgs_family) : 4; }
 
 // Elementary-function self-test (gft_math.cuh vs CUDA's functions) on the current device.
 cudaError_t run_math_selftest(int n, double* out8);

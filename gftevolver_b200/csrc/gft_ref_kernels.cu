@@ -16,16 +16,18 @@
 namespace gft {
 namespace {
 
-constexpr int DWc = 4;  // equations per direction (hypercharge + 3 isospin)
-
 template <class S>
 struct RefView {
     const LevelPtrs<S>& L;
     __device__ double th(int d, int s) const { return (double)L.th[d][s]; }
     // getSU2Representation, quaternion branch (WilsonLoops/Source/StandardModel.cpp:104-109)
-    __device__ void rep(int d, int s, bool conj, double c[4]) const
+    __device__ void rep(int d, int s, bool conj, double c[4]) const { rep_of(L.q[d], s, conj, c); }
+    // the same for the Higgs-family field (offset 5 of a direction block, TwoHDM.cpp:362-368)
+    __device__ double hth(int d, int s) const { return (double)L.hth[d][s]; }
+    __device__ void hrep(int d, int s, bool conj, double c[4]) const { rep_of(L.hq[d], s, conj, c); }
+    __device__ static void rep_of(const S* a, int s, bool conj, double c[4])
     {
-        const S* p = L.q[d] + 4 * (size_t)s;
+        const S* p = a + 4 * (size_t)s;
         c[0] = (double)p[0];
         for (int k = 1; k < 4; k++) c[k] = conj ? -(double)p[k] : (double)p[k];
     }
@@ -56,11 +58,50 @@ __device__ __forceinline__ void ref_su2_product(const double a[4], const double 
     out[3] = p3;
 }
 
-// Gradients::StandardModel::transform / TwoHDM::transform with gaugeNum = 4
-// (Gradients/Source/StandardModel.cpp:72-100, TwoHDM.cpp:72-116).
+// Gradients::StandardModel::transform / TwoHDM::transform
+// (Gradients/Source/StandardModel.cpp:72-100, TwoHDM.cpp:72-149): hypercharge
+// phase, isospin SU(2), then the Higgs-family U(1) (+theta_H on doublet 1,
+// -theta_H on doublet 2) or SU(2) (acting on doublet-1 / doublet-2 pairs).
 template <int NSC, class S>
+__device__ __forceinline__ void ref_transform_sm(const double* in, const RefView<S>& V, int d, int s, bool conj,
+                                                 double* out);
+
+template <int NSC, int HF, class S>
 __device__ __forceinline__ void ref_transform(const double* in, const RefView<S>& V, int d, int s, bool conj,
                                               double* out)
+{
+    if (HF == kHfNone) {
+        ref_transform_sm<NSC>(in, V, d, s, conj, out);
+        return;
+    }
+    double sm[8];
+    ref_transform_sm<8>(in, V, d, s, conj, sm);
+    const int conj_fac = conj ? -1 : 1;
+    if (HF == kHfU1) {
+        const double th = V.hth(d, s);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int pm = -1 + 2 * (c % 2);
+            const int pm4 = 1 - 2 * (c / 4);
+            out[c] = cos(th) * sm[c] + (double)pm * sin((double)(pm4 * conj_fac) * th) * sm[c - pm];
+        }
+    } else {
+        double u[4];
+        V.hrep(d, s, conj, u);
+#pragma unroll
+        for (int inner = 0; inner < 2; inner++) {
+            const int i = inner * 2;
+            out[i] = u[0] * sm[i] - u[3] * sm[i + 1] + u[2] * sm[i + 4] - u[1] * sm[i + 5];
+            out[i + 1] = u[3] * sm[i] + u[0] * sm[i + 1] + u[1] * sm[i + 4] + u[2] * sm[i + 5];
+            out[i + 4] = -u[2] * sm[i] - u[1] * sm[i + 1] + u[0] * sm[i + 4] + u[3] * sm[i + 5];
+            out[i + 5] = u[1] * sm[i] - u[2] * sm[i + 1] - u[3] * sm[i + 4] + u[0] * sm[i + 5];
+        }
+    }
+}
+
+template <int NSC, class S>
+__device__ __forceinline__ void ref_transform_sm(const double* in, const RefView<S>& V, int d, int s, bool conj,
+                                                 double* out)
 {
     const double th = V.th(d, s);
     const double sn = sin((conj ? -1.0 : 1.0) * th);
@@ -206,11 +247,12 @@ __device__ __forceinline__ S ref_potential_energy(const StepParams& P, const S* 
     }
 }
 
-template <class S, int MODEL, bool ENERGY>
+template <class S, int MODEL, int HF, bool ENERGY>
 __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> past,
                                                        unsigned* status, double* partials)
 {
     constexpr int NSC = (MODEL == kModelSM) ? 4 : 8;
+    constexpr int NEQ = hf_neq(HF);  // gauge equations per direction
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.z;
@@ -244,9 +286,9 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                 ref_load_scalar<NSC>(now, s, f);
                 const double w = (st == 1) ? -2.0 * P.lap[a] : P.lap[a];
                 if (st == 0) {
-                    ref_transform<NSC>(f, V, a, n.m[a], false, t);
+                    ref_transform<NSC, HF>(f, V, a, n.m[a], false, t);
                 } else if (st == 2) {
-                    ref_transform<NSC>(f, V, a, n.c, true, t);
+                    ref_transform<NSC, HF>(f, V, a, n.c, true, t);
                 } else {
 #pragma unroll
                     for (int c = 0; c < NSC; c++) t[c] = f[c];
@@ -257,27 +299,36 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
         }
 
         // ---- calcCurrents (:323-363) and, on energy steps, calcGradientEnergy (:192-235) ----
-        double J[12];
+        double J[3 * NEQ];
         S der[3 * NSC];
         for (int a = 0; a < 3; a++) {
             double f[NSC], t[NSC], nb[NSC];
             ref_load_scalar<NSC>(now, n.c, f);
-            ref_transform<NSC>(f, V, a, n.c, false, t);
+            ref_transform<NSC, HF>(f, V, a, n.c, false, t);
             ref_load_scalar<NSC>(now, n.p[a], nb);
-            double j0 = 0.0, j1 = 0.0, j2 = 0.0, j3 = 0.0;
+            double jj[NEQ];
+#pragma unroll
+            for (int k = 0; k < NEQ; k++) jj[k] = 0.0;
 #pragma unroll
             for (int db = 0; db < NSC; db += 4) {
                 const double* p = t + db;
                 const double* q = nb + db;
-                j0 += 0.25 * (p[0] * q[1] - p[1] * q[0] + p[2] * q[3] - p[3] * q[2]);
-                j1 += 0.25 * (p[0] * q[3] - p[1] * q[2] + p[2] * q[1] - p[3] * q[0]);
-                j2 += 0.25 * (-p[0] * q[2] - p[1] * q[3] + p[2] * q[0] + p[3] * q[1]);
-                j3 += 0.25 * (p[0] * q[1] - p[1] * q[0] - p[2] * q[3] + p[3] * q[2]);
+                jj[0] += 0.25 * (p[0] * q[1] - p[1] * q[0] + p[2] * q[3] - p[3] * q[2]);
+                jj[1] += 0.25 * (p[0] * q[3] - p[1] * q[2] + p[2] * q[1] - p[3] * q[0]);
+                jj[2] += 0.25 * (-p[0] * q[2] - p[1] * q[3] + p[2] * q[0] + p[3] * q[1]);
+                jj[3] += 0.25 * (p[0] * q[1] - p[1] * q[0] - p[2] * q[3] + p[3] * q[2]);
+                // Higgs-family currents (Gradients/Source/TwoHDM.cpp:465-485), i = upper or lower pair
+                const int i = db / 2;
+                if (HF == kHfU1) {
+                    jj[4 % NEQ] += 0.25 * (t[i] * nb[i + 1] - t[i + 1] * nb[i] - t[i + 4] * nb[i + 5] + t[i + 5] * nb[i + 4]);
+                } else if (HF == kHfSU2) {
+                    jj[4 % NEQ] += 0.25 * (t[i] * nb[i + 5] - t[i + 1] * nb[i + 4] + t[i + 4] * nb[i + 1] - t[i + 5] * nb[i]);
+                    jj[5 % NEQ] += 0.25 * (-t[i] * nb[i + 4] - t[i + 1] * nb[i + 5] + t[i + 4] * nb[i] + t[i + 5] * nb[i + 1]);
+                    jj[6 % NEQ] += 0.25 * (t[i] * nb[i + 1] - t[i + 1] * nb[i] - t[i + 4] * nb[i + 5] + t[i + 5] * nb[i + 4]);
+                }
             }
-            J[4 * a + 0] = j0;
-            J[4 * a + 1] = j1;
-            J[4 * a + 2] = j2;
-            J[4 * a + 3] = j3;
+#pragma unroll
+            for (int k = 0; k < NEQ; k++) J[NEQ * a + k] = jj[k];
             if (ENERGY) {
                 // stencil_iter 1 (-1/dx * U phi(x)) then stencil_iter 2 (+1/dx * phi(x+a)), accumulated in S
 #pragma unroll
@@ -301,9 +352,9 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
         }
 
         // ---- calcMagneticContributions (WilsonLoops/Source/StandardModel.cpp:324-409) ----
-        double Mg[12];
+        double Mg[3 * NEQ];
 #pragma unroll
-        for (int k = 0; k < 12; k++) Mg[k] = 0.0;
+        for (int k = 0; k < 3 * NEQ; k++) Mg[k] = 0.0;
         S mag_e = (S)0;
         double plaq2 = 0.0, plaq1 = 0.0;
         for (int i = 0; i < 3; i++) {
@@ -312,7 +363,7 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                 const int di = n.dg[i][j];
                 const double local = -V.th(j, n.p[i]) + V.th(i, n.p[j]) + V.th(j, n.c) - V.th(i, n.c);
                 const double neigh = -V.th(j, di) - V.th(i, n.m[j]) + V.th(j, n.m[j]) + V.th(i, n.c);
-                Mg[DWc * i] += (sin(local) - sin(neigh)) * P.lap[j];
+                Mg[NEQ * i] += (sin(local) - sin(neigh)) * P.lap[j];
 
                 double p1[4], mul[4];
                 V.rep(i, n.c, true, p1);
@@ -333,7 +384,7 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                 ref_su2_product(mul, p2, false, p2);
 
 #pragma unroll
-                for (int k = 1; k < 4; k++) Mg[DWc * i + k] += (p1[k] - p2[k]) * P.lap[j];
+                for (int k = 1; k < 4; k++) Mg[NEQ * i + k] += (p1[k] - p2[k]) * P.lap[j];
 
                 if (ENERGY) {
                     const double cl = cos(local);
@@ -344,24 +395,67 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                         plaq1 += cl;
                     }
                 }
+
+                // Higgs family (WilsonLoops/Source/TwoHDM.cpp:484-551)
+                if (HF == kHfU1) {
+                    const double hl = -V.hth(j, n.p[i]) + V.hth(i, n.p[j]) + V.hth(j, n.c) - V.hth(i, n.c);
+                    const double hn = -V.hth(j, di) - V.hth(i, n.m[j]) + V.hth(j, n.m[j]) + V.hth(i, n.c);
+                    Mg[NEQ * i + 4 % NEQ] += (sin(hl) - sin(hn)) * P.lap[j];
+                    if (ENERGY)
+                        mag_e = (S)((double)mag_e + 2.0 * P.lap[i] * P.lap[j] * P.inv_gpp_sqr * (1.0 - cos(hl)));
+                } else if (HF == kHfSU2) {
+                    double q1[4], q2[4], mq[4];
+                    V.hrep(i, n.c, true, q1);
+                    V.hrep(j, n.c, false, mq);
+                    ref_su2_product(mq, q1, true, q1);
+                    V.hrep(i, n.p[j], false, mq);
+                    ref_su2_product(mq, q1, true, q1);
+                    V.hrep(j, n.p[i], true, mq);
+                    ref_su2_product(mq, q1, store, q1);
+                    V.hrep(j, di, true, q2);
+                    V.hrep(i, n.m[j], true, mq);
+                    ref_su2_product(mq, q2, true, q2);
+                    V.hrep(j, n.m[j], false, mq);
+                    ref_su2_product(mq, q2, true, q2);
+                    V.hrep(i, n.c, false, mq);
+                    ref_su2_product(mq, q2, false, q2);
+#pragma unroll
+                    for (int k = 4; k < 7; k++) Mg[NEQ * i + k % NEQ] += (q1[k - 3] - q2[k - 3]) * P.lap[j];
+                    if (ENERGY)
+                        mag_e = (S)((double)mag_e + 2.0 * P.lap[i] * P.lap[j] * P.inv_gpp_sqr * (1.0 - q1[0]));
+                }
             }
         }
 
         // ---- calcElectricContributions (:412-453) ----
-        double El[12];
+        double El[3 * NEQ];
         S elec_e = (S)0;
         for (int d = 0; d < 3; d++) {
             const double ang = V.th(d, n.c) - Vp.th(d, n.c);
-            El[DWc * d] = sin(ang);
+            El[NEQ * d] = sin(ang);
             double up[4], mul[4];
             Vp.rep(d, n.c, true, up);
             V.rep(d, n.c, false, mul);
             ref_su2_product(mul, up, store, up);
 #pragma unroll
-            for (int k = 1; k < 4; k++) El[DWc * d + k] = up[k];
+            for (int k = 1; k < 4; k++) El[NEQ * d + k] = up[k];
             if (ENERGY)
                 elec_e = (S)((double)elec_e
                              + 4.0 * P.lap[d] * (P.inv_g_sqr * (1.0 - up[0]) + P.inv_gp_sqr * (1.0 - cos(ang))));
+            // Higgs family (TwoHDM.cpp:601-633)
+            if (HF == kHfU1) {
+                const double ha = V.hth(d, n.c) - Vp.hth(d, n.c);
+                El[NEQ * d + 4 % NEQ] = sin(ha);
+                if (ENERGY) elec_e = (S)((double)elec_e + 4.0 * P.lap[d] * P.inv_gpp_sqr * (1.0 - cos(ha)));
+            } else if (HF == kHfSU2) {
+                double hp[4], hm[4];
+                Vp.hrep(d, n.c, true, hp);
+                V.hrep(d, n.c, false, hm);
+                ref_su2_product(hm, hp, store, hp);
+#pragma unroll
+                for (int k = 4; k < 7; k++) El[NEQ * d + k % NEQ] = hp[k - 3];
+                if (ENERGY) elec_e = (S)((double)elec_e + 4.0 * P.lap[d] * P.inv_gpp_sqr * (1.0 - hp[0]));
+            }
         }
 
         // ---- Energy::preEvolveLocationAnalysis (Analysers/Source/Energy.cpp:117-163) ----
@@ -406,11 +500,11 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
 
         // ---- WilsonLoops::StandardModel::evolve (:456-514) ----
         for (int d = 0; d < 3; d++) {
-            double R[4];
+            double R[NEQ];
 #pragma unroll
-            for (int k = 0; k < 4; k++)
-                R[k] = (1.0 - P.damping_step) * El[DWc * d + k]
-                       + P.dt * P.dt * (Mg[DWc * d + k] + P.gsq[k] * J[DWc * d + k]);
+            for (int k = 0; k < NEQ; k++)
+                R[k] = (1.0 - P.damping_step) * El[NEQ * d + k]
+                       + P.dt * P.dt * (Mg[NEQ * d + k] + (k < 4 ? P.gsq[k & 3] : P.gsq_hf) * J[NEQ * d + k]);
             const S th_new = (S)(asin(R[0]) + V.th(d, n.c));
             if (R[0] * R[0] > 1) warn |= kWarnAsin;
             double cm = 0.0;
@@ -427,6 +521,28 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
             st4(past.q[d], n.c, q0, q1, q2, q3);
             finite = finite && isfinite((double)th_new) && isfinite((double)q0) && isfinite((double)q1)
                      && isfinite((double)q2) && isfinite((double)q3);
+            // Higgs family (TwoHDM.cpp:702-745)
+            if (HF == kHfU1) {
+                const double r4 = R[4 % NEQ];
+                const S h_new = (S)(asin(r4) + V.hth(d, n.c));
+                if (r4 * r4 > 1) warn |= kWarnAsin;
+                past.hth[d][n.c] = h_new;
+                finite = finite && isfinite((double)h_new);
+            } else if (HF == kHfSU2) {
+                double hm = 0.0;
+                hm += R[4 % NEQ] * R[4 % NEQ];
+                hm += R[5 % NEQ] * R[5 % NEQ];
+                hm += R[6 % NEQ] * R[6 % NEQ];
+                if (hm > 1) warn |= kWarnSqrt;
+                const double hu[4] = {sqrt(1.0 - hm), R[4 % NEQ], R[5 % NEQ], R[6 % NEQ]};
+                double hq[4];
+                V.hrep(d, n.c, false, hq);
+                ref_su2_product(hu, hq, true, hq);
+                const S h0 = (S)hq[0], h1 = (S)hq[1], h2 = (S)hq[2], h3 = (S)hq[3];
+                st4(past.hq[d], n.c, h0, h1, h2, h3);
+                finite = finite && isfinite((double)h0) && isfinite((double)h1) && isfinite((double)h2)
+                         && isfinite((double)h3);
+            }
         }
         if (!finite) warn |= kWarnNonFinite;
         if (!counts(P, x)) {  // ghost plane of an x-slab: no observables, no warnings
@@ -445,23 +561,28 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
 
 // GaugeCondition::postEvolveLocationAnalysis + Model::calcConstraintViolation
 // (Analysers/Source/GaugeCondition.cpp:117-165, Core/Source/Model.cpp:323-337).
-template <class S, int MODEL>
+template <class S, int MODEL, int HF>
 __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                         double* partials)
 {
     constexpr int NSC = (MODEL == kModelSM) ? 4 : 8;
+    constexpr int NEQ = hf_neq(HF);
+    constexpr int NG = 2 * NEQ;  // integrated then max |violation| per constraint
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int x = blockIdx.z;
-    double v[kGaussSlots];
+    double v[NG];
 #pragma unroll
-    for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
+    for (int k = 0; k < NG; k++) v[k] = 0.0;
     if (z < P.nz && y < P.ny && counts(P, x) && !frozen(P, x, y, z)) {
         const Nbr n = neighbours(P, x, y, z);
         const RefView<S> Vn{now};
         const RefView<S> Vf{fut};
-        // WilsonLoops::*::calcConstraintContributions (WilsonLoops/Source/StandardModel.cpp:274-322)
-        S el[4] = {(S)0, (S)0, (S)0, (S)0};
+        // WilsonLoops::*::calcConstraintContributions (WilsonLoops/Source/StandardModel.cpp:274-322,
+        // TwoHDM.cpp:312-396)
+        S el[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; k++) el[k] = (S)0;
         for (int d = 0; d < 3; d++) {
             const double la = Vf.th(d, n.c) - Vn.th(d, n.c);
             const double na = Vf.th(d, n.m[d]) - Vn.th(d, n.m[d]);
@@ -475,12 +596,29 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
             ref_su2_product(mul, p2, false, p2);
 #pragma unroll
             for (int k = 1; k < 4; k++) el[k] = el[k] + (S)((p1[k] - p2[k]) * P.lap[d]);
+            if (HF == kHfU1) {
+                const double hl = Vf.hth(d, n.c) - Vn.hth(d, n.c);
+                const double hn = Vf.hth(d, n.m[d]) - Vn.hth(d, n.m[d]);
+                el[4 % NEQ] = (S)((double)el[4 % NEQ] + (sin(hl) - sin(hn)) * P.lap[d]);
+            } else if (HF == kHfSU2) {
+                double q1[4], q2[4], mq[4];
+                Vf.hrep(d, n.c, false, q1);
+                Vn.hrep(d, n.c, true, mq);
+                ref_su2_product(mq, q1, false, q1);
+                Vn.hrep(d, n.m[d], true, q2);
+                Vf.hrep(d, n.m[d], false, mq);
+                ref_su2_product(mq, q2, false, q2);
+#pragma unroll
+                for (int k = 4; k < 7; k++) el[k % NEQ] = el[k % NEQ] + (S)((q1[k - 3] - q2[k - 3]) * P.lap[d]);
+            }
         }
         // Gradients::*::calcConstraintContributions (Gradients/Source/StandardModel.cpp:250-270, TwoHDM.cpp:329-373)
         S a[NSC], b[NSC];
         ref_load_scalar_S<NSC>(now, n.c, a);
         ref_load_scalar_S<NSC>(fut, n.c, b);
-        S gr[4] = {(S)0, (S)0, (S)0, (S)0};
+        S gr[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; k++) gr[k] = (S)0;
 #pragma unroll
         for (int db = 0; db < NSC; db += 4) {
             const S* p = a + db;
@@ -499,32 +637,72 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
                 gr[1] = (S)((double)gr[1] + 0.25 * (double)t1);
                 gr[2] = (S)((double)gr[2] + 0.25 * (double)t2);
                 gr[3] = (S)((double)gr[3] + 0.25 * (double)t3);
+                // Higgs-family charges (Gradients/Source/TwoHDM.cpp:355-372) over the full 8-vectors
+                const int i = db / 2;
+                if (HF == kHfU1) {
+                    const S h = a[i] * b[i + 1] - a[i + 1] * b[i] - a[i + 4] * b[i + 5] + a[i + 5] * b[i + 4];
+                    gr[4 % NEQ] = (S)((double)gr[4 % NEQ] + 0.25 * (double)h);
+                } else if (HF == kHfSU2) {
+                    const S h4 = a[i] * b[i + 5] - a[i + 1] * b[i + 4] + a[i + 4] * b[i + 1] - a[i + 5] * b[i];
+                    const S h5 = -a[i] * b[i + 4] - a[i + 1] * b[i + 5] + a[i + 4] * b[i] + a[i + 5] * b[i + 1];
+                    const S h6 = a[i] * b[i + 1] - a[i + 1] * b[i] - a[i + 4] * b[i + 5] + a[i + 5] * b[i + 4];
+                    gr[4 % NEQ] = (S)((double)gr[4 % NEQ] + 0.25 * (double)h4);
+                    gr[5 % NEQ] = (S)((double)gr[5 % NEQ] + 0.25 * (double)h5);
+                    gr[6 % NEQ] = (S)((double)gr[6 % NEQ] + 0.25 * (double)h6);
+                }
             }
         }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const S viol = el[k] - (S)P.gsq[k] * gr[k];
+        for (int k = 0; k < NEQ; k++) {
+            const S viol = el[k] - (S)(k < 4 ? P.gsq[k & 3] : P.gsq_hf) * gr[k];
             const double av = (double)(viol < (S)0 ? -viol : viol);
             v[k] = av;
-            v[4 + k] = av;
+            v[NEQ + k] = av;
         }
     }
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    block_reduce_store<kGaussSlots>(v, partials + (size_t)blk * kGaussSlots, 4);
+    block_reduce_store<NG>(v, partials + (size_t)blk * NG, NEQ);
 }
 
-}  // namespace
-
-template <class S, int MODEL>
-cudaError_t launch_ref_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
-                            double* partials, bool energy, cudaStream_t stream)
+template <class S, int MODEL, int HF>
+void ref_step_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                     double* partials, bool energy, cudaStream_t stream)
 {
     const dim3 block(32, 4, 1);
     const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
     if (energy)
-        ref_step_kernel<S, MODEL, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+        ref_step_kernel<S, MODEL, HF, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
     else
-        ref_step_kernel<S, MODEL, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+        ref_step_kernel<S, MODEL, HF, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+}
+
+template <class S, int MODEL, int HF>
+void ref_gauss_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
+                      cudaStream_t stream)
+{
+    const dim3 block(32, 4, 1);
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    ref_gauss_kernel<S, MODEL, HF><<<grid, block, 0, stream>>>(P, now, fut, partials);
+}
+
+}  // namespace
+
+// P.hf selects the Higgs-family variant (2HDM only); the Gauss kernel writes
+// 2 * gaugeNum partial slots per block.
+template <class S, int MODEL>
+cudaError_t launch_ref_step(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& past, unsigned* status,
+                            double* partials, bool energy, cudaStream_t stream)
+{
+    if constexpr (MODEL == kModel2HDM) {
+        if (P.hf == kHfU1)
+            ref_step_launch<S, MODEL, kHfU1>(P, now, past, status, partials, energy, stream);
+        else if (P.hf == kHfSU2)
+            ref_step_launch<S, MODEL, kHfSU2>(P, now, past, status, partials, energy, stream);
+        else
+            ref_step_launch<S, MODEL, kHfNone>(P, now, past, status, partials, energy, stream);
+    } else {
+        ref_step_launch<S, MODEL, kHfNone>(P, now, past, status, partials, energy, stream);
+    }
     return cudaGetLastError();
 }
 
@@ -532,9 +710,16 @@ template <class S, int MODEL>
 cudaError_t launch_ref_gauss(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
                              cudaStream_t stream)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
-    ref_gauss_kernel<S, MODEL><<<grid, block, 0, stream>>>(P, now, fut, partials);
+    if constexpr (MODEL == kModel2HDM) {
+        if (P.hf == kHfU1)
+            ref_gauss_launch<S, MODEL, kHfU1>(P, now, fut, partials, stream);
+        else if (P.hf == kHfSU2)
+            ref_gauss_launch<S, MODEL, kHfSU2>(P, now, fut, partials, stream);
+        else
+            ref_gauss_launch<S, MODEL, kHfNone>(P, now, fut, partials, stream);
+    } else {
+        ref_gauss_launch<S, MODEL, kHfNone>(P, now, fut, partials, stream);
+    }
     return cudaGetLastError();
 }
 

@@ -51,6 +51,68 @@ __device__ __forceinline__ Q<C> transport(Q<C> u, C cs, C sn, Q<C> f)
     return t;
 }
 
+// The isospin action alone (the 4x4 above on an already phase-rotated h); the
+// Higgs-family SU(2) acts with the same matrix on (doublet-1, doublet-2)
+// component pairs (Gradients/Source/TwoHDM.cpp:134-146).
+template <class C>
+__device__ __forceinline__ Q<C> su2_act(Q<C> u, Q<C> h)
+{
+    Q<C> t;
+    t.w = u.w * h.w - u.z * h.x + u.y * h.y - u.x * h.z;
+    t.x = u.z * h.w + u.w * h.x + u.x * h.y + u.y * h.z;
+    t.y = -u.y * h.w - u.x * h.x + u.w * h.y + u.z * h.z;
+    t.z = u.x * h.w - u.y * h.x - u.z * h.y + u.w * h.z;
+    return t;
+}
+
+// Phase rotation of both complex pairs of a doublet by (cos, sin).
+template <class C>
+__device__ __forceinline__ Q<C> rot2(Q<C> f, C cs, C sn)
+{
+    return {cs * f.w - sn * f.x, cs * f.x + sn * f.w, cs * f.y - sn * f.z, cs * f.z + sn * f.y};
+}
+
+// Higgs-family part of the 2HDM transport (Gradients/Source/TwoHDM.cpp:118-146),
+// applied to the two SM-transported doublets: U(1) = phase +theta_H on doublet 1
+// and -theta_H on doublet 2 ((hc, hs) = cos, sin of theta_H, hs negated for the
+// conjugate link); SU(2) = hu acting on (doublet 1, doublet 2) pairs.
+template <int HF, class C>
+__device__ __forceinline__ void hf_act(Q<C>& t1, Q<C>& t2, C hc, C hs, Q<C> hu)
+{
+    if constexpr (HF == kHfU1) {
+        t1 = rot2(t1, hc, hs);
+        t2 = rot2(t2, hc, -hs);
+    } else if constexpr (HF == kHfSU2) {
+        const Q<C> lo = su2_act(hu, Q<C>{t1.w, t1.x, t2.w, t2.x});
+        const Q<C> hi = su2_act(hu, Q<C>{t1.y, t1.z, t2.y, t2.z});
+        t1 = {lo.w, lo.x, hi.w, hi.x};
+        t2 = {lo.y, lo.z, hi.y, hi.z};
+    }
+}
+
+// Leapfrog update of one SU(2) link from the vector part (R1, R2, R3) of
+// u = U(t+dt) U(t)^dag (WilsonLoops/Source/StandardModel.cpp:478-504), written as
+// U + correction (see site_step); returns the new link, adds to `check`.
+template <class C>
+__device__ __forceinline__ Q<C> su2_advance(Q<C> Un, C R1, C R2, C R3, unsigned& warn, C& check)
+{
+    const C cm = R1 * R1 + R2 * R2 + R3 * R3;
+    if (cm > (C)1) warn |= kWarnSqrt;
+    const C u0m1 = sqrt1m_minus1(cm);
+    const Q<C> dU = qmul(Q<C>{u0m1, R1, R2, R3}, Un);
+    C e = fma(Un.w, Un.w, (C)-1);
+    e = fma(Un.x, Un.x, e);
+    e = fma(Un.y, Un.y, e);
+    e = fma(Un.z, Un.z, e);
+    const C udu = Un.w * dU.w + Un.x * dU.x + Un.y * dU.y + Un.z * dU.z;
+    const C dd = dU.w * dU.w + dU.x * dU.x + dU.y * dU.y + dU.z * dU.z;
+    e += (C)2 * udu + dd;
+    const C fm1 = e * ((C)0.375 * e - (C)0.5);
+    check += e;
+    return {Un.w + (dU.w + fm1 * (Un.w + dU.w)), Un.x + (dU.x + fm1 * (Un.x + dU.x)),
+            Un.y + (dU.y + fm1 * (Un.y + dU.y)), Un.z + (dU.z + fm1 * (Un.z + dU.z))};
+}
+
 // 1 - a0/|a| in the compute type without cancellation: |vec a|^2 / (|a| (|a| + a0))
 // when a0 >= 0, else 1 - a0/|a| directly (no cancellation there either).
 template <class C>
@@ -84,18 +146,22 @@ struct XCarry {
     Q<C> t0[ND];
 };
 
-// Own-site access to the past level (read, then overwritten with t + dt).
-template <class S>
+// Own-site access to the past level (read, then overwritten with t + dt).  LV is
+// LevelPtrs<S>, or any struct with its q / th / ph members when no Higgs-family
+// field is evolved.
+template <class S, class LV = LevelPtrs<S>>
 struct PastSite {
-    LevelPtrs<S> L;
+    LV L;
     int s;
 };
 
 // The per-site update.  A provides q(d, R) -> Q<C>, th(d, R) -> C, ph(k, R) -> Q<C>
-// for the "now" level.  obs receives the energy-step observables and warn the
-// warning bits, both only when `count` (the site is not on a ghost plane).
-template <class S, int MODEL, bool ENERGY, class A, class R>
-__device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S> ps,
+// for the "now" level (and hth / hq for a 2HDM Higgs-family field, HF != 0).
+// obs receives the energy-step observables and warn the warning bits, both only
+// when `count` (the site is not on a ghost plane).  With HF != 0 the x-carry is
+// not used (the caller passes an invalid one).
+template <class S, int MODEL, bool ENERGY, int HF = kHfNone, class A, class R, class LV>
+__device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S, LV> ps,
                                           XCarry<S, (MODEL == kModelSM) ? 1 : 2>& carry, double (&obs)[kObsCount],
                                           unsigned& warn, bool count = true)
 {
@@ -191,6 +257,77 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
             SB[i] = qadd_scaled(SB[i], lap[j], B);
         }
     }
+    // ---- Higgs-family magnetic term (WilsonLoops/Source/TwoHDM.cpp:484-551): the same
+    //      loops on theta_H (U(1)) or the family quaternion (SU(2)), coupling g'' ----
+    C MgH[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) MgH[i][0] = MgH[i][1] = MgH[i][2] = (C)0;
+    if constexpr (HF == kHfU1) {
+        C hc[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) hc[a] = acc.hth(a, n.c);
+#pragma unroll
+        for (int pl = 0; pl < 3; pl++) {
+            const int i = (pl == 2) ? 1 : 0;
+            const int j = (pl == 0) ? 1 : 2;
+            const C F = hc[i] + acc.hth(j, n.p[i]) - acc.hth(i, n.p[j]) - hc[j];
+            const C sF = gsin(F);
+            MgH[i][0] -= sF * lap[j];
+            MgH[j][0] += sF * lap[i];
+            if (ENERGY) {
+                const C hF = gsin((C)0.5 * F);
+                mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * (C)P.inv_gpp_sqr * ((C)2 * hF * hF);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if (j == i) continue;
+                const C neigh = -acc.hth(j, n.dg(i, j)) - acc.hth(i, n.m[j]) + acc.hth(j, n.m[j]) + hc[i];
+                MgH[i][0] -= gsin(neigh) * lap[j];
+            }
+        }
+    } else if constexpr (HF == kHfSU2) {
+        Q<C> UH[3], SAH[3], SBH[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            UH[a] = acc.hq(a, n.c);
+            SAH[a] = {(C)0, (C)0, (C)0, (C)0};
+            SBH[a] = {(C)0, (C)0, (C)0, (C)0};
+        }
+#pragma unroll
+        for (int pl = 0; pl < 3; pl++) {
+            const int i = (pl == 2) ? 1 : 0;
+            const int j = (pl == 0) ? 1 : 2;
+            const Q<C> Cij = qmul(qconj(acc.hq(j, n.p[i])), acc.hq(i, n.p[j]));
+            const Q<C> Aij = qmul(Cij, UH[j]);
+            const Q<C> Aji = qmul(qconj(Cij), UH[i]);
+            SAH[i] = qadd_scaled(SAH[i], lap[j], Aij);
+            SAH[j] = qadd_scaled(SAH[j], lap[i], Aji);
+            if (ENERGY)
+                mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * (C)P.inv_gpp_sqr * one_minus_trace(qmul(Aij, qconj(UH[i])));
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if (j == i) continue;
+                const Q<C> Bq = qmul(qmul(acc.hq(j, n.m[j]), qconj(acc.hq(i, n.m[j]))), qconj(acc.hq(j, n.dg(i, j))));
+                SBH[i] = qadd_scaled(SBH[i], lap[j], Bq);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            C a1, a2, a3, b1, b2, b3;
+            qmul_vec(SAH[i], qconj(UH[i]), a1, a2, a3);
+            qmul_vec(UH[i], SBH[i], b1, b2, b3);
+            MgH[i][0] = a1 - b1;
+            MgH[i][1] = a2 - b2;
+            MgH[i][2] = a3 - b3;
+        }
+    }
+
     C Mg[3][3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -213,7 +350,73 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         D[db] = {w * fc[db].w, w * fc[db].x, w * fc[db].y, w * fc[db].z};
     }
     C J[3][4];
+    C JH[3][3];  // Higgs-family currents (Gradients/Source/TwoHDM.cpp:465-485)
     C grad_e = (C)0;
+    if constexpr (HF != kHfNone) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            C sn, cs, smm, cmm;
+            gsincos(th[a], sn, cs);
+            gsincos(acc.th(a, n.m[a]), smm, cmm);
+            const Q<C> Um = acc.q(a, n.m[a]);
+            C hcs = (C)1, hsn = (C)0, hcm = (C)1, hsm = (C)0;
+            Q<C> uh = {(C)1, (C)0, (C)0, (C)0}, uhm = {(C)1, (C)0, (C)0, (C)0};
+            if constexpr (HF == kHfU1) {
+                gsincos(acc.hth(a, n.c), hsn, hcs);
+                gsincos(acc.hth(a, n.m[a]), hsm, hcm);
+            } else {
+                uh = acc.hq(a, n.c);
+                uhm = acc.hq(a, n.m[a]);
+            }
+            Q<C> tm[2], tp[2], t[2], fp[2];
+#pragma unroll
+            for (int db = 0; db < 2; db++) {
+                fp[db] = acc.ph(db, n.p[a]);
+                tm[db] = transport(Um, cmm, smm, acc.ph(db, n.m[a]));
+                tp[db] = transport(qconj(U[a]), cs, -sn, fp[db]);
+                t[db] = transport(U[a], cs, sn, fc[db]);
+            }
+            hf_act<HF>(tm[0], tm[1], hcm, hsm, uhm);
+            hf_act<HF>(tp[0], tp[1], hcs, -hsn, qconj(uh));
+            hf_act<HF>(t[0], t[1], hcs, hsn, uh);
+            C j0 = 0, j1 = 0, j2 = 0, j3 = 0;
+#pragma unroll
+            for (int db = 0; db < 2; db++) {
+                D[db] = qadd_scaled(D[db], lap[a], tm[db]);
+                D[db] = qadd_scaled(D[db], lap[a], tp[db]);
+                const Q<C> u = t[db], f = fp[db];
+                j0 += u.w * f.x - u.x * f.w + u.y * f.z - u.z * f.y;
+                j1 += u.w * f.z - u.x * f.y + u.y * f.x - u.z * f.w;
+                j2 += -u.w * f.y - u.x * f.z + u.y * f.w + u.z * f.x;
+                j3 += u.w * f.x - u.x * f.w - u.y * f.z + u.z * f.y;
+                if (ENERGY) {
+                    const C e0 = f.w - u.w, e1 = f.x - u.x, e2 = f.y - u.y, e3 = f.z - u.z;
+                    grad_e += (C)(0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                }
+            }
+            J[a][0] = (C)0.25 * j0;
+            J[a][1] = (C)0.25 * j1;
+            J[a][2] = (C)0.25 * j2;
+            J[a][3] = (C)0.25 * j3;
+            // family pairs: components (i, i+1) of doublet 1 and of doublet 2, i = 0 (upper) and 2 (lower)
+            const C t8[8] = {t[0].w, t[0].x, t[0].y, t[0].z, t[1].w, t[1].x, t[1].y, t[1].z};
+            const C n8[8] = {fp[0].w, fp[0].x, fp[0].y, fp[0].z, fp[1].w, fp[1].x, fp[1].y, fp[1].z};
+            C h4 = 0, h5 = 0, h6 = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i += 2) {
+                if constexpr (HF == kHfU1) {
+                    h4 += t8[i] * n8[i + 1] - t8[i + 1] * n8[i] - t8[i + 4] * n8[i + 5] + t8[i + 5] * n8[i + 4];
+                } else {
+                    h4 += t8[i] * n8[i + 5] - t8[i + 1] * n8[i + 4] + t8[i + 4] * n8[i + 1] - t8[i + 5] * n8[i];
+                    h5 += -t8[i] * n8[i + 4] - t8[i + 1] * n8[i + 5] + t8[i + 4] * n8[i] + t8[i + 5] * n8[i + 1];
+                    h6 += t8[i] * n8[i + 1] - t8[i + 1] * n8[i] - t8[i + 4] * n8[i + 5] + t8[i + 5] * n8[i + 4];
+                }
+            }
+            JH[a][0] = (C)0.25 * h4;
+            JH[a][1] = (C)0.25 * h5;
+            JH[a][2] = (C)0.25 * h6;
+        }
+    } else {
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         C sn, cs;
@@ -251,6 +454,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         J[a][1] = (C)0.25 * j1;
         J[a][2] = (C)0.25 * j2;
         J[a][3] = (C)0.25 * j3;
+    }
     }
 
     // ---- potential dV/dphi ----
@@ -387,6 +591,39 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         check += thn + e;
         ps.L.th[d][ps.s] = thn;
         st4(ps.L.q[d], ps.s, Unew.w, Unew.x, Unew.y, Unew.z);
+
+        // Higgs-family link (WilsonLoops/Source/TwoHDM.cpp:601-633, 702-745), coupling g''
+        if constexpr (HF == kHfU1) {
+            const C gH = (C)P.gsq_hf;
+            const C hn = acc.hth(d, n.c);
+            const C dh = hn - ld1<C>(ps.L.hth[d], ps.s);
+            const C RH = keep * gsin(dh) + dt2 * (MgH[d][0] + gH * JH[d][0]);
+            if (ENERGY) {
+                const C h = gsin((C)0.5 * dh);
+                elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) * (C)P.inv_gpp_sqr * ((C)2 * h * h);
+            }
+            if (RH * RH > (C)1) warn |= kWarnAsin;
+            if (fabs(hn) > (C)1e4) warn |= kWarnRange;
+            const C hnew = hn + gasin(RH);
+            check += hnew;
+            ps.L.hth[d][ps.s] = hnew;
+        } else if constexpr (HF == kHfSU2) {
+            const C gH = (C)P.gsq_hf;
+            const Q<C> Hn = acc.hq(d, n.c);
+            const Q<C> Hp = ld4<C>(ps.L.hq[d], ps.s);
+            const Q<C> dH = {Hn.w - Hp.w, Hn.x - Hp.x, Hn.y - Hp.y, Hn.z - Hp.z};
+            C F1, F2, F3;
+            qmul_vec(dH, qconj(Hp), F1, F2, F3);
+            const C H1 = keep * F1 + dt2 * (MgH[d][0] + gH * JH[d][0]);
+            const C H2 = keep * F2 + dt2 * (MgH[d][1] + gH * JH[d][1]);
+            const C H3 = keep * F3 + dt2 * (MgH[d][2] + gH * JH[d][2]);
+            if (ENERGY) {
+                const Q<C> Ed = {Hn.w * Hp.w + Hn.x * Hp.x + Hn.y * Hp.y + Hn.z * Hp.z, F1, F2, F3};
+                elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) * (C)P.inv_gpp_sqr * one_minus_trace(Ed);
+            }
+            const Q<C> Hnew = su2_advance(Hn, H1, H2, H3, warn, check);
+            st4(ps.L.hq[d], ps.s, Hnew.w, Hnew.x, Hnew.y, Hnew.z);
+        }
     }
     if (!isfinite(check)) warn |= kWarnNonFinite;
     carry.valid = true;
@@ -421,17 +658,17 @@ struct GLink {
     double tnow, tfut;
 };
 
-template <class S>
-__device__ __forceinline__ GLink gauss_link(const LevelPtrs<S>& now, const LevelPtrs<S>& fut, int d, int s)
+template <class S, class LV>
+__device__ __forceinline__ GLink gauss_link(const LV& now, const LV& fut, int d, int s)
 {
     return {ld4<double>(now.q[d], s), ld4<double>(fut.q[d], s), ld1<double>(now.th[d], s), ld1<double>(fut.th[d], s)};
 }
 
 // The residuals from the links at x (own[d]) and at x - e_d (back[d]) and the
 // doublets at x (site c).
-template <class S, int MODEL>
+template <class S, int MODEL, class LV>
 __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&own)[3], const GLink (&back)[3],
-                                           const LevelPtrs<S>& now, const LevelPtrs<S>& fut, int c,
+                                           const LV& now, const LV& fut, int c,
                                            double (&v)[kGaussSlots])
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
@@ -467,13 +704,65 @@ __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&ow
     }
 }
 
-template <class S, int MODEL>
-__device__ __forceinline__ void gauss_site(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut,
-                                           int c, int md0, int md1, int md2, double (&v)[kGaussSlots])
+// v = |violation| of the 2 * gaugeNum slots (integrated then maximum) per
+// constraint; with a Higgs-family field (HF != 0) the constraints 4.. of
+// WilsonLoops/Source/TwoHDM.cpp:357-392 and Gradients/Source/TwoHDM.cpp:355-372 follow.
+template <class S, int MODEL, int HF = kHfNone, class LV>
+__device__ __forceinline__ void gauss_site(const StepParams& P, const LV& now, const LV& fut,
+                                           int c, int md0, int md1, int md2, double (&v)[2 * hf_neq(HF)])
 {
-    const GLink own[3] = {gauss_link(now, fut, 0, c), gauss_link(now, fut, 1, c), gauss_link(now, fut, 2, c)};
-    const GLink back[3] = {gauss_link(now, fut, 0, md0), gauss_link(now, fut, 1, md1), gauss_link(now, fut, 2, md2)};
-    gauss_core<S, MODEL>(P, own, back, now, fut, c, v);
+    const GLink own[3] = {gauss_link<S>(now, fut, 0, c), gauss_link<S>(now, fut, 1, c), gauss_link<S>(now, fut, 2, c)};
+    const GLink back[3] = {gauss_link<S>(now, fut, 0, md0), gauss_link<S>(now, fut, 1, md1), gauss_link<S>(now, fut, 2, md2)};
+    if constexpr (HF == kHfNone) {
+        gauss_core<S, MODEL>(P, own, back, now, fut, c, v);
+    } else {
+        constexpr int NEQ = hf_neq(HF);
+        double vs[kGaussSlots];
+        gauss_core<S, MODEL>(P, own, back, now, fut, c, vs);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            v[k] = vs[k];
+            v[NEQ + k] = vs[4 + k];
+        }
+        const int md[3] = {md0, md1, md2};
+        double el[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if constexpr (HF == kHfU1) {
+                const double la = ld1<double>(fut.hth[d], c) - ld1<double>(now.hth[d], c);
+                const double na = ld1<double>(fut.hth[d], md[d]) - ld1<double>(now.hth[d], md[d]);
+                el[0] += (gsin(la) - gsin(na)) * P.lap[d];
+            } else {
+                double a1, a2, a3, b1, b2, b3;
+                qmul_vec(qconj(ld4<double>(now.hq[d], c)), ld4<double>(fut.hq[d], c), a1, a2, a3);
+                qmul_vec(ld4<double>(fut.hq[d], md[d]), qconj(ld4<double>(now.hq[d], md[d])), b1, b2, b3);
+                el[0] += (a1 - b1) * P.lap[d];
+                el[1] += (a2 - b2) * P.lap[d];
+                el[2] += (a3 - b3) * P.lap[d];
+            }
+        }
+        const Q<double> p1 = ld4<double>(now.ph[0], c), p2 = ld4<double>(now.ph[1], c);
+        const Q<double> q1 = ld4<double>(fut.ph[0], c), q2 = ld4<double>(fut.ph[1], c);
+        const double a8[8] = {p1.w, p1.x, p1.y, p1.z, p2.w, p2.x, p2.y, p2.z};
+        const double b8[8] = {q1.w, q1.x, q1.y, q1.z, q2.w, q2.x, q2.y, q2.z};
+        double gr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < 4; i += 2) {
+            if constexpr (HF == kHfU1) {
+                gr[0] += 0.25 * (a8[i] * b8[i + 1] - a8[i + 1] * b8[i] - a8[i + 4] * b8[i + 5] + a8[i + 5] * b8[i + 4]);
+            } else {
+                gr[0] += 0.25 * (a8[i] * b8[i + 5] - a8[i + 1] * b8[i + 4] + a8[i + 4] * b8[i + 1] - a8[i + 5] * b8[i]);
+                gr[1] += 0.25 * (-a8[i] * b8[i + 4] - a8[i + 1] * b8[i + 5] + a8[i + 4] * b8[i] + a8[i + 5] * b8[i + 1]);
+                gr[2] += 0.25 * (a8[i] * b8[i + 1] - a8[i + 1] * b8[i] - a8[i + 4] * b8[i + 5] + a8[i + 5] * b8[i + 4]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NEQ - 4; k++) {
+            const double av = fabs(el[k] - P.gsq_hf * gr[k]);
+            v[4 + k] = av;
+            v[NEQ + 4 + k] = av;
+        }
+    }
 }
 
 }  // namespace gft

@@ -206,8 +206,8 @@ __device__ __forceinline__ bool halo_cell(int tid, int& ly, int& lz)
 
 // Warm L2 with the wrapped halo sites of plane X (one plane before they are
 // patched), so the patch loads do not wait on DRAM.
-template <class S, int TY, int TZ, int ND>
-__device__ __forceinline__ void prefetch_wrapped_halo(const StepParams& P, const LevelPtrs<S>& now, int X, int y0,
+template <class S, int TY, int TZ, int ND, class LV>
+__device__ __forceinline__ void prefetch_wrapped_halo(const StepParams& P, const LV& now, int X, int y0,
                                                       int z0, int tid)
 {
     using G = Geom<S, TY, TZ, ND>;
@@ -229,8 +229,8 @@ __device__ __forceinline__ void prefetch_wrapped_halo(const StepParams& P, const
 
 // Halo cells of plane X whose (y, z) leaves the lattice: load the wrapped
 // site from global memory into the staged plane.
-template <class S, int TY, int TZ, int ND>
-__device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const LevelPtrs<S>& now, unsigned char* buf,
+template <class S, int TY, int TZ, int ND, class LV>
+__device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const LV& now, unsigned char* buf,
                                                    int X, int y0, int z0, int tid)
 {
     using G = Geom<S, TY, TZ, ND>;
@@ -266,10 +266,11 @@ struct RingPhase {
 // Evolves one tile (planes x0 .. x0+nloc-1 of columns y0.., z0..) by one step.
 // smem: NBUF plane buffers followed by NBUF initialised mbarriers; s_abort: a
 // shared flag that is 0 on entry.  Returns false (on every thread) if a wait
-// gave up; the ring is then drained and must not be reused.
-template <class S, int MODEL, int TY, int TZ, bool ENERGY>
+// gave up; the ring is then drained and must not be reused.  LV: the level
+// pointer struct (its q / th / ph members are read).
+template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV>
 __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
-                                         const LevelPtrs<S>& now, const LevelPtrs<S>& past, int y0, int z0, int x0,
+                                         const LV& now, const LV& past, int y0, int z0, int x0,
                                          int nloc, unsigned char* smem, unsigned long long* bars, RingPhase& ring,
                                          int* s_abort, double (&obs)[kObsCount], unsigned& warn)
 {
@@ -341,7 +342,7 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
             carry.valid = false;
         else
-            site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S>{past, s}, carry, obs, warn,
+            site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs, warn,
                                         counts(P, x));
 
         // plane i+3 (x+2) for the next site; its copy was issued one plane ago

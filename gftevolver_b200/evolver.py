@@ -4,7 +4,9 @@
 parameters, the step counter and the analysers' logging cadence -- the state
 the reference keeps in ``Lattice`` and ``Model`` (Core/Header/Lattice.hpp:22-212,
 Core/Header/Model.hpp:23-266).  Host arrays use the reference layout
-``scalars[2, nx, ny, nz, nsc]``, ``vectors[2, nx, ny, nz, 15]``.
+``scalars[2, nx, ny, nz, nsc]``, ``vectors[2, nx, ny, nz, 3 * dw]`` (dw = 5 link
+words per direction, 6 or 9 with a 2HDM Higgs-family U(1) phase or SU(2)
+quaternion, ``WilsonLoops/Source/TwoHDM.cpp:210-242``).
 """
 from __future__ import annotations
 
@@ -38,7 +40,7 @@ class LatticeParams:
     dt: float = 0.05
     g: float = 0.65
     gp: float = 0.35
-    gpp: float = 0.5           # Higgs-family coupling (TwoHDM gaugeNum 5/7; unused by the built models)
+    gpp: float = 0.5           # Higgs-family coupling g'' (TwoHDM gaugeNum 5/7)
     div_tol: float = 1e-9
     damping: float = 0.0
     nt_damped: int = 0
@@ -65,10 +67,21 @@ class LatticeParams:
     energy_every: int = 0
     gauss_every: int = 0
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (frozen shell), else periodic
+    higgs_family: int = 0      # 2HDM Higgs-family gauge field: 0 none, 1 U(1) (gaugeNum 5), 2 SU(2) (gaugeNum 7)
 
     @property
     def nsc(self) -> int:
         return 4 if self.model == _lib.GFT_MODEL_SM else 8
+
+    @property
+    def nve(self) -> int:
+        """Link words per site in the reference layout (3 directions x 5, 6 or 9)."""
+        return 3 * {0: 5, 1: 6, 2: 9}[self.higgs_family]
+
+    @property
+    def neq(self) -> int:
+        """Gauge equations per direction = Gauss constraints per row (gaugeNum)."""
+        return {0: 4, 1: 5, 2: 7}[self.higgs_family]
 
     @property
     def nsite(self) -> int:
@@ -94,12 +107,12 @@ class InitialData:
 ROW_KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric")
 
 
-def _row_dict(r: _lib.GftObservables) -> dict:
+def _row_dict(r: _lib.GftObservables, neq: int = 4) -> dict:
     d = {"time_iter": r.time_iter, "has_energy": bool(r.has_energy), "has_gauss": bool(r.has_gauss)}
     for k in ROW_KEYS:
         d[k] = r.__getattribute__(k)
-    d["gauss_int"] = list(r.gauss_int)
-    d["gauss_max"] = list(r.gauss_max)
+    d["gauss_int"] = list(r.gauss_int)[:neq]
+    d["gauss_max"] = list(r.gauss_max)[:neq]
     d["plaq_su2"], d["plaq_u1"], d["phi_sq"] = r.plaq_su2, r.plaq_u1, r.phi_sq
     return d
 
@@ -181,7 +194,7 @@ class Evolver:
     # -- fields --------------------------------------------------------------
     def _shapes(self):
         p = self.params
-        return (2, p.nx, p.ny, p.nz, p.nsc), (2, p.nx, p.ny, p.nz, 15)
+        return (2, p.nx, p.ny, p.nz, p.nsc), (2, p.nx, p.ny, p.nz, p.nve)
 
     def upload(self, scalars: np.ndarray, vectors: np.ndarray, time_iter: int = 0) -> None:
         ss, vs = self._shapes()
@@ -258,7 +271,7 @@ class Evolver:
         n = ctypes.c_int(0)
         self.last_warnings = _lib.check(
             self.lib.gft_evolve(self.h, int(n_steps), rows, int(max_rows), ctypes.byref(n)), self.h)
-        return [_row_dict(rows[i]) for i in range(n.value)]
+        return [_row_dict(rows[i], self.params.neq) for i in range(n.value)]
 
     def set_kernel(self, kind: int = 0, tile: int = 0, march: int = 32) -> None:
         """Step kernel of the throughput forms: 0 auto, 1 one thread per site, 2 TMA-staged tiles."""
@@ -267,7 +280,7 @@ class Evolver:
     def observe(self) -> dict:
         r = _lib.GftObservables()
         _lib.check(self.lib.gft_observe(self.h, ctypes.byref(r)), self.h)
-        return _row_dict(r)
+        return _row_dict(r, self.params.neq)
 
     @property
     def time_iter(self) -> int:

@@ -151,7 +151,15 @@ Run configure(const std::string& root)
             throw std::runtime_error("faces of axis " + std::to_string(a) +
                                      ": only periodic (3 3) or Fixed (1 1) pairs run on the GPU");
     }
-    if (nvec != 5) throw std::runtime_error("only the quaternion link representation (5 components) runs on the GPU");
+    // link words per direction: 5 (gaugeNum 4), 6 (+ Higgs-family U(1)), 9 (+ Higgs-family SU(2))
+    // in the quaternion representation (WilsonLoops/Source/TwoHDM.cpp:229-241)
+    if (nvec == 6)
+        c.higgs_family = GFT_HF_U1;
+    else if (nvec == 9)
+        c.higgs_family = GFT_HF_SU2;
+    else if (nvec != 5)
+        throw std::runtime_error("vector components per direction: 5, 6 or 9 (quaternion representation) run on the "
+                                 "GPU, not " + std::to_string(nvec));
 
     // Core/Config/Model.cfg (Core/Source/Model.cpp:173-221)
     const std::string mod = root + "/Core/Config/Model.cfg";
@@ -165,6 +173,8 @@ Run configure(const std::string& root)
         throw std::runtime_error("model (potential " + std::to_string(pot) + ", gradient " + std::to_string(grad) +
                                  ", wilson loop " + std::to_string(wl) + ", " + std::to_string(nsc) +
                                  " scalars) is not built for the GPU");
+    if (c.higgs_family != GFT_HF_NONE && c.model != GFT_MODEL_2HDM)
+        throw std::runtime_error(std::to_string(nvec) + " vector components per direction need the 2HDM (TwoHDM wilson loops)");
     c.damping = (float)num(M, 3, 0, mod);
     c.nt_damped = inum(M, 4, 0, mod);
     if (inum(M, 5, 0, mod)) c.nt_damped = static_cast<int>((float)num(M, 6, 0, mod) / c.dt);
@@ -209,6 +219,7 @@ Run configure(const std::string& root)
         const Entries W = read_cfg(w, 12);
         c.g = num(W, 0, 0, w);
         c.gp = num(W, 1, 0, w);
+        c.gpp = num(W, 2, 0, w);
         if (inum(W, 3, 0, w)) throw std::runtime_error("the generator link representation does not run on the GPU");
         c.div_tol = num(W, 4, 0, w);
     }
@@ -265,14 +276,19 @@ void dump_fields(const std::string& path, const std::vector<T>& sc, const std::v
 {
     std::ofstream ofs(path);
     const size_t nsite2 = sc.size() / nsc;
+    const size_t nve = ve.size() / nsite2;
     const size_t n = both ? nsite2 : nsite2 / 2;
     const size_t t0 = both ? 0 : (size_t)((time_step + 1) % 2) * n;
     for (size_t s = t0; s < t0 + n; s++) {
         for (int k = 0; k < nsc; k++) ofs << sc[s * nsc + k] << " ";
-        for (int k = 0; k < 15; k++) ofs << ve[s * 15 + k] << " ";
+        for (size_t k = 0; k < nve; k++) ofs << ve[s * nve + k] << " ";
         ofs << std::endl;
     }
 }
+
+// Link words per site and gauge equations per direction of a configuration.
+int vector_words(const gft_config& c) { return 3 * (c.higgs_family == GFT_HF_U1 ? 6 : (c.higgs_family == GFT_HF_SU2 ? 9 : 5)); }
+int gauss_count(const gft_config& c) { return c.higgs_family == GFT_HF_U1 ? 5 : (c.higgs_family == GFT_HF_SU2 ? 7 : 4); }
 
 // RandomUniform::setInitialFields: one std::mt19937 stream per field array from
 // the configured seed, float uniform in [lo, hi) as the reference stores it
@@ -313,8 +329,12 @@ void host_initial(const Run& r, const std::string& ic_path, std::vector<T>& sc, 
     }
     std::fill(sc.begin(), sc.end(), (T)0);
     std::fill(ve.begin(), ve.end(), (T)0);
-    for (size_t s = 0; s < ve.size() / 15; s++)
-        for (int d = 0; d < 3; d++) ve[s * 15 + d * 5 + 1] = (T)1;  // identity SU(2) links
+    const int nve = vector_words(r.cfg), dw = nve / 3;
+    for (size_t s = 0; s < ve.size() / nve; s++)
+        for (int d = 0; d < 3; d++) {
+            ve[s * nve + d * dw + 1] = (T)1;               // identity isospin link
+            if (dw == 9) ve[s * nve + d * dw + 5] = (T)1;  // identity Higgs-family SU(2) link
+        }
     if (r.ic.type[0] == 1) random_uniform(sc, r.ic);
     if (r.ic.type[1] == 1) random_uniform(ve, r.ic);
 }
@@ -326,7 +346,7 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
     gft_config& c = r.cfg;
     const int nsc = (c.model == GFT_MODEL_SM) ? 4 : 8;
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
-    std::vector<T> sc(2 * nsite * nsc), ve(2 * nsite * 15);
+    std::vector<T> sc(2 * nsite * nsc), ve(2 * nsite * vector_words(c));
     if (initial_only) {  // the host-built initial data alone, no device
         if (seed >= 0) throw std::runtime_error("--initial-only builds host initial data; drop --device-ic");
         host_initial(r, ic_path, sc, ve);
@@ -392,9 +412,9 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
             if (o.has_gauss && !r.an.gauss_path.empty()) {
                 std::ofstream ofs(data + "/" + r.an.gauss_path, std::ios::app);
                 if (r.an.gauss_opt[0])
-                    for (int k = 0; k < 4; k++) ofs << o.gauss_int[k] << " ";
+                    for (int k = 0; k < gauss_count(c); k++) ofs << o.gauss_int[k] << " ";
                 if (r.an.gauss_opt[1])
-                    for (int k = 0; k < 4; k++) ofs << o.gauss_max[k] << " ";
+                    for (int k = 0; k < gauss_count(c); k++) ofs << o.gauss_max[k] << " ";
                 ofs << "\n";
             }
         }
@@ -471,6 +491,7 @@ int main(int argc, char** argv)
                         c.energy_offset);
             std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s fixed_axes %d\n", c.energy_every,
                         c.gauss_every, r.an.energy_path.c_str(), r.an.gauss_path.c_str(), c.fixed_axes);
+            std::printf("higgs_family %d gpp %.17g\n", c.higgs_family, c.gpp);
             std::printf("ic_scalar %d ic_gauge %d ic_seed %u ic_min %.9g ic_max %.9g ic_equal %d\n", r.ic.type[0],
                         r.ic.type[1], r.ic.seed, r.ic.lo, r.ic.hi, (int)r.ic.equal);
             return 0;

@@ -125,8 +125,9 @@ def combine_rows(rows: list[dict], own_sites: int, group=None, device=None) -> l
     if not rows or not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
         return rows
     n = len(rows)
-    sums = torch.zeros((n, len(ROW_SUMS) + len(ROW_MEANS) + 5), dtype=torch.float64)
-    maxs = torch.zeros((n, 4), dtype=torch.float64)
+    neq = len(rows[0]["gauss_int"])  # Gauss constraints per row (gaugeNum)
+    sums = torch.zeros((n, len(ROW_SUMS) + len(ROW_MEANS) + neq + 1), dtype=torch.float64)
+    maxs = torch.zeros((n, neq), dtype=torch.float64)
     for i, r in enumerate(rows):
         vals = [r[k] for k in ROW_SUMS] + [r[k] * own_sites for k in ROW_MEANS] + list(r["gauss_int"]) + [own_sites]
         sums[i] = torch.tensor(vals, dtype=torch.float64)
@@ -145,7 +146,7 @@ def combine_rows(rows: list[dict], own_sites: int, group=None, device=None) -> l
             o[k] = s[j]
         for j, k in enumerate(ROW_MEANS):
             o[k] = s[len(ROW_SUMS) + j] / total
-        o["gauss_int"] = s[len(ROW_SUMS) + len(ROW_MEANS):len(ROW_SUMS) + len(ROW_MEANS) + 4]
+        o["gauss_int"] = s[len(ROW_SUMS) + len(ROW_MEANS):len(ROW_SUMS) + len(ROW_MEANS) + neq]
         o["gauss_max"] = maxs[i].tolist()
         out.append(o)
     return out
@@ -204,9 +205,9 @@ class SlabEvolver:
         key = (level, x)
         if key not in self._views:
             import torch
-            ptrs = (ctypes.c_void_p * 8)()
-            sizes = (ctypes.c_size_t * 8)()
-            n = _lib.check(self.local.lib.gft_level_planes(self.local.h, level, x, ptrs, sizes, 8), self.local.h)
+            ptrs = (ctypes.c_void_p * 11)()  # at most 11 arrays (2HDM with a Higgs-family field)
+            sizes = (ctypes.c_size_t * 11)()
+            n = _lib.check(self.local.lib.gft_level_planes(self.local.h, level, x, ptrs, sizes, 11), self.local.h)
             self._views[key] = [
                 torch.as_tensor(_DeviceBuffer(ptrs[k], sizes[k], self._typestr, self._itemsize),
                                 device=f"cuda:{self.device}")

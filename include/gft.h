@@ -13,8 +13,10 @@
  *
  * Conventions
  *   - Host field buffers use the reference layout (Lattice.cpp:358-367,
- *     658-671): scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][15] with
- *     per direction [theta_Y, c0, c1, c2, c3] (quaternion representation).
+ *     658-671): scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][3 * dw] with
+ *     per direction [theta_Y, c0, c1, c2, c3] (quaternion representation, dw = 5),
+ *     followed for a 2HDM Higgs-family gauge field by theta_H (dw = 6) or the
+ *     family quaternion d0..d3 (dw = 9) (WilsonLoops/Source/TwoHDM.cpp:210-242).
  *     Level index = the reference's time slot; at time step time_iter the
  *     "now" slot is (time_iter + 1) % 2 (Lattice.cpp:773-774).
  *   - Device memory is owned by the handle; host buffers are caller-owned and
@@ -53,7 +55,13 @@ extern "C" {
 /* ---- model / form selectors -------------------------------------------- */
 /* Model.cfg plugin triples (Core/Header/Model.hpp:19-21) that are built. */
 #define GFT_MODEL_SM 1    /* SO_N potential + Gradients::StandardModel + WilsonLoops::StandardModel */
-#define GFT_MODEL_2HDM 2  /* Double_SO_N + Gradients::TwoHDM + WilsonLoops::TwoHDM (gaugeNum = 4) */
+#define GFT_MODEL_2HDM 2  /* Double_SO_N + Gradients::TwoHDM + WilsonLoops::TwoHDM (gaugeNum 4, 5 or 7) */
+
+/* 2HDM Higgs-family gauge field (gft_config.higgs_family; WilsonLoops/Source/TwoHDM.cpp:210-242). */
+#define GFT_HF_NONE 0     /* gaugeNum 4: SU(2) x U(1) only (5 link words per direction) */
+#define GFT_HF_U1 1       /* gaugeNum 5: + a family U(1) phase theta_H (6 words) */
+#define GFT_HF_SU2 2      /* gaugeNum 7: + a family SU(2) quaternion (9 words) */
+#define GFT_MAX_GAUSS 7   /* Gauss constraint equations at most (gaugeNum) */
 
 /* Arithmetic forms. */
 #define GFT_FORM_REF 0    /* reference arithmetic: per-site math in FP64 in the reference's operation
@@ -85,18 +93,21 @@ typedef struct gft_config {
                                       are Fixed (type 1), clear = periodic (type 3).  Sites on a Fixed
                                       face are not evolved and not counted by the analysers
                                       (BoundaryConditions/Source/Fixed.cpp:159-251, Core/Source/Lattice.cpp:217-306). */
+    int higgs_family;              /* GFT_HF_*: 2HDM Higgs-family gauge field (model 2 only) */
+    double gpp;                    /* its coupling g'' (WilsonLoops/Config/TwoHDM.cfg) */
 } gft_config;
 
 /* One row of global observables (Analysers/Source/Energy.cpp:169-220,
  * Analysers/Source/GaugeCondition.cpp:167-226).  Energies are integrated over
  * the lattice (sum x dx dy dz); the Gauss entries are the integrated and the
- * maximum |violation| per constraint equation.  plaq_* and phi_sq are means
- * with no reference counterpart. */
+ * maximum |violation| per constraint equation (gaugeNum of them: hypercharge,
+ * isospin 1..3, then the Higgs family; unused entries 0).  plaq_* and phi_sq
+ * are means with no reference counterpart. */
 typedef struct gft_observables {
     int time_iter;
     int has_energy, has_gauss;
     double energy, potential, gradient, kinetic, magnetic, electric;
-    double gauss_int[4], gauss_max[4];
+    double gauss_int[GFT_MAX_GAUSS], gauss_max[GFT_MAX_GAUSS];
     double plaq_su2, plaq_u1, phi_sq;
 } gft_observables;
 
@@ -105,7 +116,8 @@ typedef struct gft_observables {
  * Both time levels are set equal (E = 0, pi = 0).  Scalars: component c ~
  * N(mean[c], sigma[c]^2), plus a periodic tanh double wall on component 0 when
  * wall_width > 0.  Links: theta_Y ~ N(0, theta_sigma^2); SU(2) =
- * (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform on S^2. */
+ * (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform on S^2; a
+ * Higgs-family phase ~ N(0, theta_sigma^2) or quaternion drawn like the SU(2) link. */
 typedef struct gft_ic {
     uint64_t seed;
     double mean[8], sigma[8];
@@ -189,8 +201,9 @@ typedef int (*gft_exchange_fn)(gft_handle* h, int level, void* user);
 int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user);
 
 /* Device addresses and byte sizes of plane x of every field array of a level
- * (3 quaternion arrays, 3 phase arrays, 1 or 2 doublet arrays, in that order);
- * returns the number of arrays (7 or 8). */
+ * (3 quaternion arrays, 3 phase arrays, 1 or 2 doublet arrays, then 3
+ * Higgs-family arrays when present, in that order); returns the number of
+ * arrays (7, 8 or 11). */
 int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes, int max);
 
 /* Allocation-free observables (no counterpart in the reference).  For callers
@@ -208,8 +221,8 @@ int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes
  * The first call on a device looks up that array's address (do it before any
  * stream capture); calls that overlap on the GPU share the array and race, so
  * the caller serialises them.  Only cfg's lattice, model and coupling fields
- * are read (form and storage_bytes are ignored); periodic lattices only
- * (fixed_axes != 0 returns GFT_E_UNSUPPORTED). */
+ * are read (form and storage_bytes are ignored); periodic lattices without a
+ * Higgs-family field only (otherwise GFT_E_UNSUPPORTED). */
 int gft_observe_static(const gft_config* cfg, const float* d_scalars, const float* d_vectors, int time_iter,
                        double* d_out, void* stream);
 
@@ -219,7 +232,8 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
  * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
  * marching along x (mixed form).  tile = tile shape (0: 8 x 32, 1: 4 x 32,
  * 2: 4 x 16, 3: 16 x 16 sites in y x z); march = planes per CTA along x.  Returns
- * GFT_E_UNSUPPORTED when the lattice does not divide into the tile. */
+ * GFT_E_UNSUPPORTED when the lattice does not divide into the tile or carries a
+ * Higgs-family field (one thread per site serves those). */
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
 /* Diagnostic with no reference counterpart: evaluates the library's own
@@ -234,7 +248,8 @@ int gft_selftest_math(int device, double* out);
  * one object, evolved together by ONE persistent kernel launch per time step
  * (no reference counterpart: the reference runs one lattice per process,
  * Core/Source/Lattice.cpp:755-876).  All members share the model, the device,
- * the analysers' cadence and the step counter; the form is GFT_FORM_MIXED; the
+ * the analysers' cadence and the step counter; the form is GFT_FORM_MIXED, with
+ * no Higgs-family field; the
  * members' (ny, nz) must share a tile shape (ny % 4 == 0 and nz % 16 == 0 at
  * least).  Each member evolves exactly as a single handle would with the same
  * tile shape and march depth (gft_set_kernel). */

@@ -52,7 +52,7 @@ class OrcConfig(ctypes.Structure):
         ("energy_offset", ctypes.c_double),
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
         ("fixed_axes", ctypes.c_int),
-        ("hf", ctypes.c_int), ("gpp", ctypes.c_double),
+        ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
     ]
 
 
@@ -110,7 +110,7 @@ class Params:
     energy_every: int = 0
     gauss_every: int = 0
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (else periodic)
-    hf: int = HF_NONE          # 2HDM Higgs-family gauge field (HF_*)
+    higgs_family: int = HF_NONE  # 2HDM Higgs-family gauge field (HF_*)
 
     @property
     def nsc(self) -> int:
@@ -119,7 +119,7 @@ class Params:
     @property
     def dw(self) -> int:
         """Link words per direction."""
-        return {HF_NONE: 5, HF_U1: 6, HF_SU2: 9}[self.hf]
+        return {HF_NONE: 5, HF_U1: 6, HF_SU2: 9}[self.higgs_family]
 
     @property
     def nve(self) -> int:
@@ -128,7 +128,7 @@ class Params:
     @property
     def neq(self) -> int:
         """Gauge equations per direction = Gauss constraints (gaugeNum)."""
-        return {HF_NONE: 4, HF_U1: 5, HF_SU2: 7}[self.hf]
+        return {HF_NONE: 4, HF_U1: 5, HF_SU2: 7}[self.higgs_family]
 
     @property
     def nsite(self) -> int:

@@ -52,10 +52,10 @@ CASES = {
     "2hdm_fixed_y_5x6x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=6, nz=4, energy_every=2, gauss_every=2, fixed_axes=2),
                            dict(seed=20, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 6, ("f32",)),
     # 2HDM with a Higgs-family gauge field: U(1) (gaugeNum 5) and SU(2) (gaugeNum 7), coupling g''
-    "2hdm_hf_u1_4x5x3": (dict(model=orc.MODEL_2HDM, nx=4, ny=5, nz=3, energy_every=2, gauss_every=3, hf=orc.HF_U1,
+    "2hdm_hf_u1_4x5x3": (dict(model=orc.MODEL_2HDM, nx=4, ny=5, nz=3, energy_every=2, gauss_every=3, higgs_family=orc.HF_U1,
                               gpp=0.47),
                          dict(seed=21, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
-    "2hdm_hf_su2_5x3x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=3, nz=4, energy_every=3, gauss_every=2, hf=orc.HF_SU2,
+    "2hdm_hf_su2_5x3x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=3, nz=4, energy_every=3, gauss_every=2, higgs_family=orc.HF_SU2,
                                gpp=0.52),
                           dict(seed=22, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
 }

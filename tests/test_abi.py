@@ -75,6 +75,15 @@ def test_create_rejects_invalid_config_without_gpu(lib):
     cfg.model = 1
     cfg.nx = 0
     assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
+    # a Higgs-family gauge field exists in the 2HDM only (WilsonLoops::TwoHDM); 0..2
+    cfg.nx = 4
+    cfg.form = _lib.GFT_FORM_MIXED
+    cfg.higgs_family = _lib.GFT_HF_U1
+    assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
+    assert b"2HDM" in lib.gft_last_error(None)
+    cfg.model = _lib.GFT_MODEL_2HDM
+    cfg.higgs_family = 3
+    assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
     assert not h.value
 
 
@@ -97,4 +106,8 @@ def test_batch_create_validates_members_without_gpu(lib):
     cfgs = (_lib.GftConfig * 2)(make_config(a), make_config(d))
     assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
     assert lib.gft_batch_create(cfgs, 0, ctypes.byref(h)) == _lib.GFT_E_INVALID
+    e = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, model=_lib.GFT_MODEL_2HDM, higgs_family=_lib.GFT_HF_SU2)
+    cfgs = (_lib.GftConfig * 1)(make_config(e))
+    assert lib.gft_batch_create(cfgs, 1, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
+    assert b"Higgs-family" in lib.gft_last_error(None)
     assert not h.value

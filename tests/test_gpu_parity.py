@@ -138,6 +138,75 @@ def test_forms_vs_oracle_random(oracle_mod, model, shape, fixed):
     assert ulp_close(ve, o32_ve, 8).all()
 
 
+@pytest.mark.parametrize("hf", [1, 2], ids=["hf_u1", "hf_su2"])
+@pytest.mark.parametrize("shape,fixed", [((8, 8, 8), 0), ((5, 6, 7), 0), ((6, 8, 12), 2)])
+def test_higgs_family_forms_vs_oracle(oracle_mod, hf, shape, fixed):
+    """2HDM with a Higgs-family U(1) (gaugeNum 5) or SU(2) (gaugeNum 7) gauge field,
+    random links of both groups, 10 steps: every form against the oracle, the
+    Gauss rows with all gaugeNum constraints."""
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=2, nx=nx, ny=ny, nz=nz, energy_every=5, gauss_every=5, fixed_axes=fixed,
+                           higgs_family=hf, gpp=0.47)
+    ic = oracle_mod.ICSpec(seed=4321 + nx + hf, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    p = _lp(op.__dict__)
+    sc64, ve64 = oracle_mod.init_fields(op, ic, np.float64)
+    assert ve64.shape[-1] == (18 if hf == 1 else 27)
+    o_sc, o_ve = sc64.copy(), ve64.copy()
+    o_rows, _ = oracle_mod.evolve(op, o_sc, o_ve, 10)
+    sc, ve, rows, warn = run_gpu(p, "fp64", sc64, ve64, 10)
+    assert warn == 0
+    assert rel_err(sc, o_sc) <= 1e-12
+    assert rel_err(ve, o_ve) <= 1e-12
+    assert [r["time_iter"] for r in rows] == [r["time_iter"] for r in o_rows]
+    for a, b in zip(rows, o_rows):
+        if b["has_energy"]:
+            for k in ("energy", "potential", "gradient", "kinetic", "magnetic", "electric"):
+                assert abs(a[k] - b[k]) <= 1e-12 * max(abs(b["energy"]), 1.0), k
+        if b["has_gauss"]:
+            assert len(a["gauss_max"]) == op.neq
+            np.testing.assert_allclose(a["gauss_int"], b["gauss_int"], rtol=1e-9, atol=1e-13)
+            np.testing.assert_allclose(a["gauss_max"], b["gauss_max"], rtol=1e-9, atol=1e-13)
+    # mixed form against the FP64 oracle
+    sc32, ve32 = oracle_mod.init_fields(op, ic, np.float32)
+    sc, ve, rows, _ = run_gpu(p, "mixed", sc32, ve32, 10)
+    assert np.max(np.abs(sc.astype(np.float64) - o_sc)) <= 6e-6
+    assert np.max(np.abs(ve.astype(np.float64) - o_ve)) <= 6e-6
+    for a, b in zip(rows, o_rows):
+        if b["has_energy"]:
+            assert abs(a["energy"] - b["energy"]) <= 1e-6 * abs(b["energy"])
+    # reference arithmetic, float storage, against the float oracle (rows in the reference's order)
+    o32_sc, o32_ve = sc32.copy(), ve32.copy()
+    o32_rows, _ = oracle_mod.evolve(op, o32_sc, o32_ve, 10)
+    sc, ve, rows, _ = run_gpu(p, "ref32", sc32, ve32, 10)
+    assert ulp_close(sc, o32_sc, 8).all()
+    assert ulp_close(ve, o32_ve, 8).all()
+    for a, b in zip(rows, o32_rows):
+        if b["has_gauss"]:
+            np.testing.assert_allclose(a["gauss_max"], b["gauss_max"], rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.parametrize("hf", [1, 2], ids=["hf_u1", "hf_su2"])
+def test_higgs_family_device_initial_data(oracle_mod, hf):
+    from gftevolver_b200 import Evolver, InitialData
+    op = oracle_mod.Params(model=2, nx=5, ny=6, nz=7, higgs_family=hf)
+    spec = dict(seed=91, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    with Evolver(_lp(op.__dict__), form="fp64") as ev:
+        ev.init_fields(InitialData(**spec))
+        g_sc, g_ve = ev.download()
+    o_sc, o_ve = oracle_mod.init_fields(op, oracle_mod.ICSpec(**spec), np.float64)
+    assert np.max(np.abs(g_sc - o_sc)) <= 4e-14
+    assert np.max(np.abs(g_ve - o_ve)) <= 1e-14
+
+
+def test_higgs_family_is_refused_where_not_built(oracle_mod):
+    """The tiled kernel and the ensemble evolve gaugeNum 4 only."""
+    from gftevolver_b200 import Evolver, _lib
+    op = oracle_mod.Params(model=2, nx=8, ny=8, nz=32, higgs_family=1)
+    with Evolver(_lp(op.__dict__), form="mixed") as ev:
+        assert ev.lib.gft_set_kernel(ev.h, 2, 0, 8) == _lib.GFT_E_UNSUPPORTED
+        assert ev.step_kernel_name == "fast_step_kernel"
+
+
 def test_time_iter_parity_and_chunking(oracle_mod):
     """Evolving 3 + 4 steps equals 7 steps; the now/past slot follows time_iter (Lattice.cpp:773)."""
     op = oracle_mod.Params(nx=6, ny=5, nz=4, energy_every=2, gauss_every=3)

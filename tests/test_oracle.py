@@ -76,7 +76,7 @@ def test_oracle_rejects_bad_config(oracle_mod):
     with pytest.raises(ValueError):
         oracle_mod.evolve(p, sc, ve, 1)
     # a Higgs-family field exists only in the 2HDM (WilsonLoops::TwoHDM)
-    p = oracle_mod.Params(model=oracle_mod.MODEL_SM, nx=2, ny=2, nz=2, hf=oracle_mod.HF_U1)
+    p = oracle_mod.Params(model=oracle_mod.MODEL_SM, nx=2, ny=2, nz=2, higgs_family=oracle_mod.HF_U1)
     sc = np.zeros((2, 2, 2, 2, p.nsc), np.float32)
     ve = np.zeros((2, 2, 2, 2, p.nve), np.float32)
     with pytest.raises(ValueError):
@@ -92,7 +92,7 @@ def test_live_reference_matches_oracle_when_built(oracle_mod):
              (oracle_mod.MODEL_2HDM, oracle_mod.HF_SU2)]
     for model, hf in cases:
         for dtype in (np.float32, np.float64):
-            p = oracle_mod.Params(model=model, nx=3, ny=4, nz=5, energy_every=2, gauss_every=2, hf=hf, gpp=0.44)
+            p = oracle_mod.Params(model=model, nx=3, ny=4, nz=5, energy_every=2, gauss_every=2, higgs_family=hf, gpp=0.44)
             ic = oracle_mod.ICSpec(seed=99, mean=[0.8] * 8, sigma=[0.15] * 8, theta_sigma=0.2, eps_sigma=0.2)
             sc, ve = oracle_mod.init_fields(p, ic, dtype)
             sc0, ve0 = sc.copy(), ve.copy()
