@@ -15,7 +15,9 @@
  *     scalars[((t*nx + x)*ny + y)*nz + z][nsc]     nsc = 4 (SM) or 8 (2HDM)
  *     vectors[((t*nx + x)*ny + y)*nz + z][3*dw]    per direction d: [theta_Y, c0, c1, c2, c3]
  *                                                  (+ theta_H, or + d0..d3, for the 2HDM
- *                                                  Higgs-family gauge field: dw = 5, 6 or 9)
+ *                                                  Higgs-family gauge field: dw = 5, 6 or 9);
+ *                                                  generator representation: [theta_Y, w1..w3]
+ *                                                  (+ theta_H or w'1..w'3: dw = 4, 5 or 7)
  * At step time_iter the "now" level is (time_iter + 1) % 2 and the update is
  * written in place into the other ("past") level (Lattice.cpp:773-774).
  */
@@ -45,6 +47,8 @@ typedef ORC_S S;
 typedef struct {
     int model, nsc;
     int hf, dw, nv, neq;         /* Higgs family, words per direction, per site, gauge equations per direction */
+    int gen;                     /* generator link representation */
+    int hf_off;                  /* offset of the Higgs-family field in a direction block */
     long long nx, ny, nz, nsite;
     double dt;
     double stencil[3][3];        /* Gradients/Source/StandardModel.cpp:14-24 */
@@ -71,10 +75,28 @@ typedef struct {
  * SU(2) helpers (WilsonLoops/Source/StandardModel.cpp:76-112, 160-191)
  * ------------------------------------------------------------------------- */
 
-/* getSU2Representation, quaternion branch: c0 = v[d+off], c_a = conj*v[d+off+a]
- * (off = 1: the isospin link; off = 5: the Higgs-family SU(2) link). */
+/* getSU2Representation (WilsonLoops/Source/StandardModel.cpp:76-112, TwoHDM.cpp:94-126):
+ * quaternion branch c0 = v[d+off], c_a = conj*v[d+off+a]; generator branch from
+ * w = v[d+off .. d+off+2]: c0 = cos|w|, c_a = conj*sin|w|*w_a/|w| (c1 = sin|w| when
+ * |w| <= tol).  off = 1: the isospin link; the Higgs-family SU(2) link at hf_off. */
+static int g_gen = 0;          /* the representation of the current run (set by ctx_init) */
+static double g_gen_tol = 0.0; /* divisionByZeroTolerance */
+
 static void su2_rep_at(const S* v, int d, int off, int conj, double c[4])
 {
+    if (g_gen) {
+        double wm = 0.0;
+        for (int k = 0; k < 3; k++) wm += (double)v[d + off + k] * (double)v[d + off + k];
+        wm = sqrt(wm);
+        c[0] = cos(wm);
+        c[1] = c[2] = c[3] = 0.0;
+        if (wm > g_gen_tol) {
+            for (int k = 1; k < 4; k++) c[k] = ((double)(conj ? -1 : 1) * sin(wm)) * (double)v[d + off + k - 1] / wm;
+        } else {
+            c[1] = sin(wm);
+        }
+        return;
+    }
     c[0] = (double)v[d + off];
     for (int k = 1; k < 4; k++) {
         S comp = conj ? (S)(-v[d + off + k]) : v[d + off + k];
@@ -84,9 +106,27 @@ static void su2_rep_at(const S* v, int d, int off, int conj, double c[4])
 
 static void su2_rep(const S* v, int d, int conj, double c[4]) { su2_rep_at(v, d, 1, conj, c); }
 
+/* invertSU2Representation (WilsonLoops/Source/StandardModel.cpp:114-158): phase =
+ * asin|c| (pi/2 when |c| > 1), pi - phase when c0 < 0; w = phase*c/|c| (w1 = phase when
+ * |c| <= tol); stored in S. */
+static void su2_invert(const double c[4], S w[3])
+{
+    double cm = 0.0;
+    for (int k = 1; k < 4; k++) cm += c[k] * c[k];
+    cm = sqrt(cm);
+    double phase = (cm > 1) ? 1.5707963267948966 : asin(cm);
+    if (c[0] < 0) phase = 3.141592653589793 - phase;
+    if (cm > g_gen_tol) {
+        for (int k = 0; k < 3; k++) w[k] = (S)(phase * c[k + 1] / cm);
+    } else {
+        w[0] = (S)phase;
+        w[1] = w[2] = (S)0;
+    }
+}
+
 /* offset of the Higgs-family field in a direction block (TwoHDM.cpp:362-368: 5 in the
- * quaternion representation) */
-#define HF_OFF 5
+ * quaternion representation, 4 in the generator representation) */
+#define HF_OFF (m->hf_off)
 
 /* SU2Product(U1, U2, calc_trace): vector part always, scalar part and
  * renormalisation only when calc_trace (component 0 stays 0 otherwise). */
@@ -536,7 +576,13 @@ static int evolve_links(const ctx_t* m, S* past, const S* now, const double R[3 
         double up[4];
         su2_rep(now, dd, 0, up);
         su2_product(u, up, 1, up);
-        for (int k = 0; k < 4; k++) past[dd + 1 + k] = (S)up[k];
+        if (m->gen) {
+            S w[3];
+            su2_invert(up, w);
+            for (int k = 0; k < 3; k++) past[dd + 1 + k] = w[k];
+        } else {
+            for (int k = 0; k < 4; k++) past[dd + 1 + k] = (S)up[k];
+        }
         /* Higgs family (TwoHDM.cpp:702-745) */
         if (m->hf == ORC_HF_U1) {
             past[dd + HF_OFF] = (S)(asin(R[e + 4]) + (double)now[dd + HF_OFF]);
@@ -549,7 +595,13 @@ static int evolve_links(const ctx_t* m, S* past, const S* now, const double R[3 
             double hq[4];
             su2_rep_at(now, dd, HF_OFF, 0, hq);
             su2_product(hu, hq, 1, hq);
-            for (int k = 0; k < 4; k++) past[dd + HF_OFF + k] = (S)hq[k];
+            if (m->gen) {
+                S w[3];
+                su2_invert(hq, w);
+                for (int k = 0; k < 3; k++) past[dd + HF_OFF + k] = w[k];
+            } else {
+                for (int k = 0; k < 4; k++) past[dd + HF_OFF + k] = (S)hq[k];
+            }
         }
     }
     return warn;
@@ -693,7 +745,14 @@ static int ctx_init(ctx_t* m, const orc_config* c)
     m->model = c->model;
     m->nsc = (c->model == ORC_MODEL_SM) ? 4 : 8;
     m->hf = c->hf;
-    m->dw = (c->hf == ORC_HF_U1) ? 6 : (c->hf == ORC_HF_SU2) ? 9 : 5;
+    m->gen = c->generator_rep != 0;
+    m->hf_off = m->gen ? 4 : 5;
+    if (m->gen)
+        m->dw = (c->hf == ORC_HF_U1) ? 5 : (c->hf == ORC_HF_SU2) ? 7 : 4;
+    else
+        m->dw = (c->hf == ORC_HF_U1) ? 6 : (c->hf == ORC_HF_SU2) ? 9 : 5;
+    g_gen = m->gen;
+    g_gen_tol = c->div_tol;
     m->nv = 3 * m->dw;
     m->neq = (c->hf == ORC_HF_U1) ? 5 : (c->hf == ORC_HF_SU2) ? 7 : 4;
     m->nx = c->nx; m->ny = c->ny; m->nz = c->nz;
@@ -930,12 +989,14 @@ static double gaussian(uint64_t seed, uint64_t stream, uint64_t i)
 #define ORC_STREAM_HF_COSPOLAR(d) (112 + (d))
 #define ORC_STREAM_HF_AZIMUTH(d) (128 + (d))
 
-/* Random unit quaternion (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform on S^2. */
-static void random_link(uint64_t seed, int s_eps, int s_cos, int s_az, uint64_t i, double eps_sigma, double q[4])
+/* Random unit quaternion q[0..3] = (cos eps, sin eps n), eps ~ N(0, eps_sigma^2), n uniform
+ * on S^2, and its generators q[4..6] = eps n. */
+static void random_link(uint64_t seed, int s_eps, int s_cos, int s_az, uint64_t i, double eps_sigma, double q[7])
 {
     const double two_pi = 6.283185307179586476925286766559;
     q[0] = 1.0;
     q[1] = q[2] = q[3] = 0.0;
+    q[4] = q[5] = q[6] = 0.0;
     if (eps_sigma > 0.0) {
         double eps = eps_sigma * gaussian(seed, (uint64_t)s_eps, i);
         double ct = 2.0 * uniform01(seed, (uint64_t)s_cos, i) - 1.0;
@@ -946,6 +1007,9 @@ static void random_link(uint64_t seed, int s_eps, int s_cos, int s_az, uint64_t 
         q[1] = se * st * cos(ph);
         q[2] = se * st * sin(ph);
         q[3] = se * ct;
+        q[4] = eps * st * cos(ph);
+        q[5] = eps * st * sin(ph);
+        q[6] = eps * ct;
     }
 }
 
@@ -953,14 +1017,17 @@ static void random_link(uint64_t seed, int s_eps, int s_cos, int s_az, uint64_t 
  * Fill both time levels (E = 0, pi = 0).  Scalars: component c ~ N(mean[c], sigma[c]^2)
  * (+ wall profile on component 0 when wall_width > 0).  Links: theta_Y ~ N(0, theta_sigma^2);
  * SU(2) = (cos eps, sin eps n) with eps ~ N(0, eps_sigma^2), n uniform on S^2; identity when
- * eps_sigma == 0 and theta_sigma == 0.  dw = words per direction (5, or 6 / 9 with a
- * Higgs-family phase ~ N(0, theta_sigma^2) / quaternion drawn like the SU(2) link).
+ * eps_sigma == 0 and theta_sigma == 0.  hf: a Higgs-family phase ~ N(0, theta_sigma^2)
+ * (ORC_HF_U1) or quaternion drawn like the SU(2) link (ORC_HF_SU2).  gen: links stored
+ * as generators, w = eps n (the same group element).
  */
-void FN(init_fields)(int nx, int ny, int nz, int nsc, int dw, S* scalars, S* vectors, unsigned long long seed,
-                     const double* mean, const double* sigma, double theta_sigma, double eps_sigma,
-                     double wall_width, double wall_value)
+void FN(init_fields)(int nx, int ny, int nz, int nsc, int hf, int gen, S* scalars, S* vectors,
+                     unsigned long long seed, const double* mean, const double* sigma, double theta_sigma,
+                     double eps_sigma, double wall_width, double wall_value)
 {
     long long N = (long long)nx * ny * nz;
+    const int dw = (gen ? 4 : 5) + (hf == ORC_HF_U1 ? 1 : (hf == ORC_HF_SU2 ? (gen ? 3 : 4) : 0));
+    const int off = gen ? 4 : 5;
     const int NV = 3 * dw;
     for (long long i = 0; i < N; i++) {
         long long z = i % nz;
@@ -975,20 +1042,26 @@ void FN(init_fields)(int nx, int ny, int nz, int nsc, int dw, S* scalars, S* vec
         }
         for (int d = 0; d < 3; d++) {
             double th = theta_sigma * gaussian(seed, ORC_STREAM_THETA(d), (uint64_t)i);
-            double q[4];
+            double q[7];
             random_link(seed, ORC_STREAM_EPS(d), ORC_STREAM_COSPOLAR(d), ORC_STREAM_AZIMUTH(d), (uint64_t)i, eps_sigma, q);
             S* v0 = vectors + i * NV + d * dw;
             S* v1 = vectors + (N + i) * NV + d * dw;
             v0[0] = v1[0] = (S)th;
-            for (int k = 0; k < 4; k++) v0[1 + k] = v1[1 + k] = (S)q[k];
-            if (dw == 6) {
+            if (gen)
+                for (int k = 0; k < 3; k++) v0[1 + k] = v1[1 + k] = (S)q[4 + k];
+            else
+                for (int k = 0; k < 4; k++) v0[1 + k] = v1[1 + k] = (S)q[k];
+            if (hf == ORC_HF_U1) {
                 double hth = theta_sigma * gaussian(seed, ORC_STREAM_HF_THETA(d), (uint64_t)i);
-                v0[5] = v1[5] = (S)hth;
-            } else if (dw == 9) {
-                double hq[4];
+                v0[off] = v1[off] = (S)hth;
+            } else if (hf == ORC_HF_SU2) {
+                double hq[7];
                 random_link(seed, ORC_STREAM_HF_EPS(d), ORC_STREAM_HF_COSPOLAR(d), ORC_STREAM_HF_AZIMUTH(d),
                             (uint64_t)i, eps_sigma, hq);
-                for (int k = 0; k < 4; k++) v0[5 + k] = v1[5 + k] = (S)hq[k];
+                if (gen)
+                    for (int k = 0; k < 3; k++) v0[off + k] = v1[off + k] = (S)hq[4 + k];
+                else
+                    for (int k = 0; k < 4; k++) v0[off + k] = v1[off + k] = (S)hq[k];
             }
         }
     }

@@ -67,6 +67,10 @@ typedef struct orc_config {
     /* 2HDM Higgs-family gauge group (ORC_HF_*) and its coupling g'' (WilsonLoops/Config/TwoHDM.cfg) */
     int hf;
     double gpp;
+    /* generator link representation: each SU(2) link stored as its 3 generators w, U =
+     * (cos|w|, sin|w| w/|w|) (WilsonLoops/Source/StandardModel.cpp:76-160); 4 words per
+     * direction [theta_Y, w1, w2, w3] (+ theta_H, or + w'1..w'3 for the Higgs family) */
+    int generator_rep;
 } orc_config;
 
 /* One row of global observables, written on every step where an analyser logs.

@@ -12,7 +12,8 @@ checker; the product never imports it.
 Arrays use the reference layout: ``scalars[2, nx, ny, nz, nsc]`` and
 ``vectors[2, nx, ny, nz, 3 * dw]`` (per direction ``[theta_Y, c0, c1, c2, c3]``,
 plus the 2HDM Higgs-family phase ``theta_H`` (dw = 6) or quaternion ``d0..d3``
-(dw = 9), ``WilsonLoops/Source/TwoHDM.cpp:210-242``).
+(dw = 9), ``WilsonLoops/Source/TwoHDM.cpp:210-242``); in the generator
+representation ``[theta_Y, w1, w2, w3]`` (+ ``theta_H`` or ``w'1..w'3``: dw = 4, 5, 7).
 """
 from __future__ import annotations
 
@@ -53,6 +54,7 @@ class OrcConfig(ctypes.Structure):
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
         ("fixed_axes", ctypes.c_int),
         ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
+        ("generator_rep", ctypes.c_int),
     ]
 
 
@@ -111,6 +113,7 @@ class Params:
     gauss_every: int = 0
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (else periodic)
     higgs_family: int = HF_NONE  # 2HDM Higgs-family gauge field (HF_*)
+    generator_rep: int = 0     # links stored as 3 generators w (U = exp(i w.sigma)) instead of quaternions
 
     @property
     def nsc(self) -> int:
@@ -119,6 +122,8 @@ class Params:
     @property
     def dw(self) -> int:
         """Link words per direction."""
+        if self.generator_rep:
+            return {HF_NONE: 4, HF_U1: 5, HF_SU2: 7}[self.higgs_family]
         return {HF_NONE: 5, HF_U1: 6, HF_SU2: 9}[self.higgs_family]
 
     @property
@@ -180,8 +185,8 @@ def _load():
                               ctypes.POINTER(OrcRow), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
                 f = getattr(lib, p + "init_fields")
                 f.restype = None
-                f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, fp,
-                              ctypes.c_ulonglong,
+                f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              fp, fp, ctypes.c_ulonglong,
                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
             _lib = lib
@@ -223,7 +228,7 @@ def init_fields(p: Params, ic: ICSpec, dtype=np.float32):
     mean = (ctypes.c_double * 8)(*[float(v) for v in (list(ic.mean) + [0.0] * 8)[:8]])
     sig = (ctypes.c_double * 8)(*[float(v) for v in (list(ic.sigma) + [0.0] * 8)[:8]])
     getattr(lib, _prefix(dtype) + "init_fields")(
-        p.nx, p.ny, p.nz, p.nsc, p.dw, _ptr(sc), _ptr(ve), ctypes.c_ulonglong(ic.seed), mean, sig,
+        p.nx, p.ny, p.nz, p.nsc, p.higgs_family, p.generator_rep, _ptr(sc), _ptr(ve), ctypes.c_ulonglong(ic.seed), mean, sig,
         float(ic.theta_sigma), float(ic.eps_sigma), float(ic.wall_width), float(ic.wall_value))
     return sc, ve
 

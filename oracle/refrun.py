@@ -131,7 +131,7 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
         _write(os.path.join(work, "WilsonLoops", "Config", "StandardModel.cfg"), wl)
     else:
         wl += [f"gpp                            : {_num(p.gpp)}", "",
-               "generator representation       : 0", "",
+               f"generator representation       : {1 if p.generator_rep else 0}", "",
                f"division tolerance             : {_num(p.div_tol)}"]
         _write(os.path.join(work, "WilsonLoops", "Config", "TwoHDM.cfg"), wl)
 

@@ -58,6 +58,12 @@ CASES = {
     "2hdm_hf_su2_5x3x4": (dict(model=orc.MODEL_2HDM, nx=5, ny=3, nz=4, energy_every=3, gauss_every=2, higgs_family=orc.HF_SU2,
                                gpp=0.52),
                           dict(seed=22, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
+    # generator link representation (links stored as w, U = exp(i w.sigma)): SM, and 2HDM with a family SU(2)
+    "sm_gen_4x5x6": (dict(model=orc.MODEL_SM, nx=4, ny=5, nz=6, energy_every=2, gauss_every=3, generator_rep=1),
+                     dict(seed=23, mean=[1.0] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
+    "2hdm_gen_hf_su2_4x3x5": (dict(model=orc.MODEL_2HDM, nx=4, ny=3, nz=5, energy_every=3, gauss_every=2,
+                                   higgs_family=orc.HF_SU2, gpp=0.52, generator_rep=1),
+                              dict(seed=24, mean=[0.7] * 8, sigma=[0.1] * 8, **RANDOM_LINKS), 8, ("f32", "f64")),
 }
 
 

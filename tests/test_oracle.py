@@ -88,11 +88,13 @@ def test_live_reference_matches_oracle_when_built(oracle_mod):
     from oracle import refrun
     if not (refrun.available(False) and refrun.available(True)):
         pytest.skip("reference binaries not built in this environment")
-    cases = [(oracle_mod.MODEL_SM, 0), (oracle_mod.MODEL_2HDM, 0), (oracle_mod.MODEL_2HDM, oracle_mod.HF_U1),
-             (oracle_mod.MODEL_2HDM, oracle_mod.HF_SU2)]
-    for model, hf in cases:
+    cases = [(oracle_mod.MODEL_SM, 0, 0), (oracle_mod.MODEL_2HDM, 0, 0), (oracle_mod.MODEL_2HDM, oracle_mod.HF_U1, 0),
+             (oracle_mod.MODEL_2HDM, oracle_mod.HF_SU2, 0), (oracle_mod.MODEL_SM, 0, 1),
+             (oracle_mod.MODEL_2HDM, oracle_mod.HF_U1, 1)]
+    for model, hf, gen in cases:
         for dtype in (np.float32, np.float64):
-            p = oracle_mod.Params(model=model, nx=3, ny=4, nz=5, energy_every=2, gauss_every=2, higgs_family=hf, gpp=0.44)
+            p = oracle_mod.Params(model=model, nx=3, ny=4, nz=5, energy_every=2, gauss_every=2, higgs_family=hf, gpp=0.44,
+                                  generator_rep=gen)
             ic = oracle_mod.ICSpec(seed=99, mean=[0.8] * 8, sigma=[0.15] * 8, theta_sigma=0.2, eps_sigma=0.2)
             sc, ve = oracle_mod.init_fields(p, ic, dtype)
             sc0, ve0 = sc.copy(), ve.copy()
