@@ -57,6 +57,7 @@ class GftConfig(ctypes.Structure):
         ("energy_every", ctypes.c_int), ("gauss_every", ctypes.c_int),
         ("fixed_axes", ctypes.c_int),
         ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
+        ("generator_rep", ctypes.c_int),
     ]
 
 

@@ -42,7 +42,8 @@ struct gft_handle {
     gft_config cfg{};
     int nsc = 4;
     int hf = 0;             // Higgs-family field (kHf*)
-    int nve = 15;           // link words per site in the reference layout (15, 18 or 27)
+    int nve = 15;           // link words per site in the reference layout (15, 18, 27; generators 12, 15, 21)
+    LinkCodec codec;        // generator representation: how host links map to device records
     int neq = 4;            // gauge equations per direction = Gauss constraints (gaugeNum)
     int nsite = 0;
     int sbytes = 4;         // storage bytes per word (4 or 8)
@@ -126,6 +127,8 @@ StepParams gft::config_params(const gft_config& c, int nsite, bool f32ref, int t
     P.inv_g_sqr = (g2 > c.div_tol) ? 1.0 / g2 : 0.0;
     P.inv_gp_sqr = (gp2 > c.div_tol) ? 1.0 / gp2 : 0.0;
     P.hf = (c.model == GFT_MODEL_2HDM) ? c.higgs_family : kHfNone;
+    P.gen = (c.generator_rep && c.form == GFT_FORM_REF) ? 1 : 0;  // the throughput forms hold quaternions
+    P.div_tol = c.div_tol;
     const double gpp2 = c.gpp * c.gpp;
     P.gsq_hf = f32ref ? (double)(float)gpp2 : gpp2;
     P.inv_gpp_sqr = (gpp2 > c.div_tol) ? 1.0 / gpp2 : 0.0;
@@ -347,6 +350,10 @@ int validate(const gft_config* c, std::string& why)
         why = "gft_create: a Higgs-family gauge field needs the 2HDM (WilsonLoops::TwoHDM)";
         return GFT_E_INVALID;
     }
+    if (c->generator_rep != 0 && c->generator_rep != 1) {
+        why = "gft_create: generator_rep is 0 (quaternion links) or 1 (generators)";
+        return GFT_E_INVALID;
+    }
     return GFT_OK;
 }
 
@@ -379,7 +386,13 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     h->cfg = *cfg;
     h->nsc = (cfg->model == GFT_MODEL_SM) ? 4 : 8;
     h->hf = (cfg->model == GFT_MODEL_2HDM) ? cfg->higgs_family : kHfNone;
-    h->nve = 3 * (h->hf == kHfU1 ? 6 : (h->hf == kHfSU2 ? 9 : 5));
+    h->codec.gen = cfg->generator_rep;
+    h->codec.convert = (cfg->form != GFT_FORM_REF) ? 1 : 0;
+    h->codec.tol = cfg->div_tol;
+    {
+        const int lw = cfg->generator_rep ? 3 : 4;  // words of one SU(2) link
+        h->nve = 3 * (1 + lw + (h->hf == kHfU1 ? 1 : (h->hf == kHfSU2 ? lw : 0)));
+    }
     h->neq = config_neq(*cfg);
     h->nsite = cfg->nx * cfg->ny * cfg->nz;
     h->sbytes = (cfg->form == GFT_FORM_REF) ? cfg->storage_bytes : (cfg->form == GFT_FORM_FP64 ? 8 : 4);
@@ -523,8 +536,8 @@ int upload_impl(gft_handle* h, const H* sc, const H* ve, int time_iter, bool on_
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         const H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
         const H* v_t = dve + (size_t)t * h->nsite * h->nve;
-        e = is_f64_storage(h) ? launch_aos_to_soa<double, H>(s_t, v_t, h->nsite, h->nsc, h->ld[t], h->stream)
-                              : launch_aos_to_soa<float, H>(s_t, v_t, h->nsite, h->nsc, h->lf[t], h->stream);
+        e = is_f64_storage(h) ? launch_aos_to_soa<double, H>(s_t, v_t, h->nsite, h->nsc, h->ld[t], h->stream, h->codec)
+                              : launch_aos_to_soa<float, H>(s_t, v_t, h->nsite, h->nsc, h->lf[t], h->stream, h->codec);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "gft_upload");
@@ -552,8 +565,8 @@ int download_impl(gft_handle* h, H* sc, H* ve, bool on_device = false)
     for (int t = 0; t < 2 && e == cudaSuccess; t++) {
         H* s_t = dsc + (size_t)t * h->nsite * h->nsc;
         H* v_t = dve + (size_t)t * h->nsite * h->nve;
-        e = is_f64_storage(h) ? launch_soa_to_aos<double, H>(h->ld[t], h->nsite, h->nsc, s_t, v_t, h->stream)
-                              : launch_soa_to_aos<float, H>(h->lf[t], h->nsite, h->nsc, s_t, v_t, h->stream);
+        e = is_f64_storage(h) ? launch_soa_to_aos<double, H>(h->ld[t], h->nsite, h->nsc, s_t, v_t, h->stream, h->codec)
+                              : launch_soa_to_aos<float, H>(h->lf[t], h->nsite, h->nsc, s_t, v_t, h->stream, h->codec);
     }
     if (!on_device) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(sc, dsc, nsc_w * sizeof(H), cudaMemcpyDeviceToHost, h->stream);
@@ -723,6 +736,7 @@ int gft_init_fields(gft_handle* h, const gft_ic* ic)
     p.wall_value = ic->wall_value;
     p.x_offset = h->x_offset;
     p.nx_global = h->nx_global;
+    p.store_generators = (h->codec.gen && !h->codec.convert) ? 1 : 0;
     const StepParams P = make_params(h, 0, false);
     cudaError_t e = is_f64_storage(h) ? launch_init_fields<double>(P, h->nsc, p, h->ld[0], h->ld[1], h->stream)
                                       : launch_init_fields<float>(P, h->nsc, p, h->lf[0], h->lf[1], h->stream);

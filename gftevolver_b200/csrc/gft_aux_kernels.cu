@@ -9,22 +9,85 @@
 namespace gft {
 namespace {
 
+// Generator w -> quaternion as the reference's getSU2Representation does it
+// (WilsonLoops/Source/StandardModel.cpp:76-112, conj = false).
+template <class H>
+__device__ __forceinline__ void gen_to_quat(const H* w, double tol, double (&c)[4])
+{
+    double wm = 0.0;
+    for (int k = 0; k < 3; k++) wm += (double)w[k] * (double)w[k];
+    wm = sqrt(wm);
+    c[0] = cos(wm);
+    c[1] = c[2] = c[3] = 0.0;
+    if (wm > tol) {
+        for (int k = 1; k < 4; k++) c[k] = sin(wm) * (double)w[k - 1] / wm;
+    } else {
+        c[1] = sin(wm);
+    }
+}
+
+// Quaternion -> generator as invertSU2Representation does it (:114-158).
+__device__ __forceinline__ void quat_to_gen(const double (&c)[4], double tol, double (&w)[3])
+{
+    double cm = sqrt(c[1] * c[1] + c[2] * c[2] + c[3] * c[3]);
+    double phase = (cm > 1) ? 1.5707963267948966 : asin(cm);
+    if (c[0] < 0) phase = 3.141592653589793 - phase;
+    if (cm > tol) {
+        for (int k = 0; k < 3; k++) w[k] = phase * c[k + 1] / cm;
+    } else {
+        w[0] = phase;
+        w[1] = w[2] = 0.0;
+    }
+}
+
+// One SU(2) link of the host record (4 words, or 3 generators) -> a device record.
+template <class S, class H>
+__device__ __forceinline__ void put_link(S* arr, int s, const H* w, const LinkCodec& cc)
+{
+    if (!cc.gen) {
+        st4(arr, s, (S)w[0], (S)w[1], (S)w[2], (S)w[3]);
+    } else if (cc.convert) {
+        double c[4];
+        gen_to_quat(w, cc.tol, c);
+        st4(arr, s, (S)c[0], (S)c[1], (S)c[2], (S)c[3]);
+    } else {
+        st4(arr, s, (S)w[0], (S)w[1], (S)w[2], (S)0);
+    }
+}
+
+template <class S, class H>
+__device__ __forceinline__ void get_link(const S* arr, int s, H* w, const LinkCodec& cc)
+{
+    const S* q = arr + 4 * (size_t)s;
+    if (!cc.gen) {
+        for (int k = 0; k < 4; k++) w[k] = (H)q[k];
+    } else if (cc.convert) {
+        const double c[4] = {(double)q[0], (double)q[1], (double)q[2], (double)q[3]};
+        double g[3];
+        quat_to_gen(c, cc.tol, g);
+        for (int k = 0; k < 3; k++) w[k] = (H)g[k];
+    } else {
+        for (int k = 0; k < 3; k++) w[k] = (H)q[k];
+    }
+}
+
 // Reference AoS record -> structure-of-arrays level (one thread per site).
 template <class S, class H>
 __global__ void aos_to_soa_kernel(const H* __restrict__ sc, const H* __restrict__ ve, int nsite, int nsc,
-                                  LevelPtrs<S> lv)
+                                  LevelPtrs<S> lv, LinkCodec cc)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsite) return;
-    const int dw = lv.hq[0] ? 9 : (lv.hth[0] ? 6 : 5);  // link words per direction
+    const int lw = cc.gen ? 3 : 4;                                  // words of one SU(2) link
+    const int dw = 1 + lw + (lv.hq[0] ? lw : (lv.hth[0] ? 1 : 0));  // link words per direction
     const H* v = ve + (size_t)s * 3 * dw;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const H* w = v + dw * d;
         lv.th[d][s] = (S)w[0];
-        st4(lv.q[d], s, (S)w[1], (S)w[2], (S)w[3], (S)w[4]);
-        if (dw == 6) lv.hth[d][s] = (S)w[5];
-        if (dw == 9) st4(lv.hq[d], s, (S)w[5], (S)w[6], (S)w[7], (S)w[8]);
+        put_link(lv.q[d], s, w + 1, cc);
+        if (lv.hth[0]) lv.hth[d][s] = (S)w[1 + lw];
+        if (lv.hq[0]) put_link(lv.hq[d], s, w + 1 + lw, cc);
     }
     const H* f = sc + (size_t)s * nsc;
     for (int db = 0; db < nsc / 4; db++)
@@ -32,25 +95,21 @@ __global__ void aos_to_soa_kernel(const H* __restrict__ sc, const H* __restrict_
 }
 
 template <class S, class H>
-__global__ void soa_to_aos_kernel(LevelPtrs<S> lv, int nsite, int nsc, H* __restrict__ sc, H* __restrict__ ve)
+__global__ void soa_to_aos_kernel(LevelPtrs<S> lv, int nsite, int nsc, H* __restrict__ sc, H* __restrict__ ve,
+                                  LinkCodec cc)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsite) return;
-    const int dw = lv.hq[0] ? 9 : (lv.hth[0] ? 6 : 5);  // link words per direction
+    const int lw = cc.gen ? 3 : 4;
+    const int dw = 1 + lw + (lv.hq[0] ? lw : (lv.hth[0] ? 1 : 0));
     H* v = ve + (size_t)s * 3 * dw;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         H* w = v + dw * d;
         w[0] = (H)lv.th[d][s];
-        const S* q = lv.q[d] + 4 * (size_t)s;
-#pragma unroll
-        for (int k = 0; k < 4; k++) w[1 + k] = (H)q[k];
-        if (dw == 6) w[5] = (H)lv.hth[d][s];
-        if (dw == 9) {
-            const S* h = lv.hq[d] + 4 * (size_t)s;
-#pragma unroll
-            for (int k = 0; k < 4; k++) w[5 + k] = (H)h[k];
-        }
+        get_link(lv.q[d], s, w + 1, cc);
+        if (lv.hth[0]) w[1 + lw] = (H)lv.hth[d][s];
+        if (lv.hq[0]) get_link(lv.hq[d], s, w + 1 + lw, cc);
     }
     H* f = sc + (size_t)s * nsc;
     for (int db = 0; db < nsc / 4; db++) {
@@ -89,17 +148,25 @@ __device__ __forceinline__ double gaussian(unsigned long long seed, unsigned lon
 
 // Unit quaternion (cos eps, sin eps n): eps ~ N(0, eps_sigma^2) from stream s0,
 // n uniform on S^2 from streams s0 + 16 (cos polar) and s0 + 32 (azimuth).
+// With ic.store_generators the record is (w1, w2, w3, 0), w = eps n: the same
+// group element in the generator representation.
 __device__ __forceinline__ void random_link(const ICParams& ic, unsigned long long s0, unsigned long long key,
                                             double (&q)[4])
 {
     const double two_pi = 6.283185307179586476925286766559;
-    q[0] = 1.0;
+    q[0] = ic.store_generators ? 0.0 : 1.0;
     q[1] = q[2] = q[3] = 0.0;
     if (ic.eps_sigma > 0.0) {
         const double eps = ic.eps_sigma * gaussian(ic.seed, s0, key);
         const double ct = 2.0 * uniform01(ic.seed, s0 + 16ULL, key) - 1.0;
         const double st = sqrt(1.0 - ct * ct);
         const double ph = two_pi * uniform01(ic.seed, s0 + 32ULL, key);
+        if (ic.store_generators) {
+            q[0] = eps * st * cos(ph);
+            q[1] = eps * st * sin(ph);
+            q[2] = eps * ct;
+            return;
+        }
         const double se = sin(eps);
         q[0] = cos(eps);
         q[1] = se * st * cos(ph);
@@ -230,16 +297,18 @@ cudaError_t run_math_selftest(int n, double* out8)
 }
 
 template <class S, class H>
-cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s)
+cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s,
+                              LinkCodec codec)
 {
-    aos_to_soa_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(aos_sc, aos_ve, nsite, nsc, lv);
+    aos_to_soa_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(aos_sc, aos_ve, nsite, nsc, lv, codec);
     return cudaGetLastError();
 }
 
 template <class S, class H>
-cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s)
+cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s,
+                              LinkCodec codec)
 {
-    soa_to_aos_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(lv, nsite, nsc, aos_sc, aos_ve);
+    soa_to_aos_kernel<S, H><<<(nsite + 255) / 256, 256, 0, s>>>(lv, nsite, nsc, aos_sc, aos_ve, codec);
     return cudaGetLastError();
 }
 
@@ -271,17 +340,17 @@ cudaError_t launch_finalize(const double* partials, int nblocks, int nslots, int
 int finalize_launches(int nblocks, bool have_mid) { return (have_mid && nblocks > 2 * kFinThreads) ? 2 : 1; }
 
 template cudaError_t launch_aos_to_soa<float, float>(const float*, const float*, int, int, LevelPtrs<float>,
-                                                     cudaStream_t);
+                                                     cudaStream_t, LinkCodec);
 template cudaError_t launch_aos_to_soa<float, double>(const double*, const double*, int, int, LevelPtrs<float>,
-                                                      cudaStream_t);
+                                                      cudaStream_t, LinkCodec);
 template cudaError_t launch_aos_to_soa<double, float>(const float*, const float*, int, int, LevelPtrs<double>,
-                                                      cudaStream_t);
+                                                      cudaStream_t, LinkCodec);
 template cudaError_t launch_aos_to_soa<double, double>(const double*, const double*, int, int, LevelPtrs<double>,
-                                                       cudaStream_t);
-template cudaError_t launch_soa_to_aos<float, float>(LevelPtrs<float>, int, int, float*, float*, cudaStream_t);
-template cudaError_t launch_soa_to_aos<float, double>(LevelPtrs<float>, int, int, double*, double*, cudaStream_t);
-template cudaError_t launch_soa_to_aos<double, float>(LevelPtrs<double>, int, int, float*, float*, cudaStream_t);
-template cudaError_t launch_soa_to_aos<double, double>(LevelPtrs<double>, int, int, double*, double*, cudaStream_t);
+                                                       cudaStream_t, LinkCodec);
+template cudaError_t launch_soa_to_aos<float, float>(LevelPtrs<float>, int, int, float*, float*, cudaStream_t, LinkCodec);
+template cudaError_t launch_soa_to_aos<float, double>(LevelPtrs<float>, int, int, double*, double*, cudaStream_t, LinkCodec);
+template cudaError_t launch_soa_to_aos<double, float>(LevelPtrs<double>, int, int, float*, float*, cudaStream_t, LinkCodec);
+template cudaError_t launch_soa_to_aos<double, double>(LevelPtrs<double>, int, int, double*, double*, cudaStream_t, LinkCodec);
 template cudaError_t launch_init_fields<float>(const StepParams&, int, const ICParams&, LevelPtrs<float>,
                                                LevelPtrs<float>, cudaStream_t);
 template cudaError_t launch_init_fields<double>(const StepParams&, int, const ICParams&, LevelPtrs<double>,

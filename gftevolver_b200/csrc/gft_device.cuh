@@ -65,8 +65,10 @@ struct StepParams {
     double gsq[4];          // coupling^2 per equation k % 4 (as the reference's getSqrCouplings returns it)
     double inv_g_sqr, inv_gp_sqr;
     int hf;                 // 2HDM Higgs-family gauge field (kHf*)
+    int gen;                // reference-arithmetic form: links stored as generators (WilsonLoops/Source/StandardModel.cpp:76-160)
     double gsq_hf;          // g''^2 of the Higgs-family equations (TwoHDM.cpp:258-267)
     double inv_gpp_sqr;     // 1/g''^2 (0 below the division tolerance)
+    double div_tol;         // divisionByZeroTolerance of the generator conversions
     double damping_step;    // 0.5 * damping * dt for this step
     // SO_N
     double lambda, eta_sqr;

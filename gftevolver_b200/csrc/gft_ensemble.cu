@@ -575,6 +575,10 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
             set_error("gft_batch_create: the ensemble has no Higgs-family gauge field (gaugeNum 4 only)");
             return GFT_E_UNSUPPORTED;
         }
+        if (cfgs[m].generator_rep) {
+            set_error("gft_batch_create: the ensemble transfers quaternion links only (generator_rep = 0)");
+            return GFT_E_UNSUPPORTED;
+        }
         if (cfgs[m].model != cfgs[0].model || cfgs[m].device != cfgs[0].device) {
             set_error("gft_batch_create: all members must share the model and the device");
             return GFT_E_INVALID;

@@ -59,11 +59,19 @@ inline void tiled_tile(int variant, int& ty, int& tz)
 
 // Auxiliary kernels (gft_aux_kernels.cu).
 // The reference record has 3 x 5 link words per site, 3 x 6 with a Higgs-family
-// phase (lv.hth set) or 3 x 9 with a Higgs-family quaternion (lv.hq set).
+// phase (lv.hth set) or 3 x 9 with a Higgs-family quaternion (lv.hq set); in the
+// generator representation 3 x 4, 3 x 5 or 3 x 7.
+struct LinkCodec {
+    int gen = 0;       // host links are generators w (WilsonLoops/Source/StandardModel.cpp:76-160)
+    int convert = 0;   // gen: the device holds quaternions (convert w <-> q), else the raw generators
+    double tol = 0.0;  // divisionByZeroTolerance of the conversions
+};
 template <class S, class H>
-cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s);
+cudaError_t launch_aos_to_soa(const H* aos_sc, const H* aos_ve, int nsite, int nsc, LevelPtrs<S> lv, cudaStream_t s,
+                              LinkCodec codec = LinkCodec());
 template <class S, class H>
-cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s);
+cudaError_t launch_soa_to_aos(LevelPtrs<S> lv, int nsite, int nsc, H* aos_sc, H* aos_ve, cudaStream_t s,
+                              LinkCodec codec = LinkCodec());
 
 struct ICParams {
     unsigned long long seed;
@@ -72,6 +80,9 @@ struct ICParams {
     // x-slab: local plane x draws the random numbers of global plane
     // (x + x_offset) mod nx_global, so slabs reproduce the whole lattice's data
     int x_offset, nx_global;
+    // store the SU(2) links as their generators w = eps n (reference-arithmetic
+    // form in the generator representation)
+    int store_generators;
 };
 template <class S>
 cudaError_t launch_init_fields(const StepParams& P, int nsc, const ICParams& ic, LevelPtrs<S> a, LevelPtrs<S> b,

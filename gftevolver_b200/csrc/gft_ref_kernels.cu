@@ -19,17 +19,63 @@ namespace {
 template <class S>
 struct RefView {
     const LevelPtrs<S>& L;
+    bool gen;    // links stored as generators (w1, w2, w3, unused)
+    double tol;  // divisionByZeroTolerance
     __device__ double th(int d, int s) const { return (double)L.th[d][s]; }
-    // getSU2Representation, quaternion branch (WilsonLoops/Source/StandardModel.cpp:104-109)
+    // getSU2Representation (WilsonLoops/Source/StandardModel.cpp:76-112)
     __device__ void rep(int d, int s, bool conj, double c[4]) const { rep_of(L.q[d], s, conj, c); }
-    // the same for the Higgs-family field (offset 5 of a direction block, TwoHDM.cpp:362-368)
+    // the same for the Higgs-family field (TwoHDM.cpp:94-126, 362-368)
     __device__ double hth(int d, int s) const { return (double)L.hth[d][s]; }
     __device__ void hrep(int d, int s, bool conj, double c[4]) const { rep_of(L.hq[d], s, conj, c); }
-    __device__ static void rep_of(const S* a, int s, bool conj, double c[4])
+    __device__ void rep_of(const S* a, int s, bool conj, double c[4]) const
     {
         const S* p = a + 4 * (size_t)s;
+        if (gen) {
+            // generator branch: c0 = cos|w|, c_a = conj * sin|w| * w_a / |w| (c1 = sin|w| when |w| <= tol)
+            double wm = 0.0;
+            wm += (double)p[0] * (double)p[0];
+            wm += (double)p[1] * (double)p[1];
+            wm += (double)p[2] * (double)p[2];
+            wm = sqrt(wm);
+            c[0] = cos(wm);
+            c[1] = c[2] = c[3] = 0.0;
+            if (wm > tol) {
+                const double cs = (double)(conj ? -1 : 1) * sin(wm);
+                for (int k = 1; k < 4; k++) c[k] = cs * (double)p[k - 1] / wm;
+            } else {
+                c[1] = sin(wm);
+            }
+            return;
+        }
         c[0] = (double)p[0];
         for (int k = 1; k < 4; k++) c[k] = conj ? -(double)p[k] : (double)p[k];
+    }
+    // Store a link: the quaternion, or (generator representation) invertSU2Representation
+    // (WilsonLoops/Source/StandardModel.cpp:114-158): phase = asin|c| (pi/2 when |c| > 1),
+    // pi - phase when c0 < 0, w = phase * c / |c| (w1 = phase when |c| <= tol).
+    __device__ void store(S* a, int s, const double c[4], bool& finite) const
+    {
+        S o[4];
+        if (gen) {
+            double cm = 0.0;
+            cm += c[1] * c[1];
+            cm += c[2] * c[2];
+            cm += c[3] * c[3];
+            cm = sqrt(cm);
+            double phase = (cm > 1) ? 1.5707963267948966 : asin(cm);
+            if (c[0] < 0) phase = 3.141592653589793 - phase;
+            if (cm > tol) {
+                for (int k = 0; k < 3; k++) o[k] = (S)(phase * c[k + 1] / cm);
+            } else {
+                o[0] = (S)phase;
+                o[1] = o[2] = (S)0;
+            }
+            o[3] = (S)0;
+        } else {
+            for (int k = 0; k < 4; k++) o[k] = (S)c[k];
+        }
+        st4(a, s, o[0], o[1], o[2], o[3]);
+        for (int k = 0; k < 4; k++) finite = finite && isfinite((double)o[k]);
     }
 };
 
@@ -264,8 +310,8 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
 
     if (active) {
         const Nbr n = neighbours(P, x, y, z);
-        const RefView<S> V{now};
-        const RefView<S> Vp{past};
+        const RefView<S> V{now, P.gen != 0, P.div_tol};
+        const RefView<S> Vp{past, P.gen != 0, P.div_tol};
         const bool store = ENERGY;
 
         // ---- potential (Model::calcPotentialContributions) ----
@@ -516,11 +562,9 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
             double up[4];
             V.rep(d, n.c, false, up);
             ref_su2_product(u, up, true, up);
-            const S q0 = (S)up[0], q1 = (S)up[1], q2 = (S)up[2], q3 = (S)up[3];
             past.th[d][n.c] = th_new;
-            st4(past.q[d], n.c, q0, q1, q2, q3);
-            finite = finite && isfinite((double)th_new) && isfinite((double)q0) && isfinite((double)q1)
-                     && isfinite((double)q2) && isfinite((double)q3);
+            V.store(past.q[d], n.c, up, finite);
+            finite = finite && isfinite((double)th_new);
             // Higgs family (TwoHDM.cpp:702-745)
             if (HF == kHfU1) {
                 const double r4 = R[4 % NEQ];
@@ -538,10 +582,7 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
                 double hq[4];
                 V.hrep(d, n.c, false, hq);
                 ref_su2_product(hu, hq, true, hq);
-                const S h0 = (S)hq[0], h1 = (S)hq[1], h2 = (S)hq[2], h3 = (S)hq[3];
-                st4(past.hq[d], n.c, h0, h1, h2, h3);
-                finite = finite && isfinite((double)h0) && isfinite((double)h1) && isfinite((double)h2)
-                         && isfinite((double)h3);
+                V.store(past.hq[d], n.c, hq, finite);
             }
         }
         if (!finite) warn |= kWarnNonFinite;
@@ -576,8 +617,8 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
     for (int k = 0; k < NG; k++) v[k] = 0.0;
     if (z < P.nz && y < P.ny && counts(P, x) && !frozen(P, x, y, z)) {
         const Nbr n = neighbours(P, x, y, z);
-        const RefView<S> Vn{now};
-        const RefView<S> Vf{fut};
+        const RefView<S> Vn{now, P.gen != 0, P.div_tol};
+        const RefView<S> Vf{fut, P.gen != 0, P.div_tol};
         // WilsonLoops::*::calcConstraintContributions (WilsonLoops/Source/StandardModel.cpp:274-322,
         // TwoHDM.cpp:312-396)
         S el[NEQ];

@@ -206,8 +206,8 @@ extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, c
         set_last_error("gft_observe_static: periodic lattices only (fixed_axes must be 0)");
         return GFT_E_UNSUPPORTED;
     }
-    if (c->higgs_family != GFT_HF_NONE) {
-        set_last_error("gft_observe_static: no Higgs-family gauge field (gaugeNum 4 only)");
+    if (c->higgs_family != GFT_HF_NONE || c->generator_rep) {
+        set_last_error("gft_observe_static: quaternion links without a Higgs-family field only");
         return GFT_E_UNSUPPORTED;
     }
     const long long n = (long long)c->nx * c->ny * c->nz;

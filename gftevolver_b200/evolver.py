@@ -6,7 +6,8 @@ the reference keeps in ``Lattice`` and ``Model`` (Core/Header/Lattice.hpp:22-212
 Core/Header/Model.hpp:23-266).  Host arrays use the reference layout
 ``scalars[2, nx, ny, nz, nsc]``, ``vectors[2, nx, ny, nz, 3 * dw]`` (dw = 5 link
 words per direction, 6 or 9 with a 2HDM Higgs-family U(1) phase or SU(2)
-quaternion, ``WilsonLoops/Source/TwoHDM.cpp:210-242``).
+quaternion, ``WilsonLoops/Source/TwoHDM.cpp:210-242``; 4, 5 or 7 in the generator
+representation).
 """
 from __future__ import annotations
 
@@ -68,6 +69,7 @@ class LatticeParams:
     gauss_every: int = 0
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (frozen shell), else periodic
     higgs_family: int = 0      # 2HDM Higgs-family gauge field: 0 none, 1 U(1) (gaugeNum 5), 2 SU(2) (gaugeNum 7)
+    generator_rep: int = 0     # host links as 3 generators w (U = exp(i w.sigma)) instead of quaternions
 
     @property
     def nsc(self) -> int:
@@ -75,8 +77,9 @@ class LatticeParams:
 
     @property
     def nve(self) -> int:
-        """Link words per site in the reference layout (3 directions x 5, 6 or 9)."""
-        return 3 * {0: 5, 1: 6, 2: 9}[self.higgs_family]
+        """Link words per site in the reference layout (3 directions x 5, 6 or 9; generators 4, 5 or 7)."""
+        lw = 3 if self.generator_rep else 4
+        return 3 * (1 + lw + {0: 0, 1: 1, 2: lw}[self.higgs_family])
 
     @property
     def neq(self) -> int:

@@ -151,15 +151,6 @@ Run configure(const std::string& root)
             throw std::runtime_error("faces of axis " + std::to_string(a) +
                                      ": only periodic (3 3) or Fixed (1 1) pairs run on the GPU");
     }
-    // link words per direction: 5 (gaugeNum 4), 6 (+ Higgs-family U(1)), 9 (+ Higgs-family SU(2))
-    // in the quaternion representation (WilsonLoops/Source/TwoHDM.cpp:229-241)
-    if (nvec == 6)
-        c.higgs_family = GFT_HF_U1;
-    else if (nvec == 9)
-        c.higgs_family = GFT_HF_SU2;
-    else if (nvec != 5)
-        throw std::runtime_error("vector components per direction: 5, 6 or 9 (quaternion representation) run on the "
-                                 "GPU, not " + std::to_string(nvec));
 
     // Core/Config/Model.cfg (Core/Source/Model.cpp:173-221)
     const std::string mod = root + "/Core/Config/Model.cfg";
@@ -173,8 +164,7 @@ Run configure(const std::string& root)
         throw std::runtime_error("model (potential " + std::to_string(pot) + ", gradient " + std::to_string(grad) +
                                  ", wilson loop " + std::to_string(wl) + ", " + std::to_string(nsc) +
                                  " scalars) is not built for the GPU");
-    if (c.higgs_family != GFT_HF_NONE && c.model != GFT_MODEL_2HDM)
-        throw std::runtime_error(std::to_string(nvec) + " vector components per direction need the 2HDM (TwoHDM wilson loops)");
+
     c.damping = (float)num(M, 3, 0, mod);
     c.nt_damped = inum(M, 4, 0, mod);
     if (inum(M, 5, 0, mod)) c.nt_damped = static_cast<int>((float)num(M, 6, 0, mod) / c.dt);
@@ -220,8 +210,31 @@ Run configure(const std::string& root)
         c.g = num(W, 0, 0, w);
         c.gp = num(W, 1, 0, w);
         c.gpp = num(W, 2, 0, w);
-        if (inum(W, 3, 0, w)) throw std::runtime_error("the generator link representation does not run on the GPU");
+        c.generator_rep = inum(W, 3, 0, w) != 0;
         c.div_tol = num(W, 4, 0, w);
+    }
+    // link words per direction (WilsonLoops/Source/StandardModel.cpp:195-210, TwoHDM.cpp:215-241):
+    // SM 5 (quaternion) or 4 (generators); TwoHDM 5 / 6 / 9 (gaugeNum 4 / 5 / 7), or 4 / 5 / 7
+    // with the generator representation
+    if (c.model == GFT_MODEL_SM) {
+        if (nvec == 4)
+            c.generator_rep = 1;
+        else if (nvec != 5)
+            throw std::runtime_error("WilsonLoops::StandardModel needs 4 or 5 vector components per direction, not " +
+                                     std::to_string(nvec));
+    } else {
+        const int lw = c.generator_rep ? 3 : 4;
+        if (nvec == 1 + lw)
+            c.higgs_family = GFT_HF_NONE;
+        else if (nvec == 2 + lw)
+            c.higgs_family = GFT_HF_U1;
+        else if (nvec == 1 + 2 * lw)
+            c.higgs_family = GFT_HF_SU2;
+        else
+            throw std::runtime_error("WilsonLoops::TwoHDM (" + std::string(c.generator_rep ? "generator" : "quaternion") +
+                                     " representation) needs " + std::to_string(1 + lw) + ", " + std::to_string(2 + lw) +
+                                     " or " + std::to_string(1 + 2 * lw) + " vector components per direction, not " +
+                                     std::to_string(nvec));
     }
 
     // Analysers/Config/*.cfg (Analysers/Source/Energy.cpp:14-47, GaugeCondition.cpp:14-47, OutputFields.cpp:14-45)
@@ -287,7 +300,11 @@ void dump_fields(const std::string& path, const std::vector<T>& sc, const std::v
 }
 
 // Link words per site and gauge equations per direction of a configuration.
-int vector_words(const gft_config& c) { return 3 * (c.higgs_family == GFT_HF_U1 ? 6 : (c.higgs_family == GFT_HF_SU2 ? 9 : 5)); }
+int vector_words(const gft_config& c)
+{
+    const int lw = c.generator_rep ? 3 : 4;
+    return 3 * (1 + lw + (c.higgs_family == GFT_HF_U1 ? 1 : (c.higgs_family == GFT_HF_SU2 ? lw : 0)));
+}
 int gauss_count(const gft_config& c) { return c.higgs_family == GFT_HF_U1 ? 5 : (c.higgs_family == GFT_HF_SU2 ? 7 : 4); }
 
 // RandomUniform::setInitialFields: one std::mt19937 stream per field array from
@@ -329,12 +346,14 @@ void host_initial(const Run& r, const std::string& ic_path, std::vector<T>& sc, 
     }
     std::fill(sc.begin(), sc.end(), (T)0);
     std::fill(ve.begin(), ve.end(), (T)0);
+    // zero gauge field: identity quaternions (Core/Source/Lattice.cpp:369-395); all zero generators
     const int nve = vector_words(r.cfg), dw = nve / 3;
-    for (size_t s = 0; s < ve.size() / nve; s++)
-        for (int d = 0; d < 3; d++) {
-            ve[s * nve + d * dw + 1] = (T)1;               // identity isospin link
-            if (dw == 9) ve[s * nve + d * dw + 5] = (T)1;  // identity Higgs-family SU(2) link
-        }
+    if (!r.cfg.generator_rep)
+        for (size_t s = 0; s < ve.size() / nve; s++)
+            for (int d = 0; d < 3; d++) {
+                ve[s * nve + d * dw + 1] = (T)1;               // identity isospin link
+                if (dw == 9) ve[s * nve + d * dw + 5] = (T)1;  // identity Higgs-family SU(2) link
+            }
     if (r.ic.type[0] == 1) random_uniform(sc, r.ic);
     if (r.ic.type[1] == 1) random_uniform(ve, r.ic);
 }
@@ -491,7 +510,7 @@ int main(int argc, char** argv)
                         c.energy_offset);
             std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s fixed_axes %d\n", c.energy_every,
                         c.gauss_every, r.an.energy_path.c_str(), r.an.gauss_path.c_str(), c.fixed_axes);
-            std::printf("higgs_family %d gpp %.17g\n", c.higgs_family, c.gpp);
+            std::printf("higgs_family %d gpp %.17g generator_rep %d\n", c.higgs_family, c.gpp, c.generator_rep);
             std::printf("ic_scalar %d ic_gauge %d ic_seed %u ic_min %.9g ic_max %.9g ic_equal %d\n", r.ic.type[0],
                         r.ic.type[1], r.ic.seed, r.ic.lo, r.ic.hi, (int)r.ic.equal);
             return 0;

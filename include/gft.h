@@ -16,7 +16,11 @@
  *     658-671): scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][3 * dw] with
  *     per direction [theta_Y, c0, c1, c2, c3] (quaternion representation, dw = 5),
  *     followed for a 2HDM Higgs-family gauge field by theta_H (dw = 6) or the
- *     family quaternion d0..d3 (dw = 9) (WilsonLoops/Source/TwoHDM.cpp:210-242).
+ *     family quaternion d0..d3 (dw = 9) (WilsonLoops/Source/TwoHDM.cpp:210-242); with
+ *     generator_rep, [theta_Y, w1, w2, w3] (dw = 4, 5 or 7).  The reference-arithmetic
+ *     form keeps the generators on the device and converts on every access as the
+ *     reference does; the throughput forms convert at upload / download and evolve
+ *     quaternions (the same group elements, different rounding).
  *     Level index = the reference's time slot; at time step time_iter the
  *     "now" slot is (time_iter + 1) % 2 (Lattice.cpp:773-774).
  *   - Device memory is owned by the handle; host buffers are caller-owned and
@@ -41,7 +45,7 @@ extern "C" {
 /* ---- status codes ------------------------------------------------------ */
 #define GFT_OK 0
 #define GFT_E_INVALID (-1)      /* bad argument / configuration (reference: std::runtime_error at construction) */
-#define GFT_E_UNSUPPORTED (-2)  /* combination not built (e.g. generator representation) */
+#define GFT_E_UNSUPPORTED (-2)  /* combination not built (e.g. a Higgs-family field in an ensemble) */
 #define GFT_E_CUDA (-3)         /* CUDA runtime error; see gft_last_error */
 #define GFT_E_NOMEM (-4)        /* device allocation failed */
 #define GFT_E_STATE (-5)        /* call out of order (e.g. evolve before upload) */
@@ -95,6 +99,9 @@ typedef struct gft_config {
                                       (BoundaryConditions/Source/Fixed.cpp:159-251, Core/Source/Lattice.cpp:217-306). */
     int higgs_family;              /* GFT_HF_*: 2HDM Higgs-family gauge field (model 2 only) */
     double gpp;                    /* its coupling g'' (WilsonLoops/Config/TwoHDM.cfg) */
+    int generator_rep;             /* 1: host vectors hold each SU(2) link as its 3 generators w,
+                                      U = (cos|w|, sin|w| w/|w|) (WilsonLoops/Source/StandardModel.cpp:76-160):
+                                      4 words per direction [theta_Y, w1, w2, w3] (+ theta_H or w'1..w'3) */
 } gft_config;
 
 /* One row of global observables (Analysers/Source/Energy.cpp:169-220,

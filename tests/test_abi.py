@@ -84,6 +84,10 @@ def test_create_rejects_invalid_config_without_gpu(lib):
     cfg.model = _lib.GFT_MODEL_2HDM
     cfg.higgs_family = 3
     assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
+    cfg.higgs_family = 0
+    cfg.generator_rep = 2
+    assert lib.gft_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.GFT_E_INVALID
+    assert b"generator_rep" in lib.gft_last_error(None)
     assert not h.value
 
 
@@ -110,4 +114,7 @@ def test_batch_create_validates_members_without_gpu(lib):
     cfgs = (_lib.GftConfig * 1)(make_config(e))
     assert lib.gft_batch_create(cfgs, 1, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
     assert b"Higgs-family" in lib.gft_last_error(None)
+    f = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, generator_rep=1)
+    cfgs = (_lib.GftConfig * 1)(make_config(f))
+    assert lib.gft_batch_create(cfgs, 1, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
     assert not h.value

@@ -207,6 +207,67 @@ def test_higgs_family_is_refused_where_not_built(oracle_mod):
         assert ev.step_kernel_name == "fast_step_kernel"
 
 
+@pytest.mark.parametrize("model,hf", [(1, 0), (2, 0), (2, 1), (2, 2)], ids=["sm", "2hdm", "2hdm_hf_u1", "2hdm_hf_su2"])
+@pytest.mark.parametrize("shape", [(8, 8, 32), (5, 6, 7)])
+def test_generator_representation_forms_vs_oracle(oracle_mod, model, hf, shape):
+    """Links stored as generators (WilsonLoops/Source/StandardModel.cpp:76-160): the
+    reference-arithmetic form converts on every access as the reference does; the
+    throughput forms convert at the transfer and evolve quaternions (8 x 8 x 32 SM
+    mixed runs the tiled kernel)."""
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, energy_every=5, gauss_every=5, higgs_family=hf,
+                           gpp=0.47, generator_rep=1)
+    ic = oracle_mod.ICSpec(seed=777 + nz + hf, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8,
+                           theta_sigma=0.1, eps_sigma=0.1)
+    p = _lp(op.__dict__)
+    sc64, ve64 = oracle_mod.init_fields(op, ic, np.float64)
+    assert ve64.shape[-1] == op.nve
+    o_sc, o_ve = sc64.copy(), ve64.copy()
+    o_rows, _ = oracle_mod.evolve(op, o_sc, o_ve, 10)
+    for form in ("fp64", "ref64"):
+        sc, ve, rows, warn = run_gpu(p, form, sc64, ve64, 10)
+        assert warn == 0
+        assert rel_err(sc, o_sc) <= 1e-12, form
+        assert rel_err(ve, o_ve) <= 1e-12, form
+        for a, b in zip(rows, o_rows):
+            if b["has_energy"]:
+                assert abs(a["energy"] - b["energy"]) <= 1e-12 * abs(b["energy"]), form
+            if b["has_gauss"]:
+                np.testing.assert_allclose(a["gauss_max"], b["gauss_max"], rtol=1e-8, atol=1e-13)
+    sc32, ve32 = oracle_mod.init_fields(op, ic, np.float32)
+    from gftevolver_b200 import Evolver
+    with Evolver(p, form="mixed") as ev:
+        ev.upload(sc32, ve32, 0)
+        rows = ev.evolve(10)
+        sc, ve = ev.download()
+        if model == 1 and shape == (8, 8, 32):
+            assert ev.step_kernel_name == "tiled_step_kernel"
+    assert np.max(np.abs(sc.astype(np.float64) - o_sc)) <= 6e-6
+    assert np.max(np.abs(ve.astype(np.float64) - o_ve)) <= 6e-6
+    for a, b in zip(rows, o_rows):
+        if b["has_energy"]:
+            assert abs(a["energy"] - b["energy"]) <= 1e-6 * abs(b["energy"])
+    o32_sc, o32_ve = sc32.copy(), ve32.copy()
+    oracle_mod.evolve(op, o32_sc, o32_ve, 10)
+    sc, ve, rows, _ = run_gpu(p, "ref32", sc32, ve32, 10)
+    assert ulp_close(sc, o32_sc, 8).all()
+    assert ulp_close(ve, o32_ve, 8).all()
+
+
+@pytest.mark.parametrize("form,dtype,tol", [("ref32", np.float32, 0.0), ("fp64", np.float64, 1e-15)])
+def test_generator_representation_device_initial_data(oracle_mod, form, dtype, tol):
+    """Device initial data in the generator representation: w = eps n."""
+    from gftevolver_b200 import Evolver, InitialData
+    op = oracle_mod.Params(model=2, nx=5, ny=6, nz=7, higgs_family=2, generator_rep=1)
+    spec = dict(seed=93, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    with Evolver(_lp(op.__dict__), form=form) as ev:
+        ev.init_fields(InitialData(**spec))
+        g_sc, g_ve = ev.download()
+    o_sc, o_ve = oracle_mod.init_fields(op, oracle_mod.ICSpec(**spec), dtype)
+    assert np.max(np.abs(g_sc.astype(np.float64) - o_sc)) <= max(tol, 1e-7 if dtype == np.float32 else 0) * 4
+    assert np.max(np.abs(g_ve.astype(np.float64) - o_ve)) <= max(tol, 1e-7 if dtype == np.float32 else 0)
+
+
 def test_time_iter_parity_and_chunking(oracle_mod):
     """Evolving 3 + 4 steps equals 7 steps; the now/past slot follows time_iter (Lattice.cpp:773)."""
     op = oracle_mod.Params(nx=6, ny=5, nz=4, energy_every=2, gauss_every=3)

@@ -30,9 +30,10 @@ def gft_run():
     return GFT_RUN
 
 
-def _params(orc, model, fixed_axes=0, higgs_family=0):
+def _params(orc, model, fixed_axes=0, higgs_family=0, generator_rep=0):
     return orc.Params(model=model, nx=6, ny=5, nz=8, dt=0.05, damping=0.3, nt_damped=2, energy_every=2,
-                      gauss_every=3, g=0.61, gp=0.33, fixed_axes=fixed_axes, higgs_family=higgs_family, gpp=0.47)
+                      gauss_every=3, g=0.61, gp=0.33, fixed_axes=fixed_axes, higgs_family=higgs_family, gpp=0.47,
+                      generator_rep=generator_rep)
 
 
 @pytest.mark.parametrize("model", [1, 2])
@@ -81,7 +82,19 @@ def test_higgs_family_is_read_from_the_vector_width(tmp_path, oracle_mod, gft_ru
         lat.write_text(lat.read_text().replace("vector components per direction: 5",
                                                "vector components per direction: " + ("6" if hf == 1 else "9")))
         r = subprocess.run([gft_run, str(tmp_path), "--print-config"], capture_output=True, text=True)
-        assert r.returncode == 1 and "2HDM" in r.stderr
+        assert r.returncode == 1 and "StandardModel needs 4 or 5" in r.stderr
+
+
+@pytest.mark.parametrize("model,hf", [(1, 0), (2, 0), (2, 1), (2, 2)])
+def test_generator_representation_is_parsed(tmp_path, oracle_mod, gft_run, model, hf):
+    """SM: 4 vector components per direction mean generators (WilsonLoops/Source/StandardModel.cpp:195-210);
+    TwoHDM: the flag in TwoHDM.cfg with 4, 5 or 7 components."""
+    from oracle import refrun
+    refrun.write_configs(str(tmp_path), _params(oracle_mod, model, higgs_family=hf, generator_rep=1), 7)
+    out = subprocess.run([gft_run, str(tmp_path), "--print-config"], capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert int(out[out.index("generator_rep") + 1]) == 1
+    assert int(out[out.index("higgs_family") + 1]) == hf
 
 
 def test_fixed_faces_are_parsed(tmp_path, oracle_mod, gft_run):
@@ -97,12 +110,13 @@ def _numbers(path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("model,fixed_axes,hf", [(1, 0, 0), (2, 0, 0), (1, 5, 0), (2, 0, 1), (2, 0, 2)])
-def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_run, model, fixed_axes, hf):
+@pytest.mark.parametrize("model,fixed_axes,hf,gen", [(1, 0, 0, 0), (2, 0, 0, 0), (1, 5, 0, 0), (2, 0, 1, 0),
+                                                     (2, 0, 2, 0), (1, 0, 0, 1), (2, 0, 2, 1)])
+def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_run, model, fixed_axes, hf, gen):
     from oracle import refrun
     if not refrun.available(False):
         pytest.skip("oracle/_ref/ref32 not built")
-    p = _params(oracle_mod, model, fixed_axes, hf)
+    p = _params(oracle_mod, model, fixed_axes, hf, gen)
     ic = oracle_mod.ICSpec(seed=5, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                            eps_sigma=0.1)
     sc, ve = oracle_mod.init_fields(p, ic, np.float32)
@@ -128,8 +142,8 @@ def test_dat_rows_and_fields_match_the_reference_run(tmp_path, oracle_mod, gft_r
 
 @pytest.mark.parametrize("ic_types,random_uniform", [((1, 0), (42, -1.0, 1.0, 1)), ((0, 1), (7, -0.5, 0.25, 0)),
                                                      ((1, 1), (-3, 0.0, 2.0, 1)), ((0, 0), (42, -1.0, 1.0, 1))])
-@pytest.mark.parametrize("model,hf", [(1, 0), (2, 0), (2, 2)])
-def test_configured_initial_condition_matches_the_reference(tmp_path, oracle_mod, gft_run, model, hf, ic_types,
+@pytest.mark.parametrize("model,hf,gen", [(1, 0, 0), (2, 0, 0), (2, 2, 0), (1, 0, 1)])
+def test_configured_initial_condition_matches_the_reference(tmp_path, oracle_mod, gft_run, model, hf, gen, ic_types,
                                                             random_uniform):
     """Zero scalars / identity links and RandomUniform (Core/Source/Lattice.cpp:358-401,
     InitialConditions/Source/RandomUniform.cpp:60-77), bit for bit against the
@@ -137,7 +151,7 @@ def test_configured_initial_condition_matches_the_reference(tmp_path, oracle_mod
     from oracle import refrun
     if not refrun.available(False):
         pytest.skip("oracle/_ref/ref32 not built")
-    p = _params(oracle_mod, model, higgs_family=hf)
+    p = _params(oracle_mod, model, higgs_family=hf, generator_rep=gen)
     ref_dir = tmp_path / "ref"
     ref_dir.mkdir()
     refrun.run(p, None, None, 1, workdir=str(ref_dir), ic_types=ic_types, random_uniform=random_uniform)
