@@ -90,8 +90,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
 def build_host() -> str:
     """The gft_run program (g++, linked against the in-tree library with an $ORIGIN rpath)."""
     cxx = os.environ.get("CXX", "g++")
-    cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), os.path.join(HERE, "host", "gft_run.cpp"),
-           "-L", HERE, "-lgft_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_RUN]
+    cmd = [cxx, "-O2", "-std=c++17", "-pthread", "-I", os.path.join(ROOT, "include"),
+           os.path.join(HERE, "host", "gft_run.cpp"), "-L", HERE, "-lgft_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_RUN]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"host program build failed:\n{r.stdout}")

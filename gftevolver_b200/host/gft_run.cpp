@@ -30,16 +30,19 @@
 // --initial-only writes the host-built initial data to --initial-bin and exits
 // without opening a device.
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <random>
 #include <iostream>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
 #include <sys/stat.h>
+#include <thread>
 #include <vector>
 
 #include "gft.h"
@@ -288,6 +291,7 @@ void dump_fields(const std::string& path, const std::vector<T>& sc, const std::v
                  bool both)
 {
     std::ofstream ofs(path);
+    if (!ofs) throw std::runtime_error("cannot open for writing");
     const size_t nsite2 = sc.size() / nsc;
     const size_t nve = ve.size() / nsite2;
     const size_t n = both ? nsite2 : nsite2 / 2;
@@ -298,6 +302,78 @@ void dump_fields(const std::string& path, const std::vector<T>& sc, const std::v
         ofs << std::endl;
     }
 }
+
+// OutputFields dumps written by a background thread, so that formatting and
+// writing the text of one dump overlaps the evolution to the next one.  One
+// dump is in flight at most: submit() waits for the previous one, then swaps
+// the caller's buffers with the writer's (the caller gets the previous, written
+// buffers back, resized, to download into).
+template <class T>
+class FieldWriter {
+public:
+    FieldWriter() : worker_([this] { loop(); }) {}
+    ~FieldWriter() { finish(); }
+
+    void submit(const std::string& path, std::vector<T>& sc, std::vector<T>& ve, int nsc, int time_step, bool both)
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !busy_; });
+        if (!err_.empty()) throw std::runtime_error(err_);
+        path_ = path;
+        sc_.swap(sc);
+        ve_.swap(ve);
+        sc.resize(sc_.size());
+        ve.resize(ve_.size());
+        nsc_ = nsc;
+        step_ = time_step;
+        both_ = both;
+        busy_ = true;
+        cv_.notify_all();
+    }
+
+    // Waits for the last dump and stops the thread; returns the first write error ("" if none).
+    std::string finish()
+    {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return !busy_; });
+            stop_ = true;
+        }
+        cv_.notify_all();
+        if (worker_.joinable()) worker_.join();
+        return err_;
+    }
+
+private:
+    void loop()
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_.wait(lk, [&] { return busy_ || stop_; });
+            if (!busy_) return;
+            lk.unlock();
+            std::string e;
+            try {
+                dump_fields(path_, sc_, ve_, nsc_, step_, both_);
+            } catch (const std::exception& ex) {
+                e = ex.what();
+            }
+            lk.lock();
+            if (!e.empty() && err_.empty()) err_ = "OutputFields " + path_ + ": " + e;
+            busy_ = false;
+            cv_.notify_all();
+        }
+    }
+
+    std::mutex mu_;
+    std::condition_variable cv_;
+    bool busy_ = false, stop_ = false;
+    std::string err_, path_;
+    std::vector<T> sc_, ve_;
+    int nsc_ = 0, step_ = 0;
+    bool both_ = false;
+    std::thread worker_;
+};
 
 // Link words per site and gauge equations per direction of a configuration.
 int vector_words(const gft_config& c)
@@ -405,10 +481,13 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
         check(gft_init_fields(h, &ic), h, "gft_init_fields");
     }
 
-    // initialAnalysis
+    // initialAnalysis (OutputFields, Analysers/Source/OutputFields.cpp:63-133, 155-200: text dumps in a
+    // background thread)
+    FieldWriter<T> writer;
     if ((r.an.fields && r.an.fields_initial) || !initial_bin.empty()) download();
-    if (r.an.fields && r.an.fields_initial) dump_fields(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
     if (!initial_bin.empty()) write_bin(initial_bin, sc, ve);
+    if (r.an.fields && r.an.fields_initial)
+        writer.submit(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
 
     // evolve: chunks end where OutputFields writes a continual dump
     const int chunk_max = (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0) ? r.an.fields_freq : 1000;
@@ -439,21 +518,19 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
         }
         if (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0 && done % r.an.fields_freq == 0) {
             download();
-            dump_fields(data + "/" + r.an.fields_continual_path + "_" + std::to_string(done) + ".dat", sc, ve, nsc, done,
-                        r.an.fields_both);
+            writer.submit(data + "/" + r.an.fields_continual_path + "_" + std::to_string(done) + ".dat", sc, ve, nsc,
+                          done, r.an.fields_both);
         }
     }
 
     // finalAnalysis
     download();
+    if (!final_bin.empty()) write_bin(final_bin, sc, ve);
     if (r.an.fields && r.an.fields_final)
-        dump_fields(data + "/" + r.an.fields_final_path, sc, ve, nsc, r.nt, r.an.fields_both);
-    if (!final_bin.empty()) {
-        std::ofstream f(final_bin, std::ios::binary);
-        f.write(reinterpret_cast<const char*>(sc.data()), sc.size() * sizeof(T));
-        f.write(reinterpret_cast<const char*>(ve.data()), ve.size() * sizeof(T));
-    }
+        writer.submit(data + "/" + r.an.fields_final_path, sc, ve, nsc, r.nt, r.an.fields_both);
+    const std::string werr = writer.finish();
     gft_destroy(h);
+    if (!werr.empty()) throw std::runtime_error(werr);
     return 0;
 }
 

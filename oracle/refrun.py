@@ -57,9 +57,12 @@ def _write(path: str, lines: list[str]) -> None:
         f.write("\n".join(lines) + "\n")
 
 
-def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1)) -> None:
+def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1),
+                  output_fields=None) -> None:
     """ic_types: Lattice.cfg initial-condition types (0 zero / identity links, 1 RandomUniform);
-    random_uniform: InitialConditions/Config/RandomUniform.cfg (seed, min, max, equal time levels)."""
+    random_uniform: InitialConditions/Config/RandomUniform.cfg (seed, min, max, equal time levels);
+    output_fields: None (OutputFields off) or (both levels, initial, final, continual, frequency)
+    for Analysers/Config/OutputFields.cfg."""
     sm = p.model == orc.MODEL_SM
     # Core/Config/Lattice.cfg -- Lattice::configure (Lattice.cpp:47-143)
     lat = _header(10, "Lattice")
@@ -82,7 +85,7 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
         f"types                          : {ic_types[0]} {ic_types[1]}",
         "",
         "analysis options",
-        "output fields                  : 0",
+        f"output fields                  : {0 if output_fields is None else 1}",
         f"calculate energy               : {1 if p.energy_every > 0 else 0}",
         f"calculate gauge condition      : {1 if p.gauss_every > 0 else 0}",
         "",
@@ -178,6 +181,18 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
         ]
         _write(os.path.join(work, "Potentials", "Config", "Double_SO_N.cfg"), d)
 
+    # Analysers/Config/OutputFields.cfg (OutputFields.cpp:5-49)
+    if output_fields is not None:
+        both, initial, final, continual, freq = output_fields
+        of = _header(13, "OutputFields")
+        of += [f"both time levels               : {int(both)}", f"initial                        : {int(initial)}",
+               f"final                          : {int(final)}", "",
+               f"continual                      : {int(continual)}", f"frequency                      : {int(freq)}", "",
+               "initial path                   : initial_fields.dat",
+               "continual path                 : Continual/fields",
+               "final path                     : final_fields.dat"]
+        _write(os.path.join(work, "Analysers", "Config", "OutputFields.cfg"), of)
+
     # Analysers/Config/Energy.cfg (Energy.cpp:14-47)
     ef = max(p.energy_every, 1)
     en = _header(13, "Energy")
@@ -201,7 +216,8 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
 
 
 def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, nt: int, fp64: bool = False,
-        workdir: str | None = None, timeout: float = 600.0, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1)):
+        workdir: str | None = None, timeout: float = 600.0, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1),
+        output_fields=None):
     """Run the reference binary from the given two-level initial data, or (scalars
     None) from its own configured initial condition (ic_types, random_uniform).
 
@@ -219,7 +235,7 @@ def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, n
         scalars = np.zeros((2, p.nx, p.ny, p.nz, p.nsc), dtype)
         vectors = np.zeros((2, p.nx, p.ny, p.nz, p.nve), dtype)
     try:
-        write_configs(work, p, nt, ic_types, random_uniform)
+        write_configs(work, p, nt, ic_types, random_uniform, output_fields)
         icp = os.path.join(work, "ic.bin")
         if given:
             with open(icp, "wb") as f:

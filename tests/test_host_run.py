@@ -177,6 +177,34 @@ def test_initial_only_refuses_device_initial_data(tmp_path, oracle_mod, gft_run)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("both", [0, 1])
+def test_output_fields_dumps_match_the_reference(tmp_path, oracle_mod, gft_run, both):
+    """OutputFields (Analysers/Source/OutputFields.cpp:63-200): the initial, every continual
+    (after steps 3 and 6) and the final dump, one or both time levels, against the reference
+    run's own files.  Values print with 6 significant digits; where the ref32 fields differ
+    from the reference's in the last float bits the printed digit may differ by one."""
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("oracle/_ref/ref32 not built")
+    p = _params(oracle_mod, 2, higgs_family=1)
+    ic = oracle_mod.ICSpec(seed=8, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(p, ic, np.float32)
+    ref_dir, gpu_dir = tmp_path / "ref", tmp_path / "gpu"
+    ref_dir.mkdir()
+    refrun.run(p, sc, ve, 7, workdir=str(ref_dir), output_fields=(both, 1, 1, 1, 3))
+    shutil.copytree(ref_dir, gpu_dir, ignore=shutil.ignore_patterns("Data", "final.bin", "rows.txt", "timing.txt"))
+    subprocess.run([gft_run, str(gpu_dir), "--form", "ref32", "--ic", str(gpu_dir / "ic.bin")], check=True,
+                   capture_output=True, text=True)
+    names = ["initial_fields.dat", "Continual/fields_3.dat", "Continual/fields_6.dat", "final_fields.dat"]
+    for name in names:
+        a, b = _numbers(gpu_dir / "Data" / name), _numbers(ref_dir / "Data" / name)
+        assert len(a) == len(b) == p.nsite * (2 if both else 1), name
+        a, b = np.array(a), np.array(b)
+        assert a.shape == b.shape == (len(b), p.nsc + p.nve), name
+        np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-6, err_msg=name)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("model", [1, 2])
 def test_configured_initial_condition_run_matches_the_reference(tmp_path, oracle_mod, gft_run, model):
     """The whole job from the configured initial condition (RandomUniform scalars,
