@@ -58,6 +58,7 @@ class GftConfig(ctypes.Structure):
         ("fixed_axes", ctypes.c_int),
         ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
         ("generator_rep", ctypes.c_int),
+        ("energy_local_every", ctypes.c_int), ("gauss_local_every", ctypes.c_int),
     ]
 
 
@@ -109,6 +110,8 @@ SIGNATURES = {
     "gft_step_kernel_ms": (ctypes.c_double, [_H, ctypes.POINTER(ctypes.c_int)]),
     "gft_step_kernel_name": (ctypes.c_char_p, [_H]),
     "gft_launch_count": (ctypes.c_longlong, [_H]),
+    "gft_local_fields": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gft_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gft_observe_static": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

@@ -82,6 +82,10 @@ struct gft_handle {
     int x_offset = 0, nx_global = 0;
     gft_exchange_fn exchange = nullptr;
     void* exchange_user = nullptr;
+    // per-site analyser outputs (gft_local_fields)
+    float* d_loc_e = nullptr;   // [nsite][6]
+    float* d_loc_g = nullptr;   // [nsite][neq]
+    int loc_e_step = -1, loc_g_step = -1;
 
     int fail(int code, const std::string& msg)
     {
@@ -334,7 +338,7 @@ int validate(const gft_config* c, std::string& why)
         why = "gft_create: spacings and time step must be positive";
         return GFT_E_INVALID;
     }
-    if (c->energy_every < 0 || c->gauss_every < 0) {
+    if (c->energy_every < 0 || c->gauss_every < 0 || c->energy_local_every < 0 || c->gauss_local_every < 0) {
         why = "gft_create: analyser frequencies must be >= 0";
         return GFT_E_INVALID;
     }
@@ -445,6 +449,16 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     h->part_cap = nb;
     h->dev_bytes += pe + pg + sizeof(unsigned) + kRowSlots * sizeof(double) * (1 + h->rows_cap) +
                     kFinMidCapacity * sizeof(double);
+    // per-site analyser outputs, zeroed (sites on Fixed faces stay 0, as in the reference)
+    const size_t le = cfg->energy_local_every > 0 ? (size_t)h->nsite * 6 * sizeof(float) : 0;
+    const size_t lg = cfg->gauss_local_every > 0 ? (size_t)h->nsite * h->neq * sizeof(float) : 0;
+    if ((le && ((e = cudaMalloc(&h->d_loc_e, le)) != cudaSuccess || (e = cudaMemset(h->d_loc_e, 0, le)) != cudaSuccess)) ||
+        (lg && ((e = cudaMalloc(&h->d_loc_g, lg)) != cudaSuccess || (e = cudaMemset(h->d_loc_g, 0, lg)) != cudaSuccess))) {
+        h->fail(GFT_E_NOMEM, std::string("cudaMalloc(local outputs): ") + cudaGetErrorString(e));
+        gft_destroy(h);
+        return GFT_E_NOMEM;
+    }
+    h->dev_bytes += le + lg;
     double scale[kRowSlots];
     row_scales(*cfg, h->nsite, scale);
     cudaMemcpy(h->d_scale, scale, sizeof(scale), cudaMemcpyHostToDevice);
@@ -484,6 +498,8 @@ void gft_destroy(gft_handle* h)
     cudaFree(h->d_mid);
     cudaFree(h->d_rows);
     cudaFree(h->d_stage);
+    cudaFree(h->d_loc_e);
+    cudaFree(h->d_loc_g);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -639,14 +655,21 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
     for (int s = 0; s < n_steps && err == cudaSuccess; s++) {
         const int ti = h->time_iter;
         const int tn = (ti + 1) % 2, tp = 1 - tn;
-        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;
+        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;  // rows
         const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
-        const StepParams P = make_params(h, ti, e);
+        // local outputs: the energy pass (and its renormalisation) also runs on their steps
+        const bool el = c.energy_local_every > 0 && ti % c.energy_local_every == 0;
+        const bool gl = c.gauss_local_every > 0 && ti % c.gauss_local_every == 0;
+        StepParams P = make_params(h, ti, e || el);
+        P.loc_energy = el ? h->d_loc_e : nullptr;
+        P.loc_gauss = gl ? h->d_loc_g : nullptr;
+        if (el) h->loc_e_step = ti;
+        if (gl) h->loc_g_step = ti;
         const bool prof = h->profile && h->ev_used < kMaxProfiled;
         if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
-        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e);
-        h->launches += 1 + (e ? finalize_launches(step_blocks(h, P), true) : 0) +
-                       (g ? 1 + finalize_launches(gauss_blocks(h, P), true) : 0);
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e || el);
+        h->launches += 1 + (e ? finalize_launches(step_blocks(h, P), true) : 0) + ((g || gl) ? 1 : 0) +
+                       (g ? finalize_launches(gauss_blocks(h, P), true) : 0);
         if (prof) {
             cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
             h->ev_used++;
@@ -663,9 +686,9 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
                 return h->fail(GFT_E_STATE, "gft_evolve: the exchange callback failed (" + std::to_string(xr) + ")");
             }
         }
-        if (g && err == cudaSuccess) {
+        if ((g || gl) && err == cudaSuccess) {
             err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
-            if (err == cudaSuccess)
+            if (err == cudaSuccess && g)
                 err = launch_finalize(h->d_part_g, gauss_blocks(h, P), 2 * h->neq, h->neq, h->d_scale + kObsCount,
                                       out + kObsCount, h->d_mid, h->stream);
         }
@@ -870,6 +893,25 @@ double gft_step_kernel_ms(gft_handle* h, int* launches)
 }
 
 long long gft_launch_count(const gft_handle* h) { return h ? h->launches : 0; }
+
+int gft_local_fields(gft_handle* h, float* energy, float* gauss, int* energy_step, int* gauss_step)
+{
+    if (!h) return GFT_E_INVALID;
+    if (energy_step) *energy_step = h->loc_e_step;
+    if (gauss_step) *gauss_step = h->loc_g_step;
+    if ((energy && !h->d_loc_e) || (gauss && !h->d_loc_g))
+        return h->fail(GFT_E_STATE, "gft_local_fields: no local-output cadence was configured for that analyser");
+    cudaSetDevice(h->cfg.device);
+    cudaError_t e = cudaSuccess;
+    if (energy)
+        e = cudaMemcpyAsync(energy, h->d_loc_e, (size_t)h->nsite * 6 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (gauss && e == cudaSuccess)
+        e = cudaMemcpyAsync(gauss, h->d_loc_g, (size_t)h->nsite * h->neq * sizeof(float), cudaMemcpyDeviceToHost,
+                            h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_local_fields");
+    return GFT_OK;
+}
 
 int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_end)
 {

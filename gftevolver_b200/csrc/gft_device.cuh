@@ -69,6 +69,10 @@ struct StepParams {
     double gsq_hf;          // g''^2 of the Higgs-family equations (TwoHDM.cpp:258-267)
     double inv_gpp_sqr;     // 1/g''^2 (0 below the division tolerance)
     double div_tol;         // divisionByZeroTolerance of the generator conversions
+    float* loc_energy;      // non-null on a local-output step: per-site densities [N][6] (energy, potential,
+                            // gradient, kinetic, magnetic, electric; Analysers/Source/Energy.cpp:117-163)
+    float* loc_gauss;       // non-null on a local-output step: per-site signed violations [N][gaugeNum]
+                            // (Analysers/Source/GaugeCondition.cpp:117-140)
     double damping_step;    // 0.5 * damping * dt for this step
     // SO_N
     double lambda, eta_sqr;

@@ -523,6 +523,15 @@ __global__ void __launch_bounds__(128) ref_step_kernel(StepParams P, LevelPtrs<S
             obs[kObsKinetic] = (double)ke;
             obs[kObsMagnetic] = (double)mag_e;
             obs[kObsElectric] = (double)ee;
+            if (P.loc_energy && counts(P, x)) {  // Energy's local densities (Analysers/Source/Energy.cpp:137-143)
+                float* o = P.loc_energy + 6 * (size_t)n.c;
+                o[0] = (float)tot;
+                o[1] = (float)pe;
+                o[2] = (float)grad_e;
+                o[3] = (float)ke;
+                o[4] = (float)mag_e;
+                o[5] = (float)ee;
+            }
             obs[kObsPlaqSU2] = plaq2;
             obs[kObsPlaqU1] = plaq1;
             double fs = 0.0;
@@ -699,6 +708,7 @@ __global__ void __launch_bounds__(128) ref_gauss_kernel(StepParams P, LevelPtrs<
             const double av = (double)(viol < (S)0 ? -viol : viol);
             v[k] = av;
             v[NEQ + k] = av;
+            if (P.loc_gauss) P.loc_gauss[(size_t)NEQ * n.c + k] = (float)viol;  // GaugeCondition local violation
         }
     }
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);

@@ -635,6 +635,15 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     if (ENERGY) {
         const double ge = (double)grad_e, ke = 0.5 * P.inv_sqr_dt * (double)kin_e;
         const double me = (double)mag_e, ee = (double)elec_e;
+        if (P.loc_energy) {  // Energy's local densities (Analysers/Source/Energy.cpp:137-143)
+            float* o = P.loc_energy + 6 * (size_t)ps.s;
+            o[0] = (float)(pot_e + ge + ke + me + ee);
+            o[1] = (float)pot_e;
+            o[2] = (float)ge;
+            o[3] = (float)ke;
+            o[4] = (float)me;
+            o[5] = (float)ee;
+        }
         obs[kObsPotential] += pot_e;
         obs[kObsGradient] += ge;
         obs[kObsKinetic] += ke;
@@ -666,7 +675,8 @@ __device__ __forceinline__ GLink gauss_link(const LV& now, const LV& fut, int d,
 
 // The residuals from the links at x (own[d]) and at x - e_d (back[d]) and the
 // doublets at x (site c).
-template <class S, int MODEL, class LV>
+// NEQ_ALL: the local-violation stride (gaugeNum; the Higgs-family constraints follow)
+template <class S, int MODEL, class LV, int NEQ_ALL = 4>
 __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&own)[3], const GLink (&back)[3],
                                            const LV& now, const LV& fut, int c,
                                            double (&v)[kGaussSlots])
@@ -698,9 +708,11 @@ __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&ow
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const double av = fabs(el[k] - P.gsq[k] * gr[k]);
+        const double viol = el[k] - P.gsq[k] * gr[k];
+        const double av = fabs(viol);
         v[k] = av;
         v[4 + k] = av;
+        if (P.loc_gauss) P.loc_gauss[(size_t)NEQ_ALL * c + k] = (float)viol;  // GaugeCondition local violation
     }
 }
 
@@ -718,7 +730,7 @@ __device__ __forceinline__ void gauss_site(const StepParams& P, const LV& now, c
     } else {
         constexpr int NEQ = hf_neq(HF);
         double vs[kGaussSlots];
-        gauss_core<S, MODEL>(P, own, back, now, fut, c, vs);
+        gauss_core<S, MODEL, LV, NEQ>(P, own, back, now, fut, c, vs);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             v[k] = vs[k];
@@ -758,9 +770,11 @@ __device__ __forceinline__ void gauss_site(const StepParams& P, const LV& now, c
         }
 #pragma unroll
         for (int k = 0; k < NEQ - 4; k++) {
-            const double av = fabs(el[k] - P.gsq_hf * gr[k]);
+            const double viol = el[k] - P.gsq_hf * gr[k];
+            const double av = fabs(viol);
             v[4 + k] = av;
             v[NEQ + 4 + k] = av;
+            if (P.loc_gauss) P.loc_gauss[(size_t)NEQ * c + 4 + k] = (float)viol;
         }
     }
 }

@@ -70,6 +70,8 @@ class LatticeParams:
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (frozen shell), else periodic
     higgs_family: int = 0      # 2HDM Higgs-family gauge field: 0 none, 1 U(1) (gaugeNum 5), 2 SU(2) (gaugeNum 7)
     generator_rep: int = 0     # host links as 3 generators w (U = exp(i w.sigma)) instead of quaternions
+    energy_local_every: int = 0  # Energy local densities kept every n steps (gft_local_fields); 0 = none
+    gauss_local_every: int = 0   # GaugeCondition local violations kept every n steps; 0 = none
 
     @property
     def nsc(self) -> int:
@@ -298,6 +300,19 @@ class Evolver:
     def launch_count(self) -> int:
         """Kernels launched by evolve() on this handle so far."""
         return int(self.lib.gft_launch_count(self.h))
+
+    def local_fields(self):
+        """Per-site analyser outputs of the latest local-output step: (energy[nsite, 6] or None,
+        step, gauss[nsite, gaugeNum] or None, step); see gft_local_fields."""
+        p = self.params
+        fp = ctypes.POINTER(ctypes.c_float)
+        e = np.zeros((p.nsite, 6), np.float32) if p.energy_local_every > 0 else None
+        g = np.zeros((p.nsite, p.neq), np.float32) if p.gauss_local_every > 0 else None
+        es, gs = ctypes.c_int(-1), ctypes.c_int(-1)
+        _lib.check(self.lib.gft_local_fields(self.h, e.ctypes.data_as(fp) if e is not None else None,
+                                             g.ctypes.data_as(fp) if g is not None else None, ctypes.byref(es),
+                                             ctypes.byref(gs)), self.h)
+        return e, es.value, g, gs.value
 
     @property
     def step_kernel_name(self) -> str:

@@ -88,6 +88,10 @@ struct Analysers {
     bool energy_opt[6] = {};
     bool gauss_opt[2] = {};
     int energy_freq = 1, gauss_freq = 1;
+    // local (per-site) outputs: Energy's six densities, GaugeCondition's violations
+    bool energy_local_opt[6] = {};
+    bool gauss_local = false;
+    std::string energy_local_path, gauss_local_path;
     bool fields_both = false, fields_initial = false, fields_final = false, fields_continual = false;
     int fields_freq = 1;
     std::string fields_initial_path, fields_continual_path, fields_final_path;
@@ -248,9 +252,11 @@ Run configure(const std::string& root)
         bool any = false;
         for (int k = 0; k < 6; k++) any |= (r.an.energy_opt[k] = inum(E, 1 + k, 0, ef) != 0);
         r.an.energy_freq = inum(E, 7, 0, ef);
-        for (int k = 0; k < 6; k++)
-            if (inum(E, 9 + k, 0, ef)) std::cerr << "gft_run: local energy densities are not written by the GPU path\n";
+        r.an.energy_local_path = tok(E, 8, 0, ef);
+        bool any_local = false;
+        for (int k = 0; k < 6; k++) any_local |= (r.an.energy_local_opt[k] = inum(E, 9 + k, 0, ef) != 0);
         c.energy_every = any ? r.an.energy_freq : 0;
+        c.energy_local_every = any_local ? inum(E, 15, 0, ef) : 0;
     }
     if (r.an.gauss) {
         const std::string gf = root + "/Analysers/Config/GaugeCondition.cfg";
@@ -259,8 +265,10 @@ Run configure(const std::string& root)
         r.an.gauss_opt[0] = inum(G, 1, 0, gf) != 0;
         r.an.gauss_opt[1] = inum(G, 2, 0, gf) != 0;
         r.an.gauss_freq = inum(G, 3, 0, gf);
-        if (inum(G, 5, 0, gf)) std::cerr << "gft_run: local Gauss violations are not written by the GPU path\n";
+        r.an.gauss_local_path = tok(G, 4, 0, gf);
+        r.an.gauss_local = inum(G, 5, 0, gf) != 0;
         c.gauss_every = (r.an.gauss_opt[0] || r.an.gauss_opt[1]) ? r.an.gauss_freq : 0;
+        c.gauss_local_every = r.an.gauss_local ? inum(G, 6, 0, gf) : 0;
     }
     if (r.an.fields) {
         const std::string of = root + "/Analysers/Config/OutputFields.cfg";
@@ -450,9 +458,9 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
     }
     const std::string data = root + "/Data";
     mkdir(data.c_str(), 0755);
-    if (!r.an.fields_continual_path.empty()) {
-        const auto slash = r.an.fields_continual_path.rfind('/');
-        if (slash != std::string::npos) mkdir((data + "/" + r.an.fields_continual_path.substr(0, slash)).c_str(), 0755);
+    for (const std::string* sub : {&r.an.fields_continual_path, &r.an.energy_local_path, &r.an.gauss_local_path}) {
+        const auto slash = sub->rfind('/');
+        if (slash != std::string::npos) mkdir((data + "/" + sub->substr(0, slash)).c_str(), 0755);
     }
 
     gft_handle* h = nullptr;
@@ -489,12 +497,22 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
     if (r.an.fields && r.an.fields_initial)
         writer.submit(data + "/" + r.an.fields_initial_path, sc, ve, nsc, 0, r.an.fields_both);
 
-    // evolve: chunks end where OutputFields writes a continual dump
-    const int chunk_max = (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0) ? r.an.fields_freq : 1000;
-    std::vector<gft_observables> rows(chunk_max + 1);
+    // evolve: chunks end where OutputFields writes a continual dump or an analyser keeps its local outputs
+    const int ffreq = (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0) ? r.an.fields_freq : 0;
+    const int lef = c.energy_local_every, lgf = c.gauss_local_every, neq = gauss_count(c);
+    auto next_stop = [&](int d) {  // steps done at the end of the chunk that starts with d done
+        int stop = std::min(r.nt, d + 1000);
+        if (ffreq > 0) stop = std::min(stop, (d / ffreq + 1) * ffreq);
+        for (int f : {lef, lgf})
+            if (f > 0) stop = std::min(stop, (d + f - 1) / f * f + 1);  // after the next local-output step
+        return stop;
+    };
+    std::vector<gft_observables> rows;
+    std::vector<float> loc_e(lef > 0 ? nsite * 6 : 0), loc_g(lgf > 0 ? nsite * (size_t)neq : 0);
     int done = 0;
     while (done < r.nt) {
-        const int n = std::min(chunk_max - done % chunk_max, r.nt - done);
+        const int n = next_stop(done) - done;
+        rows.resize((size_t)n + 1);
         int got = 0;
         check(gft_evolve(h, n, rows.data(), (int)rows.size(), &got), h, "gft_evolve");
         done += n;
@@ -510,13 +528,32 @@ int run(const std::string& root, Run& r, const std::string& ic_path, long long s
             if (o.has_gauss && !r.an.gauss_path.empty()) {
                 std::ofstream ofs(data + "/" + r.an.gauss_path, std::ios::app);
                 if (r.an.gauss_opt[0])
-                    for (int k = 0; k < gauss_count(c); k++) ofs << o.gauss_int[k] << " ";
+                    for (int k = 0; k < neq; k++) ofs << o.gauss_int[k] << " ";
                 if (r.an.gauss_opt[1])
-                    for (int k = 0; k < gauss_count(c); k++) ofs << o.gauss_max[k] << " ";
+                    for (int k = 0; k < neq; k++) ofs << o.gauss_max[k] << " ";
                 ofs << "\n";
             }
         }
-        if (r.an.fields && r.an.fields_continual && r.an.fields_freq > 0 && done % r.an.fields_freq == 0) {
+        // local outputs of step done - 1 (Energy.cpp:191-207: option-major, one value per line;
+        // GaugeCondition.cpp:194-212: site-major, gaugeNum values per site)
+        const int last = done - 1;
+        const bool le = lef > 0 && last % lef == 0, lg = lgf > 0 && last % lgf == 0;
+        if (le || lg) {
+            int es = -1, gs = -1;
+            check(gft_local_fields(h, le ? loc_e.data() : nullptr, lg ? loc_g.data() : nullptr, &es, &gs), h,
+                  "gft_local_fields");
+            if (le) {
+                std::ofstream ofs(data + "/" + r.an.energy_local_path + "_" + std::to_string(last) + ".dat");
+                for (int k = 0; k < 6; k++)
+                    if (r.an.energy_local_opt[k])
+                        for (size_t s = 0; s < nsite; s++) ofs << loc_e[s * 6 + k] << "\n";
+            }
+            if (lg) {
+                std::ofstream ofs(data + "/" + r.an.gauss_local_path + "_" + std::to_string(last) + ".dat");
+                for (size_t k = 0; k < loc_g.size(); k++) ofs << loc_g[k] << "\n";
+            }
+        }
+        if (ffreq > 0 && done % ffreq == 0) {
             download();
             writer.submit(data + "/" + r.an.fields_continual_path + "_" + std::to_string(done) + ".dat", sc, ve, nsc,
                           done, r.an.fields_both);
@@ -588,6 +625,7 @@ int main(int argc, char** argv)
             std::printf("energy_every %d gauss_every %d energy_path %s gauss_path %s fixed_axes %d\n", c.energy_every,
                         c.gauss_every, r.an.energy_path.c_str(), r.an.gauss_path.c_str(), c.fixed_axes);
             std::printf("higgs_family %d gpp %.17g generator_rep %d\n", c.higgs_family, c.gpp, c.generator_rep);
+            std::printf("energy_local_every %d gauss_local_every %d\n", c.energy_local_every, c.gauss_local_every);
             std::printf("ic_scalar %d ic_gauge %d ic_seed %u ic_min %.9g ic_max %.9g ic_equal %d\n", r.ic.type[0],
                         r.ic.type[1], r.ic.seed, r.ic.lo, r.ic.hi, (int)r.ic.equal);
             return 0;

@@ -102,6 +102,9 @@ typedef struct gft_config {
     int generator_rep;             /* 1: host vectors hold each SU(2) link as its 3 generators w,
                                       U = (cos|w|, sin|w| w/|w|) (WilsonLoops/Source/StandardModel.cpp:76-160):
                                       4 words per direction [theta_Y, w1, w2, w3] (+ theta_H or w'1..w'3) */
+    int energy_local_every;        /* Energy.cfg local-output frequency (0 = none): on those steps the
+                                      per-site densities are kept for gft_local_fields */
+    int gauss_local_every;         /* GaugeCondition.cfg local-output frequency (0 = none) */
 } gft_config;
 
 /* One row of global observables (Analysers/Source/Energy.cpp:169-220,
@@ -169,6 +172,17 @@ int gft_observe(gft_handle* h, gft_observables* row);
 
 /* Current reference step counter. */
 int gft_time_iter(const gft_handle* h);
+/* Per-site analyser outputs of the most recent local-output step (Energy's and
+ * GaugeCondition's local options, Analysers/Source/Energy.cpp:117-163, 191-207,
+ * Analysers/Source/GaugeCondition.cpp:117-140, 194-212): energy[nsite][6] =
+ * (energy, potential, gradient, kinetic, magnetic, electric) densities at
+ * step *energy_step (before its update), gauss[nsite][gaugeNum] = the signed
+ * constraint violations after step *gauss_step, sites in the reference's index
+ * order (x slowest), float as the reference stores them; sites on Fixed faces
+ * are 0.  Either buffer may be NULL; a step is -1 when none was computed yet.
+ * A local-output step also renormalises as an energy step does (the reference's
+ * storeEnergy covers both cadences). */
+int gft_local_fields(gft_handle* h, float* energy, float* gauss, int* energy_step, int* gauss_step);
 
 /* Device-resident access for callers that keep the state on the GPU:
  * the stream the handle launches on, and the number of device bytes it holds. */

@@ -796,10 +796,13 @@ static double damping_step(const ctx_t* m, int time_iter)
  * time_iter % every == 0 (the analysers' counters, Energy.cpp:212-219,
  * GaugeCondition.cpp:220-225, with the run starting at time_iter 0).
  * Returns the number of rows written (>= 0), or < 0 on error.  *warn receives
- * the OR of domain-warning bits (1: |RHS_Y| > 1, 2: |c|^2 > 1).
+ * the OR of domain-warning bits (1: |RHS_Y| > 1, 2: |c|^2 > 1).  loc_e [nsite][6] and
+ * loc_g [nsite][gaugeNum] (either may be NULL) receive the per-site densities and
+ * signed violations of the last local-output step in the run, rounded to float as
+ * the reference stores them; sites it does not visit are left untouched.
  */
 int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, int nsteps, orc_row* rows,
-               int max_rows, int* warn)
+               int max_rows, int* warn, double* loc_e, double* loc_g)
 {
     ctx_t m;
     if (ctx_init(&m, cfg) != 0) return -1;
@@ -814,7 +817,9 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
         int t_now = (time_iter + 1) % 2, t_past = 1 - t_now;
         int do_energy = cfg->energy_every > 0 && time_iter % cfg->energy_every == 0;
         int do_gauss = cfg->gauss_every > 0 && time_iter % cfg->gauss_every == 0;
-        m.store_energy = do_energy;
+        int local_e = cfg->energy_local_every > 0 && time_iter % cfg->energy_local_every == 0;
+        int local_g = cfg->gauss_local_every > 0 && time_iter % cfg->gauss_local_every == 0;
+        m.store_energy = do_energy || local_e;
         m.damping_step = damping_step(&m, time_iter);
 
         S* sc_now = scalars + (long long)t_now * N * nsc;
@@ -851,7 +856,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             calc_magnetic(&m, &st, Mg, &mag_e, &pl2, &pl1);
             calc_electric(&m, v_now, v_past, El, &elec_e);
 
-            if (do_energy) {
+            if (do_energy || local_e) {
                 S pe = potential_energy(&m, s_now);
                 S ge = gradient_energy(&m, &st);
                 S ke = kinetic_energy(&m, s_now, s_past);
@@ -859,6 +864,8 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
                 S ee = (S)(m.inv_sqr_dt * (double)elec_e);
                 S tot = pe + ge + ke + me + ee;
                 S dens[6] = {tot, pe, ge, ke, me, ee};
+                if (local_e && loc_e)
+                    for (int k = 0; k < 6; k++) loc_e[idx * 6 + k] = (double)(float)dens[k];
                 for (int k = 0; k < 6; k++) {
                     ref_sum[k] = ref_sum[k] + dens[k];
                     dsum[k] += (double)dens[k];
@@ -898,7 +905,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             row.phi_sq = phisq / ne;
         }
 
-        if (do_gauss) {
+        if (do_gauss || local_g) {
             /* post-evolve: the past slot now holds t + dt (Lattice.cpp:441-541) */
             S ref_int[ORC_MAX_EQ] = {0};
             double gint[ORC_MAX_EQ] = {0}, gmax[ORC_MAX_EQ] = {0};
@@ -921,6 +928,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
                 gradient_constraint(&m, sc_past + idx * nsc, sc_now + idx * nsc, gr);
                 for (int k = 0; k < neq; k++) {
                     S viol = el[k] - (S)m.gsq_coupling[k] * gr[k];
+                    if (local_g && loc_g) loc_g[idx * neq + k] = (double)(float)viol;
                     S v = viol < (S)0 ? -viol : viol;
                     ref_int[k] = ref_int[k] + v;
                     gint[k] += (double)v;
@@ -928,8 +936,8 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
                 }
             }
             double dv = cfg->dx * cfg->dy * cfg->dz;
-            row.has_gauss = 1;
-            for (int k = 0; k < neq; k++) {
+            row.has_gauss = do_gauss;
+            for (int k = 0; k < neq && do_gauss; k++) {
                 row.gauss_int[k] = gint[k] * dv;
                 row.gauss_max[k] = gmax[k];
                 row.ref_gauss_int[k] = (double)ref_int[k];

@@ -71,6 +71,10 @@ typedef struct orc_config {
      * (cos|w|, sin|w| w/|w|) (WilsonLoops/Source/StandardModel.cpp:76-160); 4 words per
      * direction [theta_Y, w1, w2, w3] (+ theta_H, or + w'1..w'3 for the Higgs family) */
     int generator_rep;
+    /* Energy / GaugeCondition local-output frequencies (0 = none): per-site densities and
+     * signed violations on those steps; the energy pass (storeEnergy) runs on the union of
+     * the global and local Energy cadences (Analysers/Source/Energy.cpp:212-219) */
+    int energy_local_every, gauss_local_every;
 } orc_config;
 
 /* One row of global observables, written on every step where an analyser logs.

@@ -55,6 +55,7 @@ class OrcConfig(ctypes.Structure):
         ("fixed_axes", ctypes.c_int),
         ("higgs_family", ctypes.c_int), ("gpp", ctypes.c_double),
         ("generator_rep", ctypes.c_int),
+        ("energy_local_every", ctypes.c_int), ("gauss_local_every", ctypes.c_int),
     ]
 
 
@@ -114,6 +115,8 @@ class Params:
     fixed_axes: int = 0        # bit a: both faces of axis a Fixed (else periodic)
     higgs_family: int = HF_NONE  # 2HDM Higgs-family gauge field (HF_*)
     generator_rep: int = 0     # links stored as 3 generators w (U = exp(i w.sigma)) instead of quaternions
+    energy_local_every: int = 0  # Energy local densities every n steps (0 = none)
+    gauss_local_every: int = 0   # GaugeCondition local violations every n steps (0 = none)
 
     @property
     def nsc(self) -> int:
@@ -182,7 +185,8 @@ def _load():
                 f = getattr(lib, p + "evolve")
                 f.restype = ctypes.c_int
                 f.argtypes = [ctypes.POINTER(OrcConfig), fp, fp, ctypes.c_int, ctypes.c_int,
-                              ctypes.POINTER(OrcRow), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+                              ctypes.POINTER(OrcRow), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
                 f = getattr(lib, p + "init_fields")
                 f.restype = None
                 f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -236,8 +240,11 @@ def init_fields(p: Params, ic: ICSpec, dtype=np.float32):
 ROW_KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric")
 
 
-def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, time_iter0: int = 0):
-    """Evolve in place; returns (rows, warn) with rows a list of dicts."""
+def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, time_iter0: int = 0,
+           local: bool = False):
+    """Evolve in place; returns (rows, warn) with rows a list of dicts, and with local=True
+    also the per-site outputs of the last local-output step: (rows, warn, energy[nsite, 6],
+    gauss[nsite, gaugeNum]) (zeros where no step computed them)."""
     lib = _load()
     assert scalars.flags.c_contiguous and vectors.flags.c_contiguous
     assert scalars.dtype == vectors.dtype
@@ -247,8 +254,12 @@ def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, tim
     rows = (OrcRow * max_rows)()
     warn = ctypes.c_int(0)
     cfg = p.to_c()
+    loc_e = np.zeros((p.nsite, 6), np.float64)
+    loc_g = np.zeros((p.nsite, p.neq), np.float64)
+    dp = ctypes.POINTER(ctypes.c_double)
     n = getattr(lib, _prefix(scalars.dtype) + "evolve")(
-        ctypes.byref(cfg), _ptr(scalars), _ptr(vectors), time_iter0, nsteps, rows, max_rows, ctypes.byref(warn))
+        ctypes.byref(cfg), _ptr(scalars), _ptr(vectors), time_iter0, nsteps, rows, max_rows, ctypes.byref(warn),
+        loc_e.ctypes.data_as(dp), loc_g.ctypes.data_as(dp))
     if n < 0:
         raise ValueError(f"oracle rejected the configuration (code {n})")
     out = []
@@ -262,4 +273,6 @@ def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, tim
         d["ref_energy"] = list(r.ref_energy)
         d["ref_gauss_int"] = list(r.ref_gauss_int)[: p.neq]
         out.append(d)
+    if local:
+        return out, warn.value, loc_e, loc_g
     return out, warn.value

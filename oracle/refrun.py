@@ -58,11 +58,12 @@ def _write(path: str, lines: list[str]) -> None:
 
 
 def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1),
-                  output_fields=None) -> None:
+                  output_fields=None, energy_local=(0, 1, 2, 3, 4, 5)) -> None:
     """ic_types: Lattice.cfg initial-condition types (0 zero / identity links, 1 RandomUniform);
     random_uniform: InitialConditions/Config/RandomUniform.cfg (seed, min, max, equal time levels);
     output_fields: None (OutputFields off) or (both levels, initial, final, continual, frequency)
-    for Analysers/Config/OutputFields.cfg."""
+    for Analysers/Config/OutputFields.cfg; energy_local: the Energy local options written when
+    p.energy_local_every > 0 (0 energy, 1 potential, 2 gradient, 3 kinetic, 4 magnetic, 5 electric)."""
     sm = p.model == orc.MODEL_SM
     # Core/Config/Lattice.cfg -- Lattice::configure (Lattice.cpp:47-143)
     lat = _header(10, "Lattice")
@@ -86,8 +87,8 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
         "",
         "analysis options",
         f"output fields                  : {0 if output_fields is None else 1}",
-        f"calculate energy               : {1 if p.energy_every > 0 else 0}",
-        f"calculate gauge condition      : {1 if p.gauss_every > 0 else 0}",
+        f"calculate energy               : {1 if p.energy_every > 0 or p.energy_local_every > 0 else 0}",
+        f"calculate gauge condition      : {1 if p.gauss_every > 0 or p.gauss_local_every > 0 else 0}",
         "",
         "boundary conditions",
         "six faces",
@@ -197,27 +198,31 @@ def write_configs(work: str, p: orc.Params, nt: int, ic_types=(0, 0), random_uni
     ef = max(p.energy_every, 1)
     en = _header(13, "Energy")
     en += ["global path                    : global_quantities.dat"]
-    en += [f"global option {k}                : 1" for k in range(6)]
+    en += [f"global option {k}                : {1 if p.energy_every > 0 else 0}" for k in range(6)]
+    el = max(p.energy_local_every, 1)
     en += [f"global frequency               : {ef}", "",
            "local path                     : Continual/local_quantities"]
-    en += [f"local option {k}                 : 0" for k in range(6)]
-    en += [f"local frequency                : {ef}"]
+    en += [f"local option {k}                 : {1 if p.energy_local_every > 0 and k in energy_local else 0}"
+           for k in range(6)]
+    en += [f"local frequency                : {el}"]
     _write(os.path.join(work, "Analysers", "Config", "Energy.cfg"), en)
 
     # Analysers/Config/GaugeCondition.cfg (GaugeCondition.cpp:14-47)
     gf = max(p.gauss_every, 1)
     ga = _header(13, "GaugeCondition")
     ga += ["global path                    : global_quantities_gauge.dat",
-           "integrated                     : 1", "maximum                        : 1",
+           f"integrated                     : {1 if p.gauss_every > 0 else 0}",
+           f"maximum                        : {1 if p.gauss_every > 0 else 0}",
            f"global frequency               : {gf}", "",
            "local path                     : Continual/local_quantities_gauge",
-           "local violation                : 0", f"local frequency                : {gf}"]
+           f"local violation                : {1 if p.gauss_local_every > 0 else 0}",
+           f"local frequency                : {max(p.gauss_local_every, 1)}"]
     _write(os.path.join(work, "Analysers", "Config", "GaugeCondition.cfg"), ga)
 
 
 def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, nt: int, fp64: bool = False,
         workdir: str | None = None, timeout: float = 600.0, ic_types=(0, 0), random_uniform=(42, -1.0, 1.0, 1),
-        output_fields=None):
+        output_fields=None, energy_local=(0, 1, 2, 3, 4, 5)):
     """Run the reference binary from the given two-level initial data, or (scalars
     None) from its own configured initial condition (ic_types, random_uniform).
 
@@ -235,7 +240,7 @@ def run(p: orc.Params, scalars: np.ndarray | None, vectors: np.ndarray | None, n
         scalars = np.zeros((2, p.nx, p.ny, p.nz, p.nsc), dtype)
         vectors = np.zeros((2, p.nx, p.ny, p.nz, p.nve), dtype)
     try:
-        write_configs(work, p, nt, ic_types, random_uniform, output_fields)
+        write_configs(work, p, nt, ic_types, random_uniform, output_fields, energy_local)
         icp = os.path.join(work, "ic.bin")
         if given:
             with open(icp, "wb") as f:

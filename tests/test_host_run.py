@@ -177,6 +177,41 @@ def test_initial_only_refuses_device_initial_data(tmp_path, oracle_mod, gft_run)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("model,hf", [(1, 0), (2, 2)])
+def test_local_analyser_files_match_the_reference(tmp_path, oracle_mod, gft_run, model, hf):
+    """Energy's and GaugeCondition's local files (Continual/local_quantities_<step>.dat: option-major
+    densities; Continual/local_quantities_gauge_<step>.dat: gaugeNum violations per site) of every
+    local-output step, against the reference run's own files."""
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("oracle/_ref/ref32 not built")
+    p = _params(oracle_mod, model, higgs_family=hf)
+    p.energy_local_every, p.gauss_local_every = 3, 2
+    ic = oracle_mod.ICSpec(seed=9, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
+                           eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(p, ic, np.float32)
+    ref_dir, gpu_dir = tmp_path / "ref", tmp_path / "gpu"
+    ref_dir.mkdir()
+    refrun.run(p, sc, ve, 7, workdir=str(ref_dir), energy_local=(0, 2, 5))
+    shutil.copytree(ref_dir, gpu_dir, ignore=shutil.ignore_patterns("Data", "final.bin", "rows.txt", "timing.txt"))
+    subprocess.run([gft_run, str(gpu_dir), "--form", "ref32", "--ic", str(gpu_dir / "ic.bin")], check=True,
+                   capture_output=True, text=True)
+    ref_files = sorted(os.listdir(ref_dir / "Data" / "Continual"))
+    assert ref_files == sorted(os.listdir(gpu_dir / "Data" / "Continual"))
+    assert "local_quantities_6.dat" in ref_files and "local_quantities_gauge_6.dat" in ref_files
+    for name in ref_files:
+        a = np.loadtxt(gpu_dir / "Data" / "Continual" / name)
+        b = np.loadtxt(ref_dir / "Data" / "Continual" / name)
+        assert a.shape == b.shape, name
+        np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-6 * max(np.abs(b).max(), 1e-3), err_msg=name)
+    for name in ("global_quantities.dat", "global_quantities_gauge.dat"):
+        a, b = _numbers(gpu_dir / "Data" / name), _numbers(ref_dir / "Data" / name)
+        assert len(a) == len(b)
+        for ra, rb in zip(a, b):
+            np.testing.assert_allclose(ra, rb, rtol=2e-5, atol=1e-12)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("both", [0, 1])
 def test_output_fields_dumps_match_the_reference(tmp_path, oracle_mod, gft_run, both):
     """OutputFields (Analysers/Source/OutputFields.cpp:63-200): the initial, every continual

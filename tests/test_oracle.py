@@ -83,6 +83,34 @@ def test_oracle_rejects_bad_config(oracle_mod):
         oracle_mod.evolve(p, sc, ve, 1)
 
 
+def test_local_outputs_match_the_reference(oracle_mod, tmp_path):
+    """Energy's local densities and GaugeCondition's local violations (Analysers/Source/Energy.cpp:117-163,
+    191-207; GaugeCondition.cpp:117-140, 194-212) against the reference's own files, and the fields bit
+    for bit: the energy pass (storeEnergy) runs on the union of the global and local Energy cadences."""
+    from oracle import refrun
+    if not refrun.available(False):
+        pytest.skip("reference binaries not built in this environment")
+    for model, hf, el, gl, ee, ge, fixed in ((1, 0, 3, 2, 2, 0, 2), (2, 2, 2, 3, 0, 4, 0)):
+        p = oracle_mod.Params(model=model, nx=4, ny=5, nz=3, energy_every=ee, gauss_every=ge, higgs_family=hf,
+                              gpp=0.5, energy_local_every=el, gauss_local_every=gl, fixed_axes=fixed)
+        ic = oracle_mod.ICSpec(seed=5, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+        sc, ve = oracle_mod.init_fields(p, ic, np.float32)
+        work = tmp_path / f"m{model}"
+        work.mkdir()
+        rsc, rve, _, _ = refrun.run(p, sc, ve, 7, workdir=str(work))
+        o_sc, o_ve = sc.copy(), ve.copy()
+        _, _, le, lg = oracle_mod.evolve(p, o_sc, o_ve, 7, local=True)
+        np.testing.assert_array_equal(o_sc, rsc)
+        np.testing.assert_array_equal(o_ve, rve)
+        last_e = max(t for t in range(7) if t % el == 0)
+        last_g = max(t for t in range(7) if t % gl == 0)
+        fe = np.loadtxt(work / "Data" / "Continual" / f"local_quantities_{last_e}.dat").reshape(6, -1).T
+        fg = np.loadtxt(work / "Data" / "Continual" / f"local_quantities_gauge_{last_g}.dat").reshape(-1, p.neq)
+        # the files print 6 significant digits
+        np.testing.assert_allclose(fe, le, rtol=1e-5, atol=1e-9)
+        np.testing.assert_allclose(fg, lg, rtol=1e-5, atol=1e-9)
+
+
 def test_live_reference_matches_oracle_when_built(oracle_mod):
     """If oracle/_ref was built here (the reference is mounted), compare live on a fresh random case."""
     from oracle import refrun
