@@ -22,7 +22,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, shape, model, nt, out_dir):
+def _worker(rank, world, port, shape, model, nt, out_dir, hf=0):
     import datetime
 
     import torch
@@ -36,7 +36,7 @@ def _worker(rank, world, port, shape, model, nt, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         nx, ny, nz = shape
-        op = orc.Params(model=model, nx=nx, ny=ny, nz=nz)
+        op = orc.Params(model=model, nx=nx, ny=ny, nz=nz, higgs_family=hf)
         ic = orc.ICSpec(seed=17, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                         eps_sigma=0.1)
         g_sc, g_ve = orc.init_fields(op, ic, np.float64)
@@ -45,7 +45,7 @@ def _worker(rank, world, port, shape, model, nt, out_dir):
         idx = [x % nx for x in range(x0 - 1, x1 + 1)]
         sc = np.ascontiguousarray(g_sc[:, idx])
         ve = np.ascontiguousarray(g_ve[:, idx])
-        lp = orc.Params(model=model, nx=nloc + 2, ny=ny, nz=nz)
+        lp = orc.Params(model=model, nx=nloc + 2, ny=ny, nz=nz, higgs_family=hf)
 
         def planes(level, x):
             return [torch.from_numpy(sc[level, x]), torch.from_numpy(ve[level, x])]
@@ -59,10 +59,12 @@ def _worker(rank, world, port, shape, model, nt, out_dir):
 
         # combine_rows: rank r contributes energy r+1, means (r+1)/10 over (r+1)*10 sites, max 2r
         own = (rank + 1) * 10
+        extra = [0.5, float(rank), 3.0][:op.neq - 4]  # Higgs-family constraints (gaugeNum 5 or 7)
         rows = [{"time_iter": 4, "has_energy": True, "has_gauss": True, "energy": rank + 1.0, "potential": 1.0,
                  "gradient": 0.0, "kinetic": 0.0, "magnetic": 0.0, "electric": 0.0,
                  "plaq_su2": (rank + 1) / 10.0, "plaq_u1": 1.0, "phi_sq": 2.0,
-                 "gauss_int": [1.0, 0.0, 0.0, float(rank)], "gauss_max": [2.0 * rank, 0.0, 1.0, 0.0]}]
+                 "gauss_int": [1.0, 0.0, 0.0, float(rank)] + extra,
+                 "gauss_max": [2.0 * rank, 0.0, 1.0, 0.0] + extra}]
         tot = combine_rows(rows, own)[0]
         np.savez(os.path.join(out_dir, f"rows{rank}.npz"), energy=tot["energy"], potential=tot["potential"],
                  plaq_su2=tot["plaq_su2"], plaq_u1=tot["plaq_u1"], gauss_int=tot["gauss_int"],
@@ -71,16 +73,17 @@ def _worker(rank, world, port, shape, model, nt, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,shape,model", [(2, (8, 4, 6), 1), (3, (7, 3, 5), 1), (2, (6, 4, 4), 2)])
-def test_slab_ranks_match_whole_lattice(tmp_path, oracle_mod, world, shape, model):
+@pytest.mark.parametrize("world,shape,model,hf", [(2, (8, 4, 6), 1, 0), (3, (7, 3, 5), 1, 0), (2, (6, 4, 4), 2, 0),
+                                                 (2, (6, 3, 4), 2, 2)])
+def test_slab_ranks_match_whole_lattice(tmp_path, oracle_mod, world, shape, model, hf):
     import torch.multiprocessing as mp
 
     nt = 5
     port = _free_port()
-    mp.start_processes(_worker, args=(world, port, shape, model, nt, str(tmp_path)), nprocs=world, join=True,
+    mp.start_processes(_worker, args=(world, port, shape, model, nt, str(tmp_path), hf), nprocs=world, join=True,
                        start_method="spawn")
     nx, ny, nz = shape
-    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz)
+    op = oracle_mod.Params(model=model, nx=nx, ny=ny, nz=nz, higgs_family=hf)
     ic = oracle_mod.ICSpec(seed=17, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                            eps_sigma=0.1)
     g_sc, g_ve = oracle_mod.init_fields(op, ic, np.float64)
@@ -100,8 +103,10 @@ def test_slab_ranks_match_whole_lattice(tmp_path, oracle_mod, world, shape, mode
         assert float(z["potential"]) == float(world)
         assert abs(float(z["plaq_su2"]) - sum(s * (i + 1) / 10.0 for i, s in enumerate(sites)) / sum(sites)) < 1e-15
         assert abs(float(z["plaq_u1"]) - 1.0) < 1e-15
-        assert list(z["gauss_int"]) == [float(world), 0.0, 0.0, float(sum(range(world)))]
-        assert list(z["gauss_max"]) == [2.0 * (world - 1), 0.0, 1.0, 0.0]
+        extra_sum = [0.5 * world, float(sum(range(world))), 3.0 * world][:op.neq - 4]
+        extra_max = [0.5, float(world - 1), 3.0][:op.neq - 4]
+        assert list(z["gauss_int"]) == [float(world), 0.0, 0.0, float(sum(range(world)))] + extra_sum
+        assert list(z["gauss_max"]) == [2.0 * (world - 1), 0.0, 1.0, 0.0] + extra_max
 
 
 def test_partition_covers_every_plane_once():
