@@ -57,6 +57,10 @@ struct EnsLevel {
 struct EnsParams {
     StepParams P[kGroup];
     EnsLevel lv[kGroup][2];
+    // Members with the same physics parameters (the usual ensemble: own seeds and
+    // sizes, shared couplings): their common StepParams, read as by-value kernel
+    // parameters (constant operands) instead of through the member index.
+    StepParams common;
 };
 static_assert(sizeof(EnsParams) <= 31 * 1024, "ensemble parameters exceed the kernel parameter space");
 
@@ -82,8 +86,9 @@ __device__ __forceinline__ void tmap_acquire(const TMaps& m)
 
 // One persistent launch per step: CTA b evolves tiles b, b + G, b + 2G, ...
 // items[i] = {member within the group, y0, z0, x0}; tile i's energy partials
-// go to partials row i.
-template <int MODEL, int TY, int TZ, bool ENERGY>
+// go to partials row i.  UNIFORM: the members share ep.common but for their
+// geometry (the per-member fields copied below).
+template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
     ensemble_step_kernel(const __grid_constant__ EnsParams ep, const EnsMaps* __restrict__ maps,
                          const int4* __restrict__ items, int nitems, int lx, int tn, unsigned* status,
@@ -118,7 +123,19 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
         double obs[kObsCount];
 #pragma unroll
         for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
-        const StepParams& P = ep.P[m];
+        StepParams Pu;
+        if constexpr (UNIFORM) {
+            Pu = ep.common;
+            const StepParams& Pm = ep.P[m];
+            Pu.nx = Pm.nx;
+            Pu.ny = Pm.ny;
+            Pu.nz = Pm.nz;
+            Pu.nsite = Pm.nsite;
+            Pu.obs_x0 = Pm.obs_x0;
+            Pu.obs_x1 = Pm.obs_x1;
+            Pu.fixed_axes = Pm.fixed_axes;
+        }
+        const StepParams& P = UNIFORM ? Pu : ep.P[m];
         const bool ok = run_tile<float, MODEL, TY, TZ, ENERGY>(mp.tm[tn], mp.tp[1 - tn], P, ep.lv[m][tn],
                                                                ep.lv[m][1 - tn], w.y, w.z, w.w, min(lx, P.nx - w.w),
                                                                smem, bars, ring, &s_abort, obs, warn);
@@ -181,14 +198,14 @@ __global__ void __launch_bounds__(kFinThreads) ensemble_finalize_kernel(const do
 
 // Resident CTAs per SM of a step-kernel instance (also sets its shared-memory
 // limit); evaluated outside any stream capture, by configure().
-template <int MODEL, int TY, int TZ, bool ENERGY>
+template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 int resident_ctas()
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<float, TY, TZ, ND>;
     static int per_sm = 0;
     if (per_sm == 0) {
-        auto k = ensemble_step_kernel<MODEL, TY, TZ, ENERGY>;
+        auto k = ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         int n = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, TY * TZ, G::SMEM) != cudaSuccess || n < 1) n = 1;
@@ -197,27 +214,45 @@ int resident_ctas()
     return per_sm;
 }
 
-template <int MODEL, int TY, int TZ, bool ENERGY>
-cudaError_t launch_step_t(const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems, int lx, int tn,
+template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
+cudaError_t launch_step_u(const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems, int lx, int tn,
                           unsigned* status, double* partials, int nsm, cudaStream_t s)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<float, TY, TZ, ND>;
-    const int grid = std::min(nitems, nsm * resident_ctas<MODEL, TY, TZ, ENERGY>());
+    const int grid = std::min(nitems, nsm * resident_ctas<MODEL, TY, TZ, ENERGY, UNIFORM>());
     if (grid < 1) return cudaSuccess;
-    ensemble_step_kernel<MODEL, TY, TZ, ENERGY><<<grid, dim3(TZ, TY, 1), G::SMEM, s>>>(ep, maps, items, nitems, lx,
-                                                                                        tn, status, partials);
+    ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM>
+        <<<grid, dim3(TZ, TY, 1), G::SMEM, s>>>(ep, maps, items, nitems, lx, tn, status, partials);
     return cudaGetLastError();
+}
+
+template <int MODEL, int TY, int TZ, bool ENERGY>
+cudaError_t launch_step_t(bool uniform, const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems,
+                          int lx, int tn, unsigned* status, double* partials, int nsm, cudaStream_t s)
+{
+    return uniform ? launch_step_u<MODEL, TY, TZ, ENERGY, true>(ep, maps, items, nitems, lx, tn, status, partials, nsm, s)
+                   : launch_step_u<MODEL, TY, TZ, ENERGY, false>(ep, maps, items, nitems, lx, tn, status, partials, nsm,
+                                                                 s);
+}
+
+template <int MODEL, int TY, int TZ>
+void prime_tile()
+{
+    resident_ctas<MODEL, TY, TZ, false, false>();
+    resident_ctas<MODEL, TY, TZ, true, false>();
+    resident_ctas<MODEL, TY, TZ, false, true>();
+    resident_ctas<MODEL, TY, TZ, true, true>();
 }
 
 template <int MODEL>
 void prime_variant(int variant)
 {
     switch (variant) {
-    case 0: resident_ctas<MODEL, 8, 32, false>(); resident_ctas<MODEL, 8, 32, true>(); break;
-    case 1: resident_ctas<MODEL, 4, 32, false>(); resident_ctas<MODEL, 4, 32, true>(); break;
-    case 2: resident_ctas<MODEL, 4, 16, false>(); resident_ctas<MODEL, 4, 16, true>(); break;
-    default: resident_ctas<MODEL, 16, 16, false>(); resident_ctas<MODEL, 16, 16, true>(); break;
+    case 0: prime_tile<MODEL, 8, 32>(); break;
+    case 1: prime_tile<MODEL, 4, 32>(); break;
+    case 2: prime_tile<MODEL, 4, 16>(); break;
+    default: prime_tile<MODEL, 16, 16>(); break;
     }
 }
 
@@ -231,12 +266,15 @@ cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, i
 }
 
 template <int MODEL>
-cudaError_t launch_step_m(int variant, bool energy, const EnsParams& ep, const EnsMaps* maps, const int4* items,
-                          int nitems, int lx, int tn, unsigned* status, double* partials, int nsm, cudaStream_t s)
+cudaError_t launch_step_m(int variant, bool energy, bool uniform, const EnsParams& ep, const EnsMaps* maps,
+                          const int4* items, int nitems, int lx, int tn, unsigned* status, double* partials, int nsm,
+                          cudaStream_t s)
 {
-#define GFT_ENS_STEP(TY, TZ)                                                                                       \
-    return energy ? launch_step_t<MODEL, TY, TZ, true>(ep, maps, items, nitems, lx, tn, status, partials, nsm, s)  \
-                  : launch_step_t<MODEL, TY, TZ, false>(ep, maps, items, nitems, lx, tn, status, partials, nsm, s)
+#define GFT_ENS_STEP(TY, TZ)                                                                                         \
+    return energy ? launch_step_t<MODEL, TY, TZ, true>(uniform, ep, maps, items, nitems, lx, tn, status, partials,  \
+                                                       nsm, s)                                                       \
+                  : launch_step_t<MODEL, TY, TZ, false>(uniform, ep, maps, items, nitems, lx, tn, status, partials, \
+                                                        nsm, s)
     switch (variant) {
     case 0: GFT_ENS_STEP(8, 32);
     case 1: GFT_ENS_STEP(4, 32);
@@ -343,17 +381,46 @@ void drop_graph(gft_batch* b)
     b->graph_period = 0;
 }
 
-EnsParams* fill_params(const gft_batch* b, int g, int ti, bool energy, EnsParams* ep)
+// Every StepParams field except the geometry ones (nx, ny, nz, nsite, obs_x0,
+// obs_x1, fixed_axes) equal, compared field by field (the struct has padding).
+bool same_physics(const StepParams& a, const StepParams& b)
+{
+    auto eq = [](const double* x, const double* y, int n) {
+        for (int k = 0; k < n; k++)
+            if (std::memcmp(&x[k], &y[k], sizeof(double)) != 0) return false;
+        return true;
+    };
+    const double da[] = {a.dt, a.dt2, a.inv_sqr_dt, a.inv_g_sqr, a.inv_gp_sqr, a.gsq_hf, a.inv_gpp_sqr, a.div_tol,
+                         a.damping_step, a.lambda, a.eta_sqr, a.m1, a.m2, a.l1, a.l2, a.l3, a.m12r, a.l4p5, a.l6r,
+                         a.l7r, a.m12i, a.l4m5, a.l5i, a.l6i, a.l7i, a.energy_offset};
+    const double db[] = {b.dt, b.dt2, b.inv_sqr_dt, b.inv_g_sqr, b.inv_gp_sqr, b.gsq_hf, b.inv_gpp_sqr, b.div_tol,
+                         b.damping_step, b.lambda, b.eta_sqr, b.m1, b.m2, b.l1, b.l2, b.l3, b.m12r, b.l4p5, b.l6r,
+                         b.l7r, b.m12i, b.l4m5, b.l5i, b.l6i, b.l7i, b.energy_offset};
+    return eq(da, db, (int)(sizeof(da) / sizeof(double))) && eq(a.lap, b.lap, 3) && eq(a.inv_dx, b.inv_dx, 3) &&
+           eq(a.gsq, b.gsq, 4) && a.hf == b.hf && a.gen == b.gen && a.loc_energy == b.loc_energy &&
+           a.loc_gauss == b.loc_gauss && a.break_son == b.break_son && a.break_uhalfn == b.break_uhalfn &&
+           a.apply_norm == b.apply_norm && a.store_energy == b.store_energy;
+}
+
+// Fills the group's parameters; returns whether its members share everything
+// but their geometry (then ep->common holds member 0's values, whose geometry
+// fields the kernel replaces by each member's).
+bool fill_params(const gft_batch* b, int g, int ti, bool energy, EnsParams* ep)
 {
     std::memset(ep, 0, sizeof(*ep));
+    bool uniform = true;
     for (int j = 0; j < kGroup; j++) {
         const int m = g * kGroup + j;
         if (m >= b->n) break;
         ep->P[j] = config_params(b->cfg[m], b->nsite[m], false, ti, energy);
         ep->lv[j][0] = b->lv[m][0];
         ep->lv[j][1] = b->lv[m][1];
+        if (j == 0)
+            ep->common = ep->P[0];
+        else if (!same_physics(ep->P[j], ep->common))
+            uniform = false;
     }
-    return ep;
+    return uniform;
 }
 
 // Tile list, tensor maps and partial buffers for a tile shape and march depth.
@@ -420,14 +487,14 @@ cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long 
     static thread_local EnsParams ep;
     cudaError_t err = cudaSuccess;
     for (int gr = 0; gr < b->ngroups() && err == cudaSuccess; gr++) {
-        fill_params(b, gr, ti, e, &ep);
+        const bool uniform = fill_params(b, gr, ti, e, &ep);
         const int i0 = b->group_item[gr], ni = b->group_item[gr + 1] - i0;
         const EnsMaps* maps = b->d_maps + (size_t)gr * kGroup;
         err = (b->model == GFT_MODEL_SM)
-                  ? launch_step_m<kModelSM>(b->variant, e, ep, maps, b->d_items + i0, ni, b->lx, tn, b->d_status,
-                                            b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream)
-                  : launch_step_m<kModel2HDM>(b->variant, e, ep, maps, b->d_items + i0, ni, b->lx, tn, b->d_status,
-                                              b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream);
+                  ? launch_step_m<kModelSM>(b->variant, e, uniform, ep, maps, b->d_items + i0, ni, b->lx, tn,
+                                            b->d_status, b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream)
+                  : launch_step_m<kModel2HDM>(b->variant, e, uniform, ep, maps, b->d_items + i0, ni, b->lx, tn,
+                                              b->d_status, b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream);
         (*nlaunch)++;
     }
     if (err == cudaSuccess && e) {
