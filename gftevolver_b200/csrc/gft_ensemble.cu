@@ -58,9 +58,11 @@ struct EnsParams {
     StepParams P[kGroup];
     EnsLevel lv[kGroup][2];
     // Members with the same physics parameters (the usual ensemble: own seeds and
-    // sizes, shared couplings): their common StepParams, read as by-value kernel
-    // parameters (constant operands) instead of through the member index.
+    // sizes, shared couplings): their common StepParams and float constants, read
+    // as by-value kernel parameters (constant operands) instead of through the
+    // member index.
     StepParams common;
+    FConst fcommon;
 };
 static_assert(sizeof(EnsParams) <= 31 * 1024, "ensemble parameters exceed the kernel parameter space");
 
@@ -136,7 +138,10 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
             Pu.fixed_axes = Pm.fixed_axes;
         }
         const StepParams& P = UNIFORM ? Pu : ep.P[m];
-        const bool ok = run_tile<float, MODEL, TY, TZ, ENERGY>(mp.tm[tn], mp.tp[1 - tn], P, ep.lv[m][tn],
+        FConst Fm;
+        if constexpr (!UNIFORM) Fm = make_fconst(P);
+        const FConst& F = UNIFORM ? ep.fcommon : Fm;
+        const bool ok = run_tile<float, MODEL, TY, TZ, ENERGY>(mp.tm[tn], mp.tp[1 - tn], P, F, ep.lv[m][tn],
                                                                ep.lv[m][1 - tn], w.y, w.z, w.w, min(lx, P.nx - w.w),
                                                                smem, bars, ring, &s_abort, obs, warn);
         if (!ok) {
@@ -415,8 +420,10 @@ bool fill_params(const gft_batch* b, int g, int ti, bool energy, EnsParams* ep)
         ep->P[j] = config_params(b->cfg[m], b->nsite[m], false, ti, energy);
         ep->lv[j][0] = b->lv[m][0];
         ep->lv[j][1] = b->lv[m][1];
-        if (j == 0)
+        if (j == 0) {
             ep->common = ep->P[0];
+            ep->fcommon = make_fconst(ep->P[0]);
+        }
         else if (!same_physics(ep->P[j], ep->common))
             uniform = false;
     }

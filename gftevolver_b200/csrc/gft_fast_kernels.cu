@@ -44,7 +44,7 @@ struct GlobalAcc {
 };
 
 template <class S, int MODEL, int HF, bool ENERGY>
-__global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> past,
+__global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, FConst F, LevelPtrs<S> now, LevelPtrs<S> past,
                                                         unsigned* status, double* partials)
 {
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, LevelPtrs<
         n.d21 = o.c + o.p[2] + o.m[1];
         XCarry<S, (MODEL == kModelSM) ? 1 : 2> carry;
         carry.valid = false;
-        site_step<S, MODEL, ENERGY, HF>(P, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn,
+        site_step<S, MODEL, ENERGY, HF>(P, F, GlobalAcc<S>{now}, n, PastSite<S>{past, o.c}, carry, obs, warn,
                                         counts(P, x));
     }
     if (ENERGY) {
@@ -111,9 +111,9 @@ void fast_step_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelP
     const dim3 block(32, 4, 1);
     const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
     if (energy)
-        fast_step_kernel<S, MODEL, HF, true><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+        fast_step_kernel<S, MODEL, HF, true><<<grid, block, 0, stream>>>(P, make_fconst(P), now, past, status, partials);
     else
-        fast_step_kernel<S, MODEL, HF, false><<<grid, block, 0, stream>>>(P, now, past, status, partials);
+        fast_step_kernel<S, MODEL, HF, false><<<grid, block, 0, stream>>>(P, make_fconst(P), now, past, status, partials);
 }
 
 template <class S, int MODEL, int HF>

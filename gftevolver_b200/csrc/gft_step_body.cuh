@@ -32,6 +32,15 @@
 namespace gft {
 
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+// A parameter in the compute type: the precomputed float copy, or the double.
+template <class C>
+__device__ __forceinline__ C pf(float f, double d)
+{
+    if constexpr (sizeof(C) == 4)
+        return f;
+    else
+        return d;
+}
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 
 // Doublet phi rotated by the hypercharge phase (cos, sin) then acted on by the
@@ -161,7 +170,8 @@ struct PastSite {
 // when `count` (the site is not on a ghost plane).  With HF != 0 the x-carry is
 // not used (the caller passes an invalid one).
 template <class S, int MODEL, bool ENERGY, int HF = kHfNone, class A, class R, class LV>
-__device__ __forceinline__ void site_step(const StepParams& P, const A& acc, const Stencil<R>& n, PastSite<S, LV> ps,
+__device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, const A& acc, const Stencil<R>& n,
+                                          PastSite<S, LV> ps,
                                           XCarry<S, (MODEL == kModelSM) ? 1 : 2>& carry, double (&obs)[kObsCount],
                                           unsigned& warn, bool count = true)
 {
@@ -183,7 +193,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
         }
     }
     const bool have = carry.valid;
-    const C lap[3] = {(C)P.lap[0], (C)P.lap[1], (C)P.lap[2]};
+    const C lap[3] = {pf<C>(F.lap[0], P.lap[0]), pf<C>(F.lap[1], P.lap[1]), pf<C>(F.lap[2], P.lap[2])};
 
     Q<C> U[3];
     C th[3];
@@ -346,7 +356,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     Q<C> D[ND];
 #pragma unroll
     for (int db = 0; db < ND; db++) {
-        const C w = (C)(-2.0 * (P.lap[0] + P.lap[1] + P.lap[2]));
+        const C w = pf<C>(F.diag, -2.0 * (P.lap[0] + P.lap[1] + P.lap[2]));
         D[db] = {w * fc[db].w, w * fc[db].x, w * fc[db].y, w * fc[db].z};
     }
     C J[3][4];
@@ -462,7 +472,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     double pot_e = 0.0;
     if (MODEL == kModelSM) {
         const C fsq = fc[0].w * fc[0].w + fc[0].x * fc[0].x + fc[0].y * fc[0].y + fc[0].z * fc[0].z;
-        const C k = (C)P.lambda * (fsq - (C)P.eta_sqr);
+        const C k = pf<C>(F.lambda, P.lambda) * (fsq - pf<C>(F.eta_sqr, P.eta_sqr));
         Pot[0][0] = k * fc[0].w;
         Pot[0][1] = k * fc[0].x;
         Pot[0][2] = k * fc[0].y;
@@ -521,8 +531,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
     //      phi(t+dt) = phi + [(phi - phi_past)(1 - damping) + dt^2 (D - dV)], one rounding at the end
     C kin_e = (C)0, phisq = (C)0;
     C check = (C)0;  // sum of every new value: non-finite iff one of them is
-    const C dt2 = (C)P.dt2;
-    const C keep = (C)(1.0 - P.damping_step);
+    const C dt2 = pf<C>(F.dt2, P.dt2);
+    const C keep = pf<C>(F.keep, 1.0 - P.damping_step);
 #pragma unroll
     for (int db = 0; db < ND; db++) {
         const Q<C> fpast = ENERGY ? ld4<C>(ps.L.ph[db], ps.s) : pst_f[db];
@@ -545,7 +555,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const A& acc, con
 
     // ---- link update (WilsonLoops/Source/StandardModel.cpp:456-514) ----
     C elec_e = (C)0;
-    const C gY = (C)P.gsq[0], gI = (C)P.gsq[1];
+    const C gY = pf<C>(F.gY, P.gsq[0]), gI = pf<C>(F.gI, P.gsq[1]);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const Q<C> Un = U[d];

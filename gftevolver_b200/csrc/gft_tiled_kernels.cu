@@ -18,7 +18,7 @@ using namespace tiled;
 template <class S, int MODEL, int TY, int TZ, bool ENERGY>
 __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(const __grid_constant__ TMaps maps,
                                                              const __grid_constant__ TMaps pmaps, StepParams P,
-                                                             LevelPtrs<S> now, LevelPtrs<S> past, int lx,
+                                                             FConst F, LevelPtrs<S> now, LevelPtrs<S> past, int lx,
                                                              unsigned* status, double* partials)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
     unsigned warn = 0;
     RingPhase ring = {0u};
     const int x0 = blockIdx.z * lx;
-    const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY>(maps, pmaps, P, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0,
+    const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY>(maps, pmaps, P, F, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0,
                                                        min(lx, P.nx - x0), smem, bars, ring, &s_abort, obs, warn);
     if (!ok && tid == 0) atomicOr(status, kErrTimeout);
 
@@ -144,11 +144,11 @@ static cudaError_t launch_tiled_t(const TMaps& maps, const TMaps& pmaps, const S
     if (energy) {
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, true>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, now, past, lx, status, partials);
+        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
     } else {
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, now, past, lx, status, partials);
+        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
     }
     return cudaGetLastError();
 }

@@ -269,7 +269,7 @@ struct RingPhase {
 // gave up; the ring is then drained and must not be reused.  LV: the level
 // pointer struct (its q / th / ph members are read).
 template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV>
-__device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+__device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const FConst& F,
                                          const LV& now, const LV& past, int y0, int z0, int x0,
                                          int nloc, unsigned char* smem, unsigned long long* bars, RingPhase& ring,
                                          int* s_abort, double (&obs)[kObsCount], unsigned& warn)
@@ -342,7 +342,7 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
             carry.valid = false;
         else
-            site_step<S, MODEL, ENERGY>(P, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs, warn,
+            site_step<S, MODEL, ENERGY>(P, F, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs, warn,
                                         counts(P, x));
 
         // plane i+3 (x+2) for the next site; its copy was issued one plane ago
