@@ -96,6 +96,10 @@ struct FConst {
     float dt2, keep;   // dt^2, 1 - damping_step
     float gY, gI;      // g'^2, g^2 as the couplings of the link equations
     float lambda, eta_sqr;
+    // Double_SO_N dV/dphi coefficients (Potentials/Source/Double_SO_N.cpp:244-341)
+    float m1x2n, l1x4, l3x2, m2x2n, l2x4;        // -2 m1, 4 l1, 2 l3, -2 m2, 4 l2
+    float m12rn, l4p5x2, l6r, l7r, l6rx2, l7rx2;  // -m12r, 2 l4p5, l6r, l7r, 2 l6r, 2 l7r
+    float m12i, l4m5x2, l5ix2, l6i, l7i, l6ix2, l7ix2;
 };
 
 __host__ __device__ inline FConst make_fconst(const StepParams& P)
@@ -109,6 +113,24 @@ __host__ __device__ inline FConst make_fconst(const StepParams& P)
     F.gI = (float)P.gsq[1];
     F.lambda = (float)P.lambda;
     F.eta_sqr = (float)P.eta_sqr;
+    F.m1x2n = (float)(-2.0 * P.m1);
+    F.l1x4 = (float)(4.0 * P.l1);
+    F.l3x2 = (float)(2.0 * P.l3);
+    F.m2x2n = (float)(-2.0 * P.m2);
+    F.l2x4 = (float)(4.0 * P.l2);
+    F.m12rn = (float)(-P.m12r);
+    F.l4p5x2 = (float)(2.0 * P.l4p5);
+    F.l6r = (float)P.l6r;
+    F.l7r = (float)P.l7r;
+    F.l6rx2 = (float)(2.0 * P.l6r);
+    F.l7rx2 = (float)(2.0 * P.l7r);
+    F.m12i = (float)P.m12i;
+    F.l4m5x2 = (float)(2.0 * P.l4m5);
+    F.l5ix2 = (float)(2.0 * P.l5i);
+    F.l6i = (float)P.l6i;
+    F.l7i = (float)P.l7i;
+    F.l6ix2 = (float)(2.0 * P.l6i);
+    F.l7ix2 = (float)(2.0 * P.l7i);
     return F;
 }
 

@@ -487,15 +487,19 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
         const C s2 = f2.w * f2.w + f2.x * f2.x + f2.y * f2.y + f2.z * f2.z;
         const C dot = P.break_son ? f1.w * f2.w + f1.x * f2.x + f1.y * f2.y + f1.z * f2.z : (C)0;
         const C anti = (P.break_son && P.break_uhalfn) ? f1.w * f2.x - f1.x * f2.w + f1.y * f2.z - f1.z * f2.y : (C)0;
-        const C a1 = (C)(-2.0 * P.m1) + (C)(4.0 * P.l1) * s1 + (C)(2.0 * P.l3) * s2;
-        const C a2 = (C)(-2.0 * P.m2) + (C)(4.0 * P.l2) * s2 + (C)(2.0 * P.l3) * s1;
+        const C l3x2 = pf<C>(F.l3x2, 2.0 * P.l3);
+        const C a1 = pf<C>(F.m1x2n, -2.0 * P.m1) + pf<C>(F.l1x4, 4.0 * P.l1) * s1 + l3x2 * s2;
+        const C a2 = pf<C>(F.m2x2n, -2.0 * P.m2) + pf<C>(F.l2x4, 4.0 * P.l2) * s2 + l3x2 * s1;
         // single SO(N): (-m12r + 2 l4p5 dot + l6r s1 + l7r s2) f_other + 2 l6r|l7r dot f_self
-        const C bs = (C)(-P.m12r) + (C)(2.0 * P.l4p5) * dot + (C)P.l6r * s1 + (C)P.l7r * s2;
-        const C b1 = (C)(2.0 * P.l6r) * dot, b2 = (C)(2.0 * P.l7r) * dot;
+        const C bs = pf<C>(F.m12rn, -P.m12r) + pf<C>(F.l4p5x2, 2.0 * P.l4p5) * dot + pf<C>(F.l6r, P.l6r) * s1 +
+                     pf<C>(F.l7r, P.l7r) * s2;
+        const C b1 = pf<C>(F.l6rx2, 2.0 * P.l6r) * dot, b2 = pf<C>(F.l7rx2, 2.0 * P.l7r) * dot;
         // U(N/2): (m12i + 2 l4m5 anti - 2 l5i dot - l6i s1 - l7i s2) J f_other - 2 l5i anti f_other - 2 l6i|l7i anti f_self
-        const C cu = (C)P.m12i + (C)(2.0 * P.l4m5) * anti - (C)(2.0 * P.l5i) * dot - (C)P.l6i * s1 - (C)P.l7i * s2;
-        const C c5 = (C)(2.0 * P.l5i) * anti;
-        const C c1 = (C)(2.0 * P.l6i) * anti, c2 = (C)(2.0 * P.l7i) * anti;
+        const C l5ix2 = pf<C>(F.l5ix2, 2.0 * P.l5i);
+        const C cu = pf<C>(F.m12i, P.m12i) + pf<C>(F.l4m5x2, 2.0 * P.l4m5) * anti - l5ix2 * dot -
+                     pf<C>(F.l6i, P.l6i) * s1 - pf<C>(F.l7i, P.l7i) * s2;
+        const C c5 = l5ix2 * anti;
+        const C c1 = pf<C>(F.l6ix2, 2.0 * P.l6i) * anti, c2 = pf<C>(F.l7ix2, 2.0 * P.l7i) * anti;
         const C f1v[4] = {f1.w, f1.x, f1.y, f1.z};
         const C f2v[4] = {f2.w, f2.x, f2.y, f2.z};
 #pragma unroll
