@@ -100,6 +100,11 @@ struct FConst {
     float m1x2n, l1x4, l3x2, m2x2n, l2x4;        // -2 m1, 4 l1, 2 l3, -2 m2, 4 l2
     float m12rn, l4p5x2, l6r, l7r, l6rx2, l7rx2;  // -m12r, 2 l4p5, l6r, l7r, 2 l6r, 2 l7r
     float m12i, l4m5x2, l5ix2, l6i, l7i, l6ix2, l7ix2;
+    // logging-step energy weights (the float values of the FP64 products they replace)
+    float e_plaq[3];   // 4 lap_i lap_j for the planes (0,1), (0,2), (1,2)
+    float e_grad[3];   // 0.5 / dx_a^2
+    float e_elec[3];   // 4 lap_d / dt^2
+    float inv_g_sqr, inv_gp_sqr, inv_gpp_sqr;
 };
 
 __host__ __device__ inline FConst make_fconst(const StepParams& P)
@@ -131,6 +136,15 @@ __host__ __device__ inline FConst make_fconst(const StepParams& P)
     F.l7i = (float)P.l7i;
     F.l6ix2 = (float)(2.0 * P.l6i);
     F.l7ix2 = (float)(2.0 * P.l7i);
+    const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+    for (int pl = 0; pl < 3; pl++) F.e_plaq[pl] = (float)(4.0 * P.lap[pi[pl]] * P.lap[pj[pl]]);
+    for (int a = 0; a < 3; a++) {
+        F.e_grad[a] = (float)(0.5 * P.inv_dx[a] * P.inv_dx[a]);
+        F.e_elec[a] = (float)(4.0 * P.lap[a] * P.inv_sqr_dt);
+    }
+    F.inv_g_sqr = (float)P.inv_g_sqr;
+    F.inv_gp_sqr = (float)P.inv_gp_sqr;
+    F.inv_gpp_sqr = (float)P.inv_gpp_sqr;
     return F;
 }
 

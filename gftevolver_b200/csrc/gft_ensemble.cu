@@ -64,7 +64,9 @@ struct EnsParams {
     StepParams common;
     FConst fcommon;
 };
-static_assert(sizeof(EnsParams) <= 31 * 1024, "ensemble parameters exceed the kernel parameter space");
+// Kernel parameter space (sm_70 and later, CUDA 12.1+): 32,764 bytes; the kernel's
+// other parameters take 48.
+static_assert(sizeof(EnsParams) + 64 <= 32764, "ensemble parameters exceed the kernel parameter space");
 
 // Tensor maps of one member (global memory, 64-byte aligned by CUtensorMap).
 struct EnsMaps {
@@ -148,7 +150,10 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
             if (tid == 0) atomicOr(status, kErrTimeout);
             break;
         }
-        if (ENERGY) block_reduce_store<kObsCount>(obs, partials + (size_t)it * kObsCount, kObsCount);
+        if (ENERGY) {
+            energy_total(obs);
+            block_reduce_store<kObsCount>(obs, partials + (size_t)it * kObsCount, kObsCount);
+        }
         __syncthreads();  // the reduction scratch and the plane ring are reused by the next tile
     }
     if (warn) atomicOr(status, warn);

@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(128) fast_step_kernel(StepParams P, FConst F, 
                                         counts(P, x));
     }
     if (ENERGY) {
+        energy_total(obs);
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         block_reduce_store<kObsCount>(obs, partials + (size_t)b * kObsCount, kObsCount);
     }

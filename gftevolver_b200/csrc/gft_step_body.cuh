@@ -164,11 +164,19 @@ struct PastSite {
     int s;
 };
 
+// A thread's total energy from its component sums, set once after its last site
+// (no per-site accumulator held through the update).
+__device__ __forceinline__ void energy_total(double (&obs)[kObsCount])
+{
+    obs[kObsEnergy] = obs[kObsPotential] + obs[kObsGradient] + obs[kObsKinetic] + obs[kObsMagnetic] + obs[kObsElectric];
+}
+
 // The per-site update.  A provides q(d, R) -> Q<C>, th(d, R) -> C, ph(k, R) -> Q<C>
 // for the "now" level (and hth / hq for a 2HDM Higgs-family field, HF != 0).
-// obs receives the energy-step observables and warn the warning bits, both only
-// when `count` (the site is not on a ghost plane).  With HF != 0 the x-carry is
-// not used (the caller passes an invalid one).
+// obs receives the energy-step observables except the total (energy_total after
+// the last site) and warn the warning bits, both only when `count` (the site is
+// not on a ghost plane).  With HF != 0 the x-carry is not used (the caller passes
+// an invalid one).
 template <class S, int MODEL, bool ENERGY, int HF = kHfNone, class A, class R, class LV>
 __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, const A& acc, const Stencil<R>& n,
                                           PastSite<S, LV> ps,
@@ -224,8 +232,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
         const Q<C> Ui_pj = acc.q(i, n.p[j]);
         // F_ij(x) = theta_i(x) + theta_j(x+i) - theta_i(x+j) - theta_j(x); the reference's
         // local angle is -F for link i and +F for link j (StandardModel.cpp:348-353).
-        const C F = th[i] + acc.th(j, n.p[i]) - acc.th(i, n.p[j]) - th[j];
-        const C sF = gsin(F);
+        const C Fa = th[i] + acc.th(j, n.p[i]) - acc.th(i, n.p[j]) - th[j];
+        const C sF = gsin(Fa);
         MgY[i] -= sF * lap[j];
         MgY[j] += sF * lap[i];
         if (pl == 0) carry.s01 = sF;
@@ -240,9 +248,10 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             // 1 - cos F = 2 sin^2(F/2) (no cancellation for small F)
             const Q<C> P1 = qmul(Aij, qconj(U[i]));
             const C omt = one_minus_trace(P1);
-            const C hF = gsin((C)0.5 * F);
+            const C hF = gsin((C)0.5 * Fa);
             const C omc = (C)2 * hF * hF;
-            mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * ((C)P.inv_g_sqr * omt + (C)P.inv_gp_sqr * omc);
+            mag_e += pf<C>(F.e_plaq[pl], 4.0 * P.lap[i] * P.lap[j]) *
+                     (pf<C>(F.inv_g_sqr, P.inv_g_sqr) * omt + pf<C>(F.inv_gp_sqr, P.inv_gp_sqr) * omc);
             plaq2 += (C)1 - omt;
             plaq1 += (C)1 - omc;
         }
@@ -280,13 +289,14 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
         for (int pl = 0; pl < 3; pl++) {
             const int i = (pl == 2) ? 1 : 0;
             const int j = (pl == 0) ? 1 : 2;
-            const C F = hc[i] + acc.hth(j, n.p[i]) - acc.hth(i, n.p[j]) - hc[j];
-            const C sF = gsin(F);
+            const C Fa = hc[i] + acc.hth(j, n.p[i]) - acc.hth(i, n.p[j]) - hc[j];
+            const C sF = gsin(Fa);
             MgH[i][0] -= sF * lap[j];
             MgH[j][0] += sF * lap[i];
             if (ENERGY) {
-                const C hF = gsin((C)0.5 * F);
-                mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * (C)P.inv_gpp_sqr * ((C)2 * hF * hF);
+                const C hF = gsin((C)0.5 * Fa);
+                mag_e += pf<C>(F.e_plaq[pl], 4.0 * P.lap[i] * P.lap[j]) * pf<C>(F.inv_gpp_sqr, P.inv_gpp_sqr) *
+                         ((C)2 * hF * hF);
             }
         }
 #pragma unroll
@@ -316,7 +326,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             SAH[i] = qadd_scaled(SAH[i], lap[j], Aij);
             SAH[j] = qadd_scaled(SAH[j], lap[i], Aji);
             if (ENERGY)
-                mag_e += (C)(4.0 * P.lap[i] * P.lap[j]) * (C)P.inv_gpp_sqr * one_minus_trace(qmul(Aij, qconj(UH[i])));
+                mag_e += pf<C>(F.e_plaq[pl], 4.0 * P.lap[i] * P.lap[j]) * pf<C>(F.inv_gpp_sqr, P.inv_gpp_sqr) *
+                         one_minus_trace(qmul(Aij, qconj(UH[i])));
         }
 #pragma unroll
         for (int i = 0; i < 3; i++) {
@@ -401,7 +412,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
                 j3 += u.w * f.x - u.x * f.w - u.y * f.z + u.z * f.y;
                 if (ENERGY) {
                     const C e0 = f.w - u.w, e1 = f.x - u.x, e2 = f.y - u.y, e3 = f.z - u.z;
-                    grad_e += (C)(0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                    grad_e += pf<C>(F.e_grad[a], 0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
                 }
             }
             J[a][0] = (C)0.25 * j0;
@@ -457,7 +468,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             j3 += t.w * fp.x - t.x * fp.w - t.y * fp.z + t.z * fp.y;
             if (ENERGY) {
                 const C e0 = fp.w - t.w, e1 = fp.x - t.x, e2 = fp.y - t.y, e3 = fp.z - t.z;
-                grad_e += (C)(0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+                grad_e += pf<C>(F.e_grad[a], 0.5 * P.inv_dx[a] * P.inv_dx[a]) * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
             }
         }
         J[a][0] = (C)0.25 * j0;
@@ -578,8 +589,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             // 1 - (U_now U_past^dag)_0 / |U_now U_past^dag| and 1 - cos(dtheta) = 2 sin^2(dtheta/2)
             const Q<C> Ed = {Un.w * Up.w + Un.x * Up.x + Un.y * Up.y + Un.z * Up.z, E1, E2, E3};
             const C h = gsin((C)0.5 * dth);
-            elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) *
-                      ((C)P.inv_g_sqr * one_minus_trace(Ed) + (C)P.inv_gp_sqr * (C)2 * h * h);
+            elec_e += pf<C>(F.e_elec[d], 4.0 * P.lap[d] * P.inv_sqr_dt) *
+                      (pf<C>(F.inv_g_sqr, P.inv_g_sqr) * one_minus_trace(Ed) + pf<C>(F.inv_gp_sqr, P.inv_gp_sqr) * (C)2 * h * h);
         }
         if (R0 * R0 > (C)1) warn |= kWarnAsin;
         if (fabs(th[d]) > (C)1e4) warn |= kWarnRange;
@@ -614,7 +625,7 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             const C RH = keep * gsin(dh) + dt2 * (MgH[d][0] + gH * JH[d][0]);
             if (ENERGY) {
                 const C h = gsin((C)0.5 * dh);
-                elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) * (C)P.inv_gpp_sqr * ((C)2 * h * h);
+                elec_e += pf<C>(F.e_elec[d], 4.0 * P.lap[d] * P.inv_sqr_dt) * pf<C>(F.inv_gpp_sqr, P.inv_gpp_sqr) * ((C)2 * h * h);
             }
             if (RH * RH > (C)1) warn |= kWarnAsin;
             if (fabs(hn) > (C)1e4) warn |= kWarnRange;
@@ -633,7 +644,8 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
             const C H3 = keep * F3 + dt2 * (MgH[d][2] + gH * JH[d][2]);
             if (ENERGY) {
                 const Q<C> Ed = {Hn.w * Hp.w + Hn.x * Hp.x + Hn.y * Hp.y + Hn.z * Hp.z, F1, F2, F3};
-                elec_e += (C)(4.0 * P.lap[d] * P.inv_sqr_dt) * (C)P.inv_gpp_sqr * one_minus_trace(Ed);
+                elec_e += pf<C>(F.e_elec[d], 4.0 * P.lap[d] * P.inv_sqr_dt) * pf<C>(F.inv_gpp_sqr, P.inv_gpp_sqr) *
+                          one_minus_trace(Ed);
             }
             const Q<C> Hnew = su2_advance(Hn, H1, H2, H3, warn, check);
             st4(ps.L.hq[d], ps.s, Hnew.w, Hnew.x, Hnew.y, Hnew.z);
@@ -663,7 +675,6 @@ __device__ __forceinline__ void site_step(const StepParams& P, const FConst& F, 
         obs[kObsKinetic] += ke;
         obs[kObsMagnetic] += me;
         obs[kObsElectric] += ee;
-        obs[kObsEnergy] += pot_e + ge + ke + me + ee;
         obs[kObsPlaqSU2] += (double)plaq2;
         obs[kObsPlaqU1] += (double)plaq1;
         obs[kObsPhiSq] += (double)phisq;

@@ -48,6 +48,7 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
     if (!ok && tid == 0) atomicOr(status, kErrTimeout);
 
     if (ENERGY) {
+        energy_total(obs);
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         block_reduce_store<kObsCount>(obs, partials + (size_t)b * kObsCount, kObsCount);
     }
