@@ -43,8 +43,10 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
     unsigned warn = 0;
     RingPhase ring = {0u};
     const int x0 = blockIdx.z * lx;
-    const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY>(maps, pmaps, P, F, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0,
-                                                       min(lx, P.nx - x0), smem, bars, ring, &s_abort, obs, warn);
+    constexpr bool STAGE = !ENERGY && HaloStage<S, TY, TZ, ND>::kUse;
+    const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY, LevelPtrs<S>, STAGE>(
+        maps, pmaps, P, F, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0, min(lx, P.nx - x0), smem, bars, ring,
+        &s_abort, obs, warn, smem + HaloStage<S, TY, TZ, ND>::OFFSET);
     if (!ok && tid == 0) atomicOr(status, kErrTimeout);
 
     if (ENERGY) {
@@ -147,9 +149,11 @@ static cudaError_t launch_tiled_t(const TMaps& maps, const TMaps& pmaps, const S
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
     } else {
+        using H = HaloStage<S, TY, TZ, ND>;
+        constexpr int SMEM = H::kUse ? H::SMEM : G::SMEM;  // plain steps stage their wrapped halo cells
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, false>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+        k<<<grid, block, SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
     }
     return cudaGetLastError();
 }

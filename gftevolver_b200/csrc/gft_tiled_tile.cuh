@@ -73,6 +73,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     }
 }
 
+// Per-thread asynchronous copies global -> shared (cp.async): they complete on
+// their own (no wait of another thread is involved) and the issuing thread
+// sees the data after cp.async.wait_all.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                             unsigned long long* bar)
 {
@@ -136,6 +152,24 @@ struct Geom {
     static constexpr int NBUF = 4;
     static constexpr unsigned TX = 3 * QBOX + 3 * HBOX + ND * QBOX;  // bytes per plane copy
     static constexpr int SMEM = NBUF * BUF + 128 + 64;             // + alignment slack + barriers
+};
+
+// Staging area for the wrapped halo cells of one plane (plain steps of the
+// tiled kernel): one slot per halo cell (the halo_cell numbering), quaternion
+// records [3 + ND][NH] then phases [3][NH], placed after the plane barriers.
+// FP32 only (the tiled kernel serves the mixed form).
+template <class S, int TY, int TZ, int ND>
+struct HaloStage {
+    using G = Geom<S, TY, TZ, ND>;
+    static constexpr int NH = 2 * G::QP + 2 * TY;
+    static constexpr int OFF_H = (3 + ND) * NH * 16;
+    static constexpr int BYTES = OFF_H + 3 * NH * 4;
+    static constexpr int OFFSET = G::NBUF * G::BUF + 64;  // 16-byte aligned (BUF is a multiple of 128)
+    static constexpr int SMEM = OFFSET + BYTES + 128;      // + alignment slack of the dynamic base
+    // Used only when it leaves the resident CTAs per SM unchanged: 228 KB of
+    // shared memory per SM, 1 KB reserved and 16 bytes static per CTA.
+    static constexpr int per_sm(int dyn) { return (228 * 1024) / (dyn + 16 + 1024); }
+    static constexpr bool kUse = sizeof(S) == 4 && SMEM <= 227 * 1024 && per_sm(SMEM) >= per_sm(G::SMEM);
 };
 
 // Reference to a site in a staged plane: buffer base, q/phi cell, theta cell.
@@ -255,6 +289,57 @@ __device__ __forceinline__ void patch_wrapped_halo(const StepParams& P, const LV
     }
 }
 
+// As prefetch_wrapped_halo, but the wrapped sites of plane X go by cp.async
+// into this thread's slots of the staging area, one plane before they are
+// patched (patch_from_stage).
+template <class S, int TY, int TZ, int ND, class LV>
+__device__ __forceinline__ void stage_wrapped_halo(const StepParams& P, const LV& now, int X, int y0, int z0, int tid,
+                                                   unsigned char* stage)
+{
+    using G = Geom<S, TY, TZ, ND>;
+    using H = HaloStage<S, TY, TZ, ND>;
+    static_assert(sizeof(S) == 4, "the halo stage holds FP32 records");
+    int ly, lz;
+    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
+    int y = y0 - 1 + ly, z = z0 - 1 + lz;
+    if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;
+    y = (y < 0) ? y + P.ny : (y >= P.ny ? y - P.ny : y);
+    z = (z < 0) ? z + P.nz : (z >= P.nz ? z - P.nz : z);
+    const size_t s = ((size_t)X * P.ny + y) * P.nz + z;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        cp_async16(stage + (d * H::NH + tid) * 16, now.q[d] + 4 * s);
+        cp_async4(stage + H::OFF_H + (d * H::NH + tid) * 4, now.th[d] + s);
+    }
+#pragma unroll
+    for (int k = 0; k < ND; k++) cp_async16(stage + ((3 + k) * H::NH + tid) * 16, now.ph[k] + 4 * s);
+    cp_async_commit();
+}
+
+// The wrapped halo cells of the plane in `buf` from this thread's staging
+// slots (filled by stage_wrapped_halo for that plane).
+template <class S, int TY, int TZ, int ND>
+__device__ __forceinline__ void patch_from_stage(const StepParams& P, unsigned char* buf, int y0, int z0, int tid,
+                                                 const unsigned char* stage)
+{
+    using G = Geom<S, TY, TZ, ND>;
+    using H = HaloStage<S, TY, TZ, ND>;
+    int ly, lz;
+    if (!halo_cell<TY, G::QP>(tid, ly, lz)) return;
+    const int y = y0 - 1 + ly, z = z0 - 1 + lz;
+    if (y >= 0 && y < P.ny && z >= 0 && z < P.nz) return;
+    cp_async_wait_all();
+    const int cq = ly * G::QP + lz, ch = ly * G::HP + lz + G::TP - 1;
+    const float4* sq = reinterpret_cast<const float4*>(stage);
+    const float* sh = reinterpret_cast<const float*>(stage + H::OFF_H);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        reinterpret_cast<float4*>(buf + d * G::QB)[cq] = sq[d * H::NH + tid];
+        reinterpret_cast<float*>(buf + G::OFF_TH + d * G::HB)[ch] = sh[d * H::NH + tid];
+    }
+#pragma unroll
+    for (int k = 0; k < ND; k++) reinterpret_cast<float4*>(buf + G::OFF_PH + k * G::QB)[cq] = sq[(3 + k) * H::NH + tid];
+}
 
 // Parity of the completed phases of the NBUF plane barriers (bit b for
 // barrier b), carried from tile to tile by a persistent CTA (every thread
@@ -268,11 +353,15 @@ struct RingPhase {
 // shared flag that is 0 on entry.  Returns false (on every thread) if a wait
 // gave up; the ring is then drained and must not be reused.  LV: the level
 // pointer struct (its q / th / ph members are read).
-template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV>
+// STAGE: the wrapped halo cells of plane i+4 are copied by cp.async into
+// `stage` (HaloStage) while plane i+1 is computed, instead of prefetched into L2
+// and loaded after the plane's wait.
+template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV, bool STAGE = false>
 __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const FConst& F,
                                          const LV& now, const LV& past, int y0, int z0, int x0,
                                          int nloc, unsigned char* smem, unsigned long long* bars, RingPhase& ring,
-                                         int* s_abort, double (&obs)[kObsCount], unsigned& warn)
+                                         int* s_abort, double (&obs)[kObsCount], unsigned& warn,
+                                         unsigned char* stage = nullptr)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<S, TY, TZ, ND>;
@@ -294,7 +383,12 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         // past level of the first two planes computed (relative planes 1 and 2)
         for (int p = 1; p <= 2 && p <= nloc; p++) prefetch_past<ND>(pmaps, plane_x(p), y0, z0);
     }
-    if (wraps && nplanes > 3) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(3), y0, z0, tid);
+    if (wraps && nplanes > 3) {
+        if constexpr (STAGE)
+            stage_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(3), y0, z0, tid, stage);
+        else
+            prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(3), y0, z0, tid);
+    }
 
     // own cells
     const int cq0 = (ty + 1) * G::QP + (tz + 1);
@@ -349,9 +443,13 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         bool okn = true;
         if (i + 3 < nplanes) {
             okn = mbar_wait_bounded(&bars[(i + 3) % G::NBUF], parity(i + 3));
-            if (okn && wraps)
-                patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + ((i + 3) % G::NBUF) * G::BUF, plane_x(i + 3), y0, z0,
-                                                  tid);
+            if (okn && wraps) {
+                if constexpr (STAGE)
+                    patch_from_stage<S, TY, TZ, ND>(P, smem + ((i + 3) % G::NBUF) * G::BUF, y0, z0, tid, stage);
+                else
+                    patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + ((i + 3) % G::NBUF) * G::BUF, plane_x(i + 3), y0,
+                                                      z0, tid);
+            }
         }
         if (!okn) *s_abort = 1;
         __syncthreads();
@@ -362,11 +460,17 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
             break;
         }
         if (tid == 32 % (TY * TZ) && i + 3 <= nloc) prefetch_past<ND>(pmaps, plane_x(i + 3), y0, z0);
-        if (wraps && i + 4 < nplanes) prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 4), y0, z0, tid);
+        if (wraps && i + 4 < nplanes) {
+            if constexpr (STAGE)
+                stage_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 4), y0, z0, tid, stage);
+            else
+                prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(i + 4), y0, z0, tid);
+        }
         if (tid == 0 && i + G::NBUF < nplanes)
             issue_plane<S, TY, TZ, ND>(maps, smem + (i % G::NBUF) * G::BUF, &bars[i % G::NBUF],
                                        plane_x(i + G::NBUF), y0, z0);
     }
+    if constexpr (STAGE) cp_async_wait_all();  // a staged plane not patched (abort) is still in flight
     if (aborted) {
         // drain: wait (bounded) for the copies still in flight into this CTA's buffers
         if (tid == 0)
