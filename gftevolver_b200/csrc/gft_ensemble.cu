@@ -92,6 +92,21 @@ __device__ __forceinline__ void tmap_acquire(const TMaps& m)
 // items[i] = {member within the group, y0, z0, x0}; tile i's energy partials
 // go to partials row i.  UNIFORM: the members share ep.common but for their
 // geometry (the per-member fields copied below).
+// Plain steps stage the wrapped halo sites (run_tile's STAGE) where the staging
+// area leaves the resident CTAs per SM unchanged; the dynamic shared memory
+// then includes it.
+template <int MODEL, int TY, int TZ, bool ENERGY>
+constexpr bool ens_stage()
+{
+    return !ENERGY && HaloStage<float, TY, TZ, (MODEL == kModelSM) ? 1 : 2>::kUse;
+}
+template <int MODEL, int TY, int TZ, bool ENERGY>
+constexpr int ens_smem()
+{
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    return ens_stage<MODEL, TY, TZ, ENERGY>() ? HaloStage<float, TY, TZ, ND>::SMEM : Geom<float, TY, TZ, ND>::SMEM;
+}
+
 template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
     ensemble_step_kernel(const __grid_constant__ EnsParams ep, const EnsMaps* __restrict__ maps,
@@ -143,9 +158,9 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
         FConst Fm;
         if constexpr (!UNIFORM) Fm = make_fconst(P);
         const FConst& F = UNIFORM ? ep.fcommon : Fm;
-        const bool ok = run_tile<float, MODEL, TY, TZ, ENERGY>(mp.tm[tn], mp.tp[1 - tn], P, F, ep.lv[m][tn],
-                                                               ep.lv[m][1 - tn], w.y, w.z, w.w, min(lx, P.nx - w.w),
-                                                               smem, bars, ring, &s_abort, obs, warn);
+        const bool ok = run_tile<float, MODEL, TY, TZ, ENERGY, EnsLevel, ens_stage<MODEL, TY, TZ, ENERGY>()>(
+            mp.tm[tn], mp.tp[1 - tn], P, F, ep.lv[m][tn], ep.lv[m][1 - tn], w.y, w.z, w.w, min(lx, P.nx - w.w), smem,
+            bars, ring, &s_abort, obs, warn, smem + HaloStage<float, TY, TZ, ND>::OFFSET);
         if (!ok) {
             if (tid == 0) atomicOr(status, kErrTimeout);
             break;
@@ -211,14 +226,13 @@ __global__ void __launch_bounds__(kFinThreads) ensemble_finalize_kernel(const do
 template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 int resident_ctas()
 {
-    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
-    using G = Geom<float, TY, TZ, ND>;
+    constexpr int SMEM = ens_smem<MODEL, TY, TZ, ENERGY>();
     static int per_sm = 0;
     if (per_sm == 0) {
         auto k = ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, TY * TZ, G::SMEM) != cudaSuccess || n < 1) n = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, TY * TZ, SMEM) != cudaSuccess || n < 1) n = 1;
         per_sm = n;
     }
     return per_sm;
@@ -228,12 +242,10 @@ template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 cudaError_t launch_step_u(const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems, int lx, int tn,
                           unsigned* status, double* partials, int nsm, cudaStream_t s)
 {
-    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
-    using G = Geom<float, TY, TZ, ND>;
     const int grid = std::min(nitems, nsm * resident_ctas<MODEL, TY, TZ, ENERGY, UNIFORM>());
     if (grid < 1) return cudaSuccess;
-    ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM>
-        <<<grid, dim3(TZ, TY, 1), G::SMEM, s>>>(ep, maps, items, nitems, lx, tn, status, partials);
+    ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM><<<grid, dim3(TZ, TY, 1), ens_smem<MODEL, TY, TZ, ENERGY>(), s>>>(
+        ep, maps, items, nitems, lx, tn, status, partials);
     return cudaGetLastError();
 }
 
