@@ -18,7 +18,8 @@ reference's shipped analyser configuration.
              x sites / average step-kernel duration, vs measured HBM copy
              bandwidth.
   cpu_baseline  the reference itself (oracle/_ref/ref32, compiled from its own
-             sources) on the host cores, a bounded sample.
+             sources) on the host cores, a bounded sample; forms.fp64 carries the
+             same for its double-storage build (oracle/_ref/ref64).
   precision  the mixed form against the FP64 form on the same initial data
              over --precision-steps steps (default 1000): field deviation,
              energy drift and Gauss-law residual.
@@ -166,8 +167,9 @@ def committed_traffic(kernel: str):
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference binary (or the oracle port) on the host cores
 # ---------------------------------------------------------------------------
-def cpu_reference_throughput(model: str, n: int, steps: int, procs: int):
-    """Run `procs` independent reference processes, each n^3 for `steps` steps; aggregate site-updates/s."""
+def cpu_reference_throughput(model: str, n: int, steps: int, procs: int, fp64: bool = False):
+    """Run `procs` independent reference processes, each n^3 for `steps` steps; aggregate site-updates/s.
+    fp64: the reference built with double storage (oracle/_ref/ref64) instead of its float build."""
     import numpy as np
     from oracle import oracle as orc
     from oracle import refrun
@@ -177,11 +179,11 @@ def cpu_reference_throughput(model: str, n: int, steps: int, procs: int):
     ic = orc.ICSpec(seed=7, mean=[1.0 if model == "sm" else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                     eps_sigma=0.1)
     sc, ve = orc.init_fields(op, ic, np.float32)
-    if refrun.available(False):
+    if refrun.available(fp64):
         results = [None] * procs
 
         def one(k):
-            results[k] = refrun.run(op, sc, ve, steps, fp64=False)[3]
+            results[k] = refrun.run(op, sc, ve, steps, fp64=fp64)[3]
 
         ths = [threading.Thread(target=one, args=(k,)) for k in range(procs)]
         t0 = time.perf_counter()
@@ -194,8 +196,11 @@ def cpu_reference_throughput(model: str, n: int, steps: int, procs: int):
         agg = procs * op.nsite * steps / max(results)
         return {"value": agg, "unit": "site-updates/s", "cores": procs, "kind": "reference",
                 "per_process": statistics.median(per), "wall_s": wall,
-                "sample": f"{procs} independent processes of the reference (oracle/_ref/ref32, -O3) "
+                "sample": f"{procs} independent processes of the reference "
+                          f"(oracle/_ref/{'ref64' if fp64 else 'ref32'}, -O3) "
                           f"each {n}^3 x {steps} steps, analysers every {LOG_EVERY}"}
+    if fp64:
+        return None  # the FP64 figure is reported only for the reference itself
     # oracle port (single thread per process)
     t0 = time.perf_counter()
     orc.evolve(op, sc, ve, steps)
@@ -568,6 +573,12 @@ def main():
             cpu = cpu_reference_throughput(args.model, 40, 10, host_cores())
         except Exception as ex:  # the baseline is reported, not required
             cpu = {"value": None, "error": str(ex)}
+        if fp64 is not None:
+            # the reference's double-storage build beside the FP64 form
+            try:
+                fp64["cpu_reference"] = cpu_reference_throughput(args.model, 40, 10, host_cores(), fp64=True)
+            except Exception as ex:
+                fp64["cpu_reference"] = {"value": None, "error": str(ex)}
     line = {
         "metric": "site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
