@@ -7,8 +7,8 @@ sm_100a CUDA kernels behind the C ABI of ``include/gft.h``
 """
 from ._lib import (GFT_FORM_FP64, GFT_FORM_MIXED, GFT_FORM_REF, GFT_MODEL_2HDM, GFT_MODEL_SM, GftError,  # noqa: F401
                    load)
-from .ensemble import Ensemble  # noqa: F401
+from .ensemble import Ensemble, ShardedEnsemble, member_shard  # noqa: F401
 from .evolver import FORMS, Evolver, InitialData, LatticeParams  # noqa: F401
 
-__all__ = ["Evolver", "Ensemble", "LatticeParams", "InitialData", "FORMS", "GftError", "load",
+__all__ = ["Evolver", "Ensemble", "ShardedEnsemble", "member_shard", "LatticeParams", "InitialData", "FORMS", "GftError", "load",
            "GFT_MODEL_SM", "GFT_MODEL_2HDM", "GFT_FORM_REF", "GFT_FORM_FP64", "GFT_FORM_MIXED"]

@@ -8,6 +8,11 @@ list of tiles of every member, whole logging periods replay from a CUDA graph,
 and ``autotune()`` picks the tile shape and march depth by timing them on the
 ensemble itself.  Every member evolves exactly as ``Evolver`` with
 ``set_kernel(2, tile, march)`` would (mixed form).
+
+On several GPUs the members are replicas, not a decomposition: with one process
+per GPU, ``ShardedEnsemble`` deals them round-robin (``member_shard``) and each
+rank evolves its share as an ``Ensemble``; the ranks exchange no fields, and the
+analyser rows meet only when ``gather_rows`` is called.
 """
 from __future__ import annotations
 
@@ -131,3 +136,75 @@ class Ensemble:
     @property
     def nsite(self) -> int:
         return sum(p.nsite for p in self.params)
+
+
+def member_shard(n_members: int, rank: int, world: int) -> list[int]:
+    """The members that rank `rank` of `world` evolves when `n_members` realisations
+    are dealt round-robin over one process per GPU (member m goes to rank m % world)."""
+    if world < 1 or not 0 <= rank < world or n_members < 0:
+        raise ValueError(f"bad shard request: {n_members} members, rank {rank} of {world}")
+    return list(range(rank, n_members, world))
+
+
+def gather_member_rows(local_rows: list, n_members: int, rank: int, world: int, group=None) -> list:
+    """Every member's analyser rows, in member order, on every rank, from each rank's
+    rows of its own members (`local_rows[k]` belongs to member_shard(...)[k]).  One
+    all_gather of Python objects through torch.distributed; it is the only exchange
+    of a sharded ensemble and runs outside the step loop."""
+    import torch.distributed as dist
+
+    mine = member_shard(n_members, rank, world)
+    if len(local_rows) != len(mine):
+        raise ValueError(f"rank {rank} holds {len(mine)} members but passed rows for {len(local_rows)}")
+    got = [None] * world
+    dist.all_gather_object(got, list(local_rows), group=group)
+    out = [None] * n_members
+    for r in range(world):
+        for k, m in enumerate(member_shard(n_members, r, world)):
+            out[m] = got[r][k]
+    return out
+
+
+class ShardedEnsemble:
+    """This rank's round-robin share of an ensemble (one process per GPU).
+
+    rank / world default to torch.distributed's when a process group is
+    initialised, else to a single rank.  A rank with no members (fewer members
+    than ranks) holds no device state and evolves nothing."""
+
+    def __init__(self, params: list[LatticeParams], device: int = 0, rank: int | None = None,
+                 world: int | None = None):
+        if rank is None or world is None:
+            import torch.distributed as dist
+            on = dist.is_available() and dist.is_initialized()
+            if rank is None:
+                rank = dist.get_rank() if on else 0
+            if world is None:
+                world = dist.get_world_size() if on else 1
+        self.n_members, self.rank, self.world = len(params), rank, world
+        self.members = member_shard(len(params), rank, world)
+        self.local = Ensemble([params[m] for m in self.members], device=device) if self.members else None
+
+    def init_fields(self, ics: list[InitialData]) -> None:
+        if len(ics) != self.n_members:
+            raise ValueError("one InitialData per member of the whole ensemble")
+        if self.local is not None:
+            self.local.init_fields([ics[m] for m in self.members])
+
+    def evolve(self, n_steps: int) -> list[list[dict]]:
+        """Advance this rank's members; their rows, in member_shard order."""
+        return self.local.evolve(n_steps) if self.local is not None else []
+
+    def gather_rows(self, local_rows: list, group=None) -> list:
+        return gather_member_rows(local_rows, self.n_members, self.rank, self.world, group)
+
+    def close(self) -> None:
+        if self.local is not None:
+            self.local.close()
+            self.local = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

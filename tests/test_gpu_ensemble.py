@@ -170,3 +170,29 @@ def test_member_with_fixed_faces_evolves_like_a_single_handle(oracle_mod):
         one.init_fields([InitialData(**ics[1])])
         init = one.download(0)
     assert np.array_equal(out[1][0][:, :, 0], init[0][:, :, 0]) and np.array_equal(out[1][1][:, :, -1], init[1][:, :, -1])
+
+
+def test_sharded_ensemble_halves_match_the_whole(oracle_mod):
+    """Two round-robin shards (ranks 0 and 1 of 2, run one after the other on one GPU)
+    evolve their members exactly as the whole ensemble does: same kernel instance,
+    same tile and march, each member's tiles and reductions independent of the others."""
+    from gftevolver_b200 import Ensemble, InitialData, ShardedEnsemble
+    ps, ics = _members(oracle_mod, 1, [(16, 8, 16), (8, 12, 32), (24, 4, 16), (8, 8, 32), (16, 16, 16)])
+    ics = [InitialData(**ic) for ic in ics]
+    with Ensemble(ps) as whole:
+        whole.set_kernel(2, 8)
+        whole.init_fields(ics)
+        w_rows = whole.evolve(6)
+        w_fields = [whole.download(m) for m in range(len(ps))]
+    got_rows = [None] * len(ps)
+    for rank in range(2):
+        with ShardedEnsemble(ps, rank=rank, world=2) as se:
+            assert se.members == list(range(rank, len(ps), 2))
+            se.local.set_kernel(2, 8)
+            se.init_fields(ics)
+            rows = se.evolve(6)
+            for k, m in enumerate(se.members):
+                got_rows[m] = rows[k]
+                sc, ve = se.local.download(k)
+                assert np.array_equal(sc, w_fields[m][0]) and np.array_equal(ve, w_fields[m][1])
+    assert got_rows == w_rows
