@@ -271,27 +271,35 @@ __global__ void math_selftest_kernel(int n, unsigned long long* err_bits)
         e6 = fabs((double)gasin((float)x) - asin(xf)) / fmax(fabs(asin(xf)), 1e-300);
         e7 = fabs(gasin(x) - asin(x)) / fmax(fabs(asin(x)), 1e-300);
     }
-    const double e[8] = {e0, e1, e2, e3, e4, e5, e6, e7};
-    for (int k = 0; k < 8; k++) atomicMax(err_bits + k, (unsigned long long)__double_as_longlong(e[k]));
+    // one_minus_cos_nr on the quaternion (cos x, sin x n) with |n|^2 = 1 + 2^-20 (not exactly
+    // unit, as stored links are not), against the same expression in FP64 from the same floats
+    const float w = (float)cos(x), sn = (float)sin(x);
+    const float v1 = sn * 0.6f, v3 = sn * 0.8f * 1.0000005f;
+    const float v2f = v1 * v1 + v3 * v3;
+    const double v2 = (double)v1 * v1 + (double)v3 * v3, nrm = sqrt((double)w * w + v2);
+    const double ex = (w >= 0.0f) ? v2 / (nrm * (nrm + w)) : 1.0 - w / nrm;
+    const double e8 = (ex > 0.0) ? fabs((double)one_minus_cos_nr(w, v2f) - ex) / ex : 0.0;
+    const double e[9] = {e0, e1, e2, e3, e4, e5, e6, e7, e8};
+    for (int k = 0; k < 9; k++) atomicMax(err_bits + k, (unsigned long long)__double_as_longlong(e[k]));
 }
 
 }  // namespace
 
-cudaError_t run_math_selftest(int n, double* out8)
+cudaError_t run_math_selftest(int n, double* out9)
 {
     unsigned long long* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, 8 * sizeof(unsigned long long));
+    cudaError_t e = cudaMalloc(&d, 9 * sizeof(unsigned long long));
     if (e != cudaSuccess) return e;
-    cudaMemset(d, 0, 8 * sizeof(unsigned long long));
+    cudaMemset(d, 0, 9 * sizeof(unsigned long long));
     math_selftest_kernel<<<(n + 255) / 256, 256>>>(n, d);
     e = cudaGetLastError();
-    unsigned long long h[8] = {0};
+    unsigned long long h[9] = {0};
     if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(d);
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < 9; k++) {
         double v;
         memcpy(&v, &h[k], sizeof(double));
-        out8[k] = v;
+        out9[k] = v;
     }
     return e;
 }

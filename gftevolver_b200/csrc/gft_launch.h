@@ -122,6 +122,6 @@ constexpr int kRowSlotCount = kObsCount + kGaussSlotsMax;
 inline int config_neq(const gft_config& c) { return c.model == GFT_MODEL_2HDM ? hf_neq(c.higgs_family) : 4; }
 
 // Elementary-function self-test (gft_math.cuh vs CUDA's functions) on the current device.
-cudaError_t run_math_selftest(int n, double* out8);
+cudaError_t run_math_selftest(int n, double* out9);
 
 }  // namespace gft

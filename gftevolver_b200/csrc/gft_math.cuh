@@ -239,4 +239,34 @@ __device__ __forceinline__ double sqrt1m_minus1(double c)
     return sqrt1m_wide(c);
 }
 
+// 1/sqrt(s) and 1/d for arguments of order one: the hardware approximations
+// (rsqrt.approx, rcp.approx; relative error below 2^-22) refined by one
+// Newton-Raphson step each, r <- r (3 - s r^2) / 2 and q <- q (2 - d q), which
+// squares that error; the results are within about one ulp of the rounded
+// quotients.
+__device__ __forceinline__ float rsqrt_nr(float s)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(s));
+    return r * fmaf(-0.5f * s * r, r, 1.5f);
+}
+__device__ __forceinline__ float rcp_nr(float d)
+{
+    float q;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(q) : "f"(d));
+    return q * fmaf(-d, q, 2.0f);
+}
+
+// 1 - a0/|a| of a quaternion with scalar part w and |vector part|^2 = v2,
+// without cancellation: v2 / (|a| (|a| + w)) = v2 r^2 / (1 + w r) when w >= 0
+// (r = 1/|a|), else 1 - w r.  Float form of the energy terms' plaquette and
+// electric traces; a few ulp of the same expression evaluated with IEEE
+// square root and division (checked by gft_selftest_math).
+__device__ __forceinline__ float one_minus_cos_nr(float w, float v2)
+{
+    const float r = rsqrt_nr(fmaf(w, w, v2));
+    const float c = w * r;
+    return (w >= 0.0f) ? v2 * r * r * rcp_nr(1.0f + c) : 1.0f - c;
+}
+
 }  // namespace gft

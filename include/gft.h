@@ -259,9 +259,11 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
 /* Diagnostic with no reference counterpart: evaluates the library's own
  * sin/cos/asin (range-reduced series used by the throughput forms) against
- * CUDA's functions on `device`.  out[8] = max abs error of float sincos.sin,
+ * CUDA's functions on `device`.  out[9] = max abs error of float sincos.sin,
  * float sincos.cos, float sin, double sincos.sin, double sincos.cos, double sin;
- * max relative error of float asin, double asin. */
+ * max relative error of float asin, double asin, and of the float 1 - a0/|a| of
+ * the energy terms (Newton-refined reciprocal square root and reciprocal) against
+ * the same expression in double. */
 int gft_selftest_math(int device, double* out);
 
 /* ---- ensembles ---------------------------------------------------------- */
