@@ -568,7 +568,7 @@ def main():
     achieved = balg * p.nsite / (kms / 1e3) / 1e9
     traffic = committed_traffic(f"{kernel_name}_{args.model}_{form}_{args.size}")
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baselines belong to the N = 1 line
         try:
             cpu = cpu_reference_throughput(args.model, 40, 10, host_cores())
         except Exception as ex:  # the baseline is reported, not required
