@@ -148,6 +148,24 @@ __host__ __device__ inline FConst make_fconst(const StepParams& P)
     return F;
 }
 
+// Per-thread asynchronous copies global -> shared (cp.async): they complete on
+// their own (no wait of another thread is involved) and the issuing thread
+// sees the data after cp.async.wait_all.  Both addresses aligned to the size.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // A site on a Fixed face (BoundaryConditions/Source/Fixed.cpp:159-251): not
 // evolved, not part of the analysers' domain.
 __device__ __forceinline__ bool frozen(const StepParams& P, int x, int y, int z)

@@ -707,11 +707,11 @@ __device__ __forceinline__ GLink gauss_link(const LV& now, const LV& fut, int d,
 }
 
 // The residuals from the links at x (own[d]) and at x - e_d (back[d]) and the
-// doublets at x (site c).
+// doublets at x (phn / phf: both levels; site c for the local output).
 // NEQ_ALL: the local-violation stride (gaugeNum; the Higgs-family constraints follow)
-template <class S, int MODEL, class LV, int NEQ_ALL = 4>
+template <int MODEL, int NEQ_ALL = 4>
 __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&own)[3], const GLink (&back)[3],
-                                           const LV& now, const LV& fut, int c,
+                                           const Q<double> (&phn)[2], const Q<double> (&phf)[2], int c,
                                            double (&v)[kGaussSlots])
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
@@ -732,8 +732,8 @@ __device__ __forceinline__ void gauss_core(const StepParams& P, const GLink (&ow
     double gr[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int db = 0; db < ND; db++) {
-        const Q<double> p = ld4<double>(now.ph[db], c);
-        const Q<double> q = ld4<double>(fut.ph[db], c);
+        const Q<double> p = phn[db];
+        const Q<double> q = phf[db];
         gr[0] += 0.25 * (p.w * q.x - p.x * q.w + p.y * q.z - p.z * q.y);
         gr[1] += 0.25 * (p.w * q.z - p.x * q.y + p.y * q.x - p.z * q.w);
         gr[2] += 0.25 * (-p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x);
@@ -758,12 +758,18 @@ __device__ __forceinline__ void gauss_site(const StepParams& P, const LV& now, c
 {
     const GLink own[3] = {gauss_link<S>(now, fut, 0, c), gauss_link<S>(now, fut, 1, c), gauss_link<S>(now, fut, 2, c)};
     const GLink back[3] = {gauss_link<S>(now, fut, 0, md0), gauss_link<S>(now, fut, 1, md1), gauss_link<S>(now, fut, 2, md2)};
+    Q<double> phn[2], phf[2];
+#pragma unroll
+    for (int db = 0; db < ((MODEL == kModelSM) ? 1 : 2); db++) {
+        phn[db] = ld4<double>(now.ph[db], c);
+        phf[db] = ld4<double>(fut.ph[db], c);
+    }
     if constexpr (HF == kHfNone) {
-        gauss_core<S, MODEL>(P, own, back, now, fut, c, v);
+        gauss_core<MODEL>(P, own, back, phn, phf, c, v);
     } else {
         constexpr int NEQ = hf_neq(HF);
         double vs[kGaussSlots];
-        gauss_core<S, MODEL, LV, NEQ>(P, own, back, now, fut, c, vs);
+        gauss_core<MODEL, NEQ>(P, own, back, phn, phf, c, vs);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             v[k] = vs[k];

@@ -73,22 +73,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     }
 }
 
-// Per-thread asynchronous copies global -> shared (cp.async): they complete on
-// their own (no wait of another thread is involved) and the issuing thread
-// sees the data after cp.async.wait_all.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* dst, const void* src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                             unsigned long long* bar)
 {
