@@ -343,7 +343,10 @@ def ensemble_report(steps: int, device: int) -> dict:
                     f"{LOG_EVERY} steps",
         "members": 64, "sites": nsite, "edges_histogram": {str(e): edges.count(e) for e in (32, 48, 64, 96)},
         "steps": steps, "value": nsite * steps / (ms / 1e3), "unit": "site-updates/s",
-        "ms_per_step": ms / steps, "tile": ["8x32", "4x32", "4x16", "16x16"][tile], "march": march, "graphs": True,
+        "ms_per_step": ms / steps,
+        # 228 B per site-update (the single lattice's algorithmic bytes) over the whole step, launches included
+        "roofline_frac": B_ALG[("sm", 4)] * nsite * steps / (ms / 1e3) / 1e9 / measured_peaks()[0],
+        "tile": ["8x32", "4x32", "4x16", "16x16"][tile], "march": march, "graphs": True,
         "kernel_launches_per_step": launches / steps, "nonfinite_rows": len(bad),
     }
 
@@ -505,7 +508,7 @@ def main():
     fp64 = None
     if form == "mixed" and not args.no_fp64:
         ev.runner.close()
-        fsteps = args.fp64_steps or max(args.steps // 4, 10)
+        fsteps = args.fp64_steps or args.steps  # the same step count (and logging steps) as the mixed form
         ev64, ms64, kms64, nk64, _, _ = timed_run("fp64", fsteps, min(args.warmup, 3))
         ms64 = max_over_ranks(ms64)
         v64 = world * p.nsite * fsteps / (ms64 / 1e3)
@@ -581,6 +584,10 @@ def main():
                 fp64["cpu_reference"] = {"value": None, "error": str(ex)}
     line = {
         "metric": "site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
+        # the FP64 form on the same workload, up front so that short records of the line keep it
+        "fp64_value": fp64["value"] if fp64 else None,
+        "mixed_over_fp64": fp64["mixed_over_fp64"] if fp64 else None,
+        "fp64_roofline_frac": fp64["roofline_frac"] if fp64 else None,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if sbytes == 4 else "f64", "data": "synthetic",

@@ -73,6 +73,7 @@ struct gft_handle {
     int kernel_kind = 0;    // 0 auto, 1 global-memory kernel, 2 tiled (TMA) kernel
     int tile_variant = 0;   // tiled: index into the built tile shapes
     int march = 32;         // tiled: planes per CTA along x
+    unsigned long long wait_limit_ns = 0;  // gft_set_wait_limit (0: the 2 s default)
     bool tiled_ready = false;
     TMaps tm[2];   // staged "now" planes (with halo), per level
     TMaps tp[2];   // past-level L2 prefetch boxes (no halo), per level
@@ -193,6 +194,7 @@ StepParams make_params(const gft_handle* h, int time_iter, bool energy)
         P.obs_x0 = h->x_begin;
         P.obs_x1 = h->x_end;
     }
+    P.wait_limit_ns = h->wait_limit_ns;
     return P;
 }
 
@@ -815,6 +817,13 @@ int gft_observe(gft_handle* h, gft_observables* row)
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "gft_observe");
     fill_row(row, ti, true, false, host.data(), h->neq);
+    return GFT_OK;
+}
+
+int gft_set_wait_limit(gft_handle* h, unsigned long long ns)
+{
+    if (!h) return GFT_E_INVALID;
+    h->wait_limit_ns = ns;
     return GFT_OK;
 }
 

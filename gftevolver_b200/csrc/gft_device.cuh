@@ -84,6 +84,8 @@ struct StepParams {
     int obs_x0, obs_x1;     // planes whose sites count in observables, Gauss residuals and warnings
                             // (all planes, except on an x-slab with ghost planes)
     int fixed_axes;         // bit a: the two faces of axis a are Fixed (frozen, not evolved)
+    unsigned long long wait_limit_ns;  // limit of the tiled kernels' plane waits (0: 2 s); the drain
+                                       // after a failed wait keeps the 2 s bound
 };
 
 // The mixed form's per-site constants in float, precomputed on the host and

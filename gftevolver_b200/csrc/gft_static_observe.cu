@@ -22,7 +22,9 @@
 // In host code the array's name is only a host-side stand-in; its device
 // address is obtained with cudaGetSymbolAddress once per device, on the first
 // call made with that device current.  That first call therefore issues a
-// runtime query and should come before any stream capture.
+// runtime query and should come before any stream capture.  The address is kept
+// per device ordinal for the life of the process: after cudaDeviceReset on a
+// device, the library must not be called on that device again.
 #include <mutex>
 #include <string>
 
@@ -199,9 +201,25 @@ using namespace gft;
 extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, const float* d_vectors, int time_iter,
                                   double* d_out, void* stream)
 {
-    if (!c || !d_scalars || !d_vectors || !d_out || time_iter < 0) return GFT_E_INVALID;
-    if (c->model != GFT_MODEL_SM && c->model != GFT_MODEL_2HDM) return GFT_E_UNSUPPORTED;
-    if (c->nx < 1 || c->ny < 1 || c->nz < 1) return GFT_E_INVALID;
+    if (!c || !d_scalars || !d_vectors || !d_out || time_iter < 0) {
+        set_last_error("gft_observe_static: null configuration or buffer, or negative time_iter");
+        return GFT_E_INVALID;
+    }
+    {
+        // the same checks as gft_create (lattice extents, spacings, time step, couplings, model)
+        // form and storage_bytes are not read here: validate as the mixed form
+        gft_config v = *c;
+        v.form = GFT_FORM_MIXED;
+        v.storage_bytes = 4;
+        std::string why;
+        const int rc = validate_config(&v, why);
+        if (rc != GFT_OK) {
+            const std::string pre = "gft_create: ";
+            if (why.compare(0, pre.size(), pre) == 0) why = why.substr(pre.size());
+            set_last_error("gft_observe_static: " + why);
+            return rc;
+        }
+    }
     if (c->fixed_axes != 0) {
         set_last_error("gft_observe_static: periodic lattices only (fixed_axes must be 0)");
         return GFT_E_UNSUPPORTED;
@@ -217,7 +235,11 @@ extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, c
         return GFT_E_UNSUPPORTED;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GFT_E_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        set_last_error("gft_observe_static: no current CUDA device, or its ordinal is beyond " +
+                       std::to_string(kMaxDevices - 1));
+        return GFT_E_CUDA;
+    }
     double* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_static_mu);

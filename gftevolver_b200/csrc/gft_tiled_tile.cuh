@@ -14,9 +14,10 @@
 // wrapped sites.  The own-site past level is read and written directly
 // (coalesced: consecutive threads are consecutive z).
 //
-// Bounded waits: every mbarrier wait gives up after 2 s of %globaltimer; the
-// tile then waits (with the same bound) for its copies still in flight,
-// reports failure and the caller records kErrTimeout in the status word.
+// Bounded waits: every mbarrier wait gives up after 2 s of %globaltimer (or the
+// shorter diagnostic limit StepParams::wait_limit_ns); the tile then waits, with
+// the 2 s bound, for its copies still in flight, reports failure and the caller
+// records kErrTimeout in the status word.
 #pragma once
 
 #include <cuda.h>
@@ -62,14 +63,35 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Wait for phase `parity` of `bar`; false after 2 s.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity)
+// Non-blocking test of phase `parity` of `bar`.
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity)
 {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+
+// Wait for phase `parity` of `bar`; false after `limit_ns` (0: 2 s).  A limit
+// below 1 us is one non-blocking test (the diagnostic of gft_set_wait_limit:
+// it fails whenever the copy has not landed yet).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned long long limit_ns = 0)
+{
+    if (limit_ns != 0 && limit_ns < 1000ull) return mbar_test_wait(bar, parity);
+    const unsigned long long lim = limit_ns ? limit_ns : kWaitLimitNs;
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer_ns() - t0 > 2000000000ull) return false;
+        if (globaltimer_ns() - t0 > lim) return false;
     }
 }
 
@@ -384,7 +406,7 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
     // planes 0, 1, 2 (x0-1, x0, x0+1) resident and patched before the first site
     bool ok = true;
     for (int p = 0; p < 3; p++) {  // nplanes >= 3
-        ok = ok && mbar_wait_bounded(&bars[p], parity(p));
+        ok = ok && mbar_wait_bounded(&bars[p], parity(p), P.wait_limit_ns);
         if (ok && wraps) patch_wrapped_halo<S, TY, TZ, ND>(P, now, smem + p * G::BUF, plane_x(p), y0, z0, tid);
     }
     if (!ok) *s_abort = 1;
@@ -426,7 +448,7 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
         // plane i+3 (x+2) for the next site; its copy was issued one plane ago
         bool okn = true;
         if (i + 3 < nplanes) {
-            okn = mbar_wait_bounded(&bars[(i + 3) % G::NBUF], parity(i + 3));
+            okn = mbar_wait_bounded(&bars[(i + 3) % G::NBUF], parity(i + 3), P.wait_limit_ns);
             if (okn && wraps) {
                 if constexpr (STAGE)
                     patch_from_stage<S, TY, TZ, ND>(P, smem + ((i + 3) % G::NBUF) * G::BUF, y0, z0, tid, stage);

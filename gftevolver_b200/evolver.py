@@ -278,6 +278,10 @@ class Evolver:
             self.lib.gft_evolve(self.h, int(n_steps), rows, int(max_rows), ctypes.byref(n)), self.h)
         return [_row_dict(rows[i], self.params.neq) for i in range(n.value)]
 
+    def set_wait_limit(self, ns: int = 0) -> None:
+        """Time limit of the tiled kernel's plane waits in ns (0: the 2 s default); see gft_set_wait_limit."""
+        _lib.check(self.lib.gft_set_wait_limit(self.h, int(ns)), self.h)
+
     def set_kernel(self, kind: int = 0, tile: int = 0, march: int = 32) -> None:
         """Step kernel of the throughput forms: 0 auto, 1 one thread per site, 2 TMA-staged tiles."""
         _lib.check(self.lib.gft_set_kernel(self.h, int(kind), int(tile), int(march)), self.h)

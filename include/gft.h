@@ -240,8 +240,10 @@ int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes
  * Allocates nothing: its scratch is a fixed 1.2 MB device array compiled into
  * the library, so lattices above 67,108,864 sites return GFT_E_UNSUPPORTED.
  * The first call on a device looks up that array's address (do it before any
- * stream capture); calls that overlap on the GPU share the array and race, so
- * the caller serialises them.  Only cfg's lattice, model and coupling fields
+ * stream capture) and keeps it for the life of the process, so a device that
+ * has been reset with cudaDeviceReset must not be used with it again.  Calls
+ * that overlap on the GPU share the array and race, so the caller serialises
+ * them.  Only cfg's lattice, model and coupling fields
  * are read (form and storage_bytes are ignored); periodic lattices without a
  * Higgs-family field only (otherwise GFT_E_UNSUPPORTED). */
 int gft_observe_static(const gft_config* cfg, const float* d_scalars, const float* d_vectors, int time_iter,
@@ -256,6 +258,15 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
  * GFT_E_UNSUPPORTED when the lattice does not divide into the tile or carries a
  * Higgs-family field (one thread per site serves those). */
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
+
+/* Diagnostic with no reference counterpart: the time limit, in nanoseconds, of
+ * the tiled kernel's waits for its staged planes (0 restores the default, 2 s).
+ * When a wait gives up, the tile still waits, with the 2 s bound, for its copies
+ * in flight, then the step returns GFT_E_TIMEOUT and the fields are invalid
+ * until the next upload.  A limit below 1 us makes each wait a single
+ * non-blocking test, which fails whenever the copy has not yet landed: a way to
+ * exercise that error path with copies that do complete. */
+int gft_set_wait_limit(gft_handle* h, unsigned long long ns);
 
 /* Diagnostic with no reference counterpart: evaluates the library's own
  * sin/cos/asin (range-reduced series used by the throughput forms) against

@@ -11,6 +11,7 @@ mounted:  ``sh oracle/build_ref.sh && python tests/golden/make_golden.py``
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import sys
@@ -67,6 +68,48 @@ CASES = {
 }
 
 
+# Benchmark configuration 1 at its own size (SM 32^3, identity links, Higgs N(0, 0.1^2), analysers
+# every 10 steps): too large for a field fixture, so the reference's final fields are kept as a
+# SHA-256 digest of their bytes (both levels, reference layout) next to the analysers' raw sums.
+DIGESTS = {
+    "config1_sm_32": (dict(model=orc.MODEL_SM, nx=32, ny=32, nz=32, energy_every=10, gauss_every=10),
+                      dict(seed=7, mean=[0.0] * 8, sigma=[0.1] * 8), 10, ("f32", "f64")),
+}
+
+
+def field_digest(sc: np.ndarray, ve: np.ndarray) -> str:
+    """SHA-256 of the scalar then the vector array bytes (C order)."""
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(sc).tobytes())
+    h.update(np.ascontiguousarray(ve).tobytes())
+    return h.hexdigest()
+
+
+def make_digest(name: str) -> None:
+    pover, icover, nt, storages = DIGESTS[name]
+    p = orc.Params(**pover)
+    ic = orc.ICSpec(**icover)
+    out = {"params": p.__dict__, "ic": ic.__dict__, "nt": nt, "runs": {}}
+    for st in storages:
+        fp64 = st == "f64"
+        dtype = np.float64 if fp64 else np.float32
+        sc, ve = orc.init_fields(p, ic, dtype)
+        ic_digest = field_digest(sc, ve)
+        rs, rv, rows, _ = refrun.run(p, sc, ve, nt, fp64=fp64)
+        out["runs"][st] = {
+            "generator": "oracle/_ref/" + ("ref64" if fp64 else "ref32"),
+            "ic_sha256": ic_digest, "fields_sha256": field_digest(rs, rv),
+            "rows": [{"time_iter": r["time_iter"], "has_energy": r["has_energy"], "has_gauss": r["has_gauss"],
+                      "ref_energy": r["ref_energy"], "ref_gauss_int": r["ref_gauss_int"],
+                      "gauss_max": r["gauss_max"]} for r in rows],
+        }
+    path = os.path.join(HERE, f"{name}_digest.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+        f.write("\n")
+    print("wrote", os.path.relpath(path, ROOT), os.path.getsize(path), "bytes")
+
+
 def make(name: str) -> None:
     pover, icover, nt, storages = CASES[name]
     p = orc.Params(**pover)
@@ -94,5 +137,8 @@ def make(name: str) -> None:
 if __name__ == "__main__":
     if not (refrun.available(False) and refrun.available(True)):
         sys.exit("reference binaries missing: run sh oracle/build_ref.sh first")
-    for n in (sys.argv[1:] or CASES):
-        make(n)
+    for n in (sys.argv[1:] or list(CASES) + list(DIGESTS)):
+        if n in DIGESTS:
+            make_digest(n)
+        else:
+            make(n)

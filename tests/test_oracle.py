@@ -130,3 +130,40 @@ def test_live_reference_matches_oracle_when_built(oracle_mod):
             rs, rv, _, _ = refrun.run(p, sc0, ve0, 4, fp64=dtype == np.float64)
             np.testing.assert_array_equal(sc, rs)
             np.testing.assert_array_equal(ve, rv)
+
+
+def test_oracle_reproduces_reference_at_config1_size(oracle_mod):
+    """Benchmark configuration 1 at its own size (SM 32^3, identity links, Higgs
+    N(0, 0.1^2), 10 steps, analysers every 10): the oracle's fields hash to the
+    reference's (tests/golden/config1_sm_32_digest.json, made by the reference
+    binaries) and its analyser sums equal the reference's, in both storages."""
+    import hashlib
+    import json
+
+    from conftest import GOLDEN_DIR
+    with open(os.path.join(GOLDEN_DIR, "config1_sm_32_digest.json")) as f:
+        d = json.load(f)
+    p = oracle_mod.Params(**d["params"])
+    ic = oracle_mod.ICSpec(**d["ic"])
+
+    def digest(sc, ve):
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(sc).tobytes())
+        h.update(np.ascontiguousarray(ve).tobytes())
+        return h.hexdigest()
+
+    for st, run in d["runs"].items():
+        dtype = np.float64 if st == "f64" else np.float32
+        sc, ve = oracle_mod.init_fields(p, ic, dtype)
+        assert digest(sc, ve) == run["ic_sha256"], st
+        rows, warn = oracle_mod.evolve(p, sc, ve, d["nt"])
+        assert warn == 0
+        assert digest(sc, ve) == run["fields_sha256"], st
+        assert len(rows) == len(run["rows"])
+        for r, g in zip(rows, run["rows"]):
+            assert r["time_iter"] == g["time_iter"]
+            if g["has_energy"]:
+                assert r["ref_energy"] == g["ref_energy"]
+            if g["has_gauss"]:
+                assert r["ref_gauss_int"] == g["ref_gauss_int"]
+                assert r["gauss_max"] == g["gauss_max"]

@@ -21,10 +21,15 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _state(model, shape, steps):
+# 2HDM couplings beyond the default: the U(N/2)-breaking terms and the energy offset
+COUPLED_2HDM = dict(m12i=0.03, l5i=0.02, l6i=-0.015, l7i=0.01, l6r=0.012, l7r=-0.008, apply_norm=1,
+                    energy_offset=0.37)
+
+
+def _state(model, shape, steps, extra=None):
     from gftevolver_b200 import Evolver, InitialData, LatticeParams
     nx, ny, nz = shape
-    p = LatticeParams(model=model, nx=nx, ny=ny, nz=nz, energy_every=1)
+    p = LatticeParams(model=model, nx=nx, ny=ny, nz=nz, energy_every=1, **(extra or {}))
     ic = InitialData(seed=4242, mean=[1.0 if model == 1 else 0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1,
                      eps_sigma=0.1)
     with Evolver(p, form="mixed") as ev:
@@ -39,13 +44,14 @@ def _state(model, shape, steps):
 KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "plaq_su2", "plaq_u1", "phi_sq")
 
 
-@pytest.mark.parametrize("model,shape", [(1, (24, 16, 32)), (2, (12, 10, 18))], ids=["sm", "2hdm"])
-def test_observe_static_matches_observe_twice(model, shape):
+@pytest.mark.parametrize("model,shape,extra", [(1, (24, 16, 32), None), (2, (12, 10, 18), None),
+                                               (2, (10, 12, 14), COUPLED_2HDM)], ids=["sm", "2hdm", "2hdm_coupled"])
+def test_observe_static_matches_observe_twice(model, shape, extra):
     import torch
     from gftevolver_b200 import _lib
     from gftevolver_b200.evolver import make_config
     lib = _lib.load()
-    p, ref, sc, ve, ti = _state(model, shape, 3)
+    p, ref, sc, ve, ti = _state(model, shape, 3, extra)
     cfg = make_config(p, "mixed", 0)
     d_sc = torch.from_numpy(sc).cuda()
     d_ve = torch.from_numpy(ve).cuda()
@@ -75,3 +81,17 @@ def test_observe_static_rejects_lattices_beyond_its_scratch():
     rc = lib.gft_observe_static(ctypes.byref(cfg), dummy, dummy, 0, dummy, None)
     assert rc == _lib.GFT_E_UNSUPPORTED
     assert "67108864" in _lib.last_error()
+
+
+def test_observe_static_rejects_an_invalid_configuration_with_a_message():
+    import dataclasses
+
+    from gftevolver_b200 import LatticeParams, _lib
+    from gftevolver_b200.evolver import make_config
+    lib = _lib.load()
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the configuration check comes first
+    for bad in (dict(dx=0.0), dict(dt=float("nan")), dict(nx=0)):
+        cfg = make_config(dataclasses.replace(LatticeParams(nx=8, ny=8, nz=8), **bad), "mixed", 0)
+        rc = lib.gft_observe_static(ctypes.byref(cfg), dummy, dummy, 0, dummy, None)
+        assert rc == _lib.GFT_E_INVALID, bad
+        assert _lib.last_error().startswith("gft_observe_static: "), _lib.last_error()
