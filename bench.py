@@ -61,10 +61,15 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=None, help="steps for the FP64 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--kernel", choices=["auto", "global", "tiled"], default="auto",
+    ap.add_argument("--exchange", choices=["library", "python"], default="library",
+                    help="x-slabs (--slab, N > 1): ghost-plane exchange posted by the library over NCCL and "
+                         "overlapped with the interior planes, or a per-step callback through torch.distributed")
+    ap.add_argument("--kernel", choices=["auto", "global", "tiled", "pair"], default="auto",
                     help="step kernel of the throughput forms")
     ap.add_argument("--tile", type=int, default=0, help="tiled kernel: tile shape index (0: 8x32, 1: 4x32, 2: 4x16, 3: 16x16)")
     ap.add_argument("--march", type=int, default=32, help="tiled kernel: planes per CTA along x")
+    ap.add_argument("--precision-table", type=int, default=0,
+                    help="steps of a run of every form (mixed, ref32, fp64) against the FP64 form (0: skip)")
     ap.add_argument("--precision-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 precision run (0: skip)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison run")
@@ -308,6 +313,56 @@ def precision_report(p, ic, steps: int, device: int) -> dict:
     }
 
 
+def precision_table(p, ic, steps: int, device: int) -> dict:
+    """Every form on the same device initial data for `steps` steps, against the FP64 form:
+    storage bytes per site-update, the largest Gauss residual (over sites, constraints and
+    logging steps), the largest relative energy difference from the FP64 form at the logging
+    steps, the largest |stored word - FP64| after the run, and site-updates/s of the run.
+
+    ref32 is the reference's own design: float storage with every per-site operation in FP64
+    (renormalisation and momentum accumulation included), in the reference's order."""
+    import torch
+
+    from gftevolver_b200 import Evolver
+
+    out, fields, rows = {}, {}, {}
+    for form in ("fp64", "mixed", "ref32"):
+        ev = Evolver(p, form=form, device=device)
+        ev.init_fields(ic)
+        st = torch.cuda.ExternalStream(ev.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        rows[form] = ev.evolve(steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        dt = torch.float64 if form == "fp64" else torch.float32
+        sc = torch.empty((2, p.nx, p.ny, p.nz, p.nsc), dtype=dt, device=f"cuda:{device}")
+        ve = torch.empty((2, p.nx, p.ny, p.nz, p.nve), dtype=dt, device=f"cuda:{device}")
+        ev.download_device(sc.data_ptr(), ve.data_ptr(), form == "fp64")
+        torch.cuda.synchronize()
+        ev.close()
+        if form == "fp64":
+            fields["fp64"] = (sc, ve)
+        else:
+            dev = max((sc.double() - fields["fp64"][0]).abs().max().item(),
+                      (ve.double() - fields["fp64"][1]).abs().max().item())
+            del sc, ve
+        g = [max(r["gauss_max"]) for r in rows[form] if r["has_gauss"]]
+        out[form] = {"bytes_per_site_update": B_ALG[("sm" if p.model == 1 else "2hdm", 8 if form == "fp64" else 4)],
+                     "gauss_max": max(g) if g else None, "value": p.nsite * steps / (ms / 1e3),
+                     "field_max_abs_dev_vs_fp64": 0.0 if form == "fp64" else dev}
+    del fields
+    torch.cuda.empty_cache()
+    e64 = [r["energy"] for r in rows["fp64"] if r["has_energy"]]
+    for form in out:
+        e = [r["energy"] for r in rows[form] if r["has_energy"]]
+        out[form]["energy_vs_fp64_rel"] = max(abs(a - b) / abs(b) for a, b in zip(e, e64))
+        out[form]["energy_drift_rel"] = max(abs(a - e[0]) for a in e) / abs(e[0])
+    return {"steps": steps, "lattice": [p.nx, p.ny, p.nz], "log_every": LOG_EVERY, "forms": out}
+
+
 # ---------------------------------------------------------------------------
 # Ensemble: 64 SM realisations of uneven sizes in one persistent launch per step
 # ---------------------------------------------------------------------------
@@ -455,7 +510,7 @@ def main():
     sbytes = 8 if form in ("fp64", "ref64") else 4
     balg = B_ALG[(args.model, sbytes)]
 
-    kind = {"auto": 0, "global": 1, "tiled": 2}[args.kernel]
+    kind = {"auto": 0, "global": 1, "tiled": 2, "pair": 3}[args.kernel]
 
     def make_runner(form_):
         """N = 1: the whole lattice.  N > 1: this rank's x-slab of an (N * n) x n x n lattice
@@ -464,7 +519,8 @@ def main():
             import dataclasses
 
             from gftevolver_b200.slab import SlabEvolver
-            s = SlabEvolver(dataclasses.replace(p, nx=p.nx * world), form=form_, device=local)
+            s = SlabEvolver(dataclasses.replace(p, nx=p.nx * world), form=form_, device=local,
+                            exchange=args.exchange)
             return s, s.local
         e = Evolver(p, form=form_, device=local)
         return e, e
@@ -560,6 +616,9 @@ def main():
     precision = None
     if args.precision_steps > 0 and form == "mixed" and world == 1:
         precision = precision_report(p, ic, args.precision_steps, local)
+    ptable = None
+    if args.precision_table > 0 and world == 1:
+        ptable = precision_table(p, ic, args.precision_table, local)
     ensemble = None
     if args.ensemble_steps > 0 and world == 1:
         ensemble = ensemble_report(args.ensemble_steps, local)
@@ -573,13 +632,15 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:  # the CPU baselines belong to the N = 1 line
         try:
-            cpu = cpu_reference_throughput(args.model, 40, 10, host_cores())
+            # 52^3 x 20 steps per process: about 10 s of each core's time at the reference's ~2.7e5
+            # site-updates/s per core
+            cpu = cpu_reference_throughput(args.model, 52, 20, host_cores())
         except Exception as ex:  # the baseline is reported, not required
             cpu = {"value": None, "error": str(ex)}
         if fp64 is not None:
             # the reference's double-storage build beside the FP64 form
             try:
-                fp64["cpu_reference"] = cpu_reference_throughput(args.model, 40, 10, host_cores(), fp64=True)
+                fp64["cpu_reference"] = cpu_reference_throughput(args.model, 52, 20, host_cores(), fp64=True)
             except Exception as ex:
                 fp64["cpu_reference"] = {"value": None, "error": str(ex)}
     line = {
@@ -599,8 +660,11 @@ def main():
                    "lattice": [p.nx, p.ny, p.nz], "form": form, "log_every": LOG_EVERY,
                    "l2": "inputs larger than L2 (state %.2f GB per level pair)" % (2 * p.nsite * (15 + p.nsc) * sbytes / 1e9),
                    "parallelism": (f"x-slabs x{world}: lattice {world * p.nx}x{p.ny}x{p.nz}, one ghost plane per "
-                                   "side exchanged over NCCL send/recv after every step, FP64 all-reduce of "
-                                   "the analyser rows") if world > 1 else "single GPU",
+                                   "side exchanged over NCCL send/recv every step ("
+                                   + ("posted by the library, overlapped with the interior planes"
+                                      if args.exchange == "library" else "after the step, from a callback")
+                                   + "), FP64 all-reduce of the analyser rows") if world > 1 else
+                                  ("single GPU, one x-slab exchanging with itself" if args.slab else "single GPU"),
                    "kernel": args.kernel, "tile": args.tile, "march": args.march},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": kernel_name,
@@ -611,6 +675,7 @@ def main():
         "e2e": e2e,
         "cpu_baseline": cpu,
         "precision": precision,
+        "precision_table": ptable,
         "ensemble": ensemble,
         "configs": configs,
         "analyser_rows": len(rows),

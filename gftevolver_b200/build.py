@@ -31,6 +31,7 @@ SOURCES = [
     ("gft_aux_kernels.cu", []),
     ("gft_static_observe.cu", []),
     ("gft_ensemble.cu", []),
+    ("gft_slab_nccl.cu", []),
     ("gft_abi.cu", []),
 ]
 

@@ -70,10 +70,11 @@ struct gft_handle {
     std::string err;
     size_t dev_bytes = 0;
     // step kernel selection for the throughput forms
-    int kernel_kind = 0;    // 0 auto, 1 global-memory kernel, 2 tiled (TMA) kernel
+    int kernel_kind = 0;    // 0 auto, 1 global-memory kernel, 2 tiled (TMA) kernel, 3 tiled with two
+                            // sites per thread on plain steps (SM)
     int tile_variant = 0;   // tiled: index into the built tile shapes
     int march = 32;         // tiled: planes per CTA along x
-    unsigned long long wait_limit_ns = 0;  // gft_set_wait_limit (0: the 2 s default)
+    unsigned wait_limit_ns = 0;  // gft_set_wait_limit (0: the 2 s default)
     bool tiled_ready = false;
     TMaps tm[2];   // staged "now" planes (with halo), per level
     TMaps tp[2];   // past-level L2 prefetch boxes (no halo), per level
@@ -83,6 +84,12 @@ struct gft_handle {
     int x_offset = 0, nx_global = 0;
     gft_exchange_fn exchange = nullptr;
     void* exchange_user = nullptr;
+    // gft_set_slab_nccl: the ghost-plane exchange posted by gft_evolve itself over
+    // NCCL, on comm_stream, overlapped with the interior planes
+    SlabComm* comm = nullptr;
+    cudaStream_t comm_stream = nullptr;
+    cudaEvent_t ev_bound = nullptr, ev_comm = nullptr;
+    double comm_timeout_s = 300.0;
     // per-site analyser outputs (gft_local_fields)
     float* d_loc_e = nullptr;   // [nsite][6]
     float* d_loc_g = nullptr;   // [nsite][neq]
@@ -256,6 +263,14 @@ bool use_tiled(const gft_handle* h, const StepParams& P)
     return tiled_supported(P, h->tile_variant);
 }
 
+// Plain steps of the SM mixed form with two sites per thread (kernel kind 3):
+// periodic lattices (no Fixed faces) in a tile shape the paired kernel is built for.
+bool use_pair(const gft_handle* h, const StepParams& P)
+{
+    return h->kernel_kind == 3 && h->cfg.model == GFT_MODEL_SM && P.fixed_axes == 0 &&
+           tiled_pair_tile(h->tile_variant);
+}
+
 int step_blocks(const gft_handle* h, const StepParams& P)
 {
     if (h->cfg.form == GFT_FORM_REF) return ref_launch_blocks(P);
@@ -264,9 +279,11 @@ int step_blocks(const gft_handle* h, const StepParams& P)
 }
 
 // `tn` is the index (0 or 1) of the handle level passed as `now`.
+// xa, xn: planes [xa, xa + xn) only (the tiled kernels; xn < 0: every plane);
+// st: the stream of a tiled launch (null: the handle's).
 template <class S>
 cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelPtrs<S>& now, const LevelPtrs<S>& past,
-                        bool energy)
+                        bool energy, int xa = 0, int xn = -1, cudaStream_t st = nullptr)
 {
     const int model = h->cfg.model;
     if (h->cfg.form == GFT_FORM_REF) {
@@ -275,11 +292,15 @@ cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelP
     }
     if constexpr (sizeof(S) == 4) {
         if (use_tiled(h, P)) {
+            cudaStream_t s = st ? st : h->stream;
+            if (!energy && use_pair(h, P))
+                return launch_tiled_pair_step(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
+                                              h->d_status, s, xa, xn);
             if (model == GFT_MODEL_SM)
                 return launch_tiled_step<S, kModelSM>(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
-                                                      h->d_status, h->d_part_e, energy, h->stream);
+                                                      h->d_status, h->d_part_e, energy, s, xa, xn);
             return launch_tiled_step<S, kModel2HDM>(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
-                                                    h->d_status, h->d_part_e, energy, h->stream);
+                                                    h->d_status, h->d_part_e, energy, s, xa, xn);
         }
     }
     if (model == GFT_MODEL_SM)
@@ -489,6 +510,11 @@ void gft_destroy(gft_handle* h)
     if (!h) return;
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->comm_stream) cudaStreamSynchronize(h->comm_stream);
+    slab_comm_destroy(h->comm, false);
+    if (h->ev_bound) cudaEventDestroy(h->ev_bound);
+    if (h->ev_comm) cudaEventDestroy(h->ev_comm);
+    if (h->comm_stream) cudaStreamDestroy(h->comm_stream);
     for (auto& x : h->ev)
         if (x) cudaEventDestroy(x);
     for (int t = 0; t < 2; t++)
@@ -634,6 +660,64 @@ void fill_row(gft_observables* r, int time_iter, bool e, bool g, const double* v
     }
 }
 
+// The four planes of every field array of `level` that one slab exchange moves.
+int fill_slab_planes(gft_handle* h, int level, SlabPlanes& pl)
+{
+    size_t b[kMaxPlaneArrays];
+    int n = gft_level_planes(h, level, h->x_begin, pl.send_lo, pl.bytes, kMaxPlaneArrays);
+    if (n < 0) return n;
+    if (gft_level_planes(h, level, h->x_end - 1, pl.send_hi, b, kMaxPlaneArrays) < 0 ||
+        gft_level_planes(h, level, h->x_begin - 1, pl.recv_lo, b, kMaxPlaneArrays) < 0 ||
+        gft_level_planes(h, level, h->x_end, pl.recv_hi, b, kMaxPlaneArrays) < 0)
+        return GFT_E_INVALID;
+    pl.n = n;
+    return GFT_OK;
+}
+
+// A plain step of an x-slab with the exchange in the library (tiled kernels).
+// The first and the last x-chunk of own planes (march planes each, so that no
+// CTA pays the ring's start-up for fewer planes than usual) are computed on
+// comm_stream, created with the highest priority so that their CTAs are
+// scheduled first, and the two boundary planes are sent from there while the
+// interior chunks are computed concurrently on the handle's stream; the plane
+// sets are disjoint and all read only the "now" level, so the kernels may
+// overlap.  The handle's stream then waits for the exchange before anything
+// reads the ghost planes.  `launches` counts the step kernels; `why` receives
+// an NCCL error.
+template <class S>
+cudaError_t split_slab_step(gft_handle* h, const StepParams& P, int tn, const LevelPtrs<S>* lv, int& launches,
+                            int& rc, std::string& why)
+{
+    const int tp = 1 - tn;
+    const int a = h->x_begin, b = h->x_end, nloc = b - a;  // own planes [a, b)
+    // everything before this step (the previous step's writes and exchange) precedes the boundary planes
+    cudaError_t err = cudaEventRecord(h->ev_bound, h->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(h->comm_stream, h->ev_bound, 0);
+    if (err != cudaSuccess) return err;
+    const int m = h->march;  // boundary chunks [a, a + m) and [b - m, b); interior [a + m, b - m)
+    const bool interior = nloc > 2 * m;
+    if (!interior) {
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], false, a, nloc, h->comm_stream);
+        launches += 1;
+    } else {
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], false, a, m, h->comm_stream);
+        if (err == cudaSuccess) err = launch_step<S>(h, P, tn, lv[tn], lv[tp], false, b - m, m, h->comm_stream);
+        launches += 2;
+    }
+    if (err != cudaSuccess) return err;
+    SlabPlanes pl;
+    rc = fill_slab_planes(h, tp, pl);
+    if (rc == GFT_OK) rc = slab_comm_exchange(h->comm, pl, h->comm_stream, why);
+    if (rc != GFT_OK) return cudaSuccess;
+    err = cudaEventRecord(h->ev_comm, h->comm_stream);
+    if (err == cudaSuccess && interior) {
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], false, a + m, nloc - 2 * m);
+        launches += 1;
+    }
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(h->stream, h->ev_comm, 0);
+    return err;
+}
+
 template <class S>
 int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observables* rows, int max_rows, int* n_rows)
 {
@@ -669,8 +753,19 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         if (gl) h->loc_g_step = ti;
         const bool prof = h->profile && h->ev_used < kMaxProfiled;
         if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
-        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e || el);
-        h->launches += 1 + (e ? finalize_launches(step_blocks(h, P), true) : 0) + ((g || gl) ? 1 : 0) +
+        // an x-slab with the exchange in the library overlaps it with the interior on plain steps
+        const bool split = h->comm && !(e || el) && sizeof(S) == 4 && use_tiled(h, P) && h->x_begin == 1 &&
+                           h->x_end == c.nx - 1;
+        int nstep = 1, crc = GFT_OK;
+        std::string cwhy;
+        if (split) {
+            nstep = 0;
+            err = split_slab_step<S>(h, P, tn, lv, nstep, crc, cwhy);
+            if (crc != GFT_OK) return h->fail(crc, "gft_evolve: " + cwhy);
+        } else {
+            err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e || el);
+        }
+        h->launches += nstep + (e ? finalize_launches(step_blocks(h, P), true) : 0) + ((g || gl) ? 1 : 0) +
                        (g ? finalize_launches(gauss_blocks(h, P), true) : 0);
         if (prof) {
             cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
@@ -680,6 +775,13 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
         double* out = h->d_rows + (size_t)row * kRowSlots;
         if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->d_mid,
                                          h->stream);
+        if (h->comm && !split && err == cudaSuccess) {
+            // logging steps (and forms without the split): the exchange after the whole step
+            SlabPlanes pl;
+            int xrc = fill_slab_planes(h, tp, pl);
+            if (xrc == GFT_OK) xrc = slab_comm_exchange(h->comm, pl, h->stream, cwhy);
+            if (xrc != GFT_OK) return h->fail(xrc, "gft_evolve: " + cwhy);
+        }
         if (h->exchange && err == cudaSuccess) {
             // refresh the ghost planes of the level just written before anything reads them
             const int xr = h->exchange(h, tp, h->exchange_user);
@@ -707,6 +809,12 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
                                        cudaMemcpyDeviceToHost, h->stream);
     if (err == cudaSuccess) err = cudaMemcpyAsync(&status, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
+    if (err == cudaSuccess && h->comm) {
+        // bounded: a peer that is gone must not hold this rank for good
+        std::string why;
+        const int wrc = slab_comm_wait(h->comm, h->stream, h->comm_timeout_s, why);
+        if (wrc != GFT_OK) return h->fail(wrc, "gft_evolve: " + why);
+    }
     if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
     if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve");
     if (status & 8u) return h->fail(GFT_E_TIMEOUT, "gft_evolve: a device wait timed out (tensor-copy barrier)");
@@ -823,22 +931,26 @@ int gft_observe(gft_handle* h, gft_observables* row)
 int gft_set_wait_limit(gft_handle* h, unsigned long long ns)
 {
     if (!h) return GFT_E_INVALID;
-    h->wait_limit_ns = ns;
+    if (ns > 4000000000ull) return h->fail(GFT_E_INVALID, "gft_set_wait_limit: the limit is at most 4 s");
+    h->wait_limit_ns = (unsigned)ns;
     return GFT_OK;
 }
 
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
 {
     if (!h) return GFT_E_INVALID;
-    if (kind < 0 || kind > 2 || march < 1) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad kind or march");
+    if (kind < 0 || kind > 3 || march < 1) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad kind or march");
+    if (kind == 3 && (h->cfg.model != GFT_MODEL_SM || h->cfg.fixed_axes != 0 || !tiled_pair_tile(tile)))
+        return h->fail(GFT_E_UNSUPPORTED,
+                       "gft_set_kernel: two sites per thread serve the periodic SM model in 8 x 32 or 16 x 16 tiles");
     if (kind == 1) {
         h->kernel_kind = 1;
         return GFT_OK;
     }
-    if (kind == 2 && h->hf != kHfNone)
+    if (kind >= 2 && h->hf != kHfNone)
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel has no Higgs-family field");
     if (h->cfg.form != GFT_FORM_MIXED) {
-        if (kind == 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
+        if (kind >= 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
         h->kernel_kind = 0;
         return GFT_OK;
     }
@@ -946,9 +1058,45 @@ int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_
     return GFT_OK;
 }
 
+int gft_nccl_unique_id(unsigned char* id)
+{
+    if (!id) return GFT_E_INVALID;
+    std::string why;
+    const int rc = nccl_unique_id(id, why);
+    if (rc != GFT_OK) set_global_error("gft_nccl_unique_id: " + why);
+    return rc;
+}
+
+int gft_set_slab_nccl(gft_handle* h, const unsigned char* id, int nranks, int rank, double timeout_s)
+{
+    if (!h) return GFT_E_INVALID;
+    if (!id || nranks < 1 || rank < 0 || rank >= nranks || !(timeout_s > 0))
+        return h->fail(GFT_E_INVALID, "gft_set_slab_nccl: need an id, 0 <= rank < nranks and a positive timeout");
+    if (h->x_end == 0 || h->x_begin != 1 || h->x_end != h->cfg.nx - 1)
+        return h->fail(GFT_E_STATE, "gft_set_slab_nccl: call gft_set_slab first, with one ghost plane on each side");
+    if (h->exchange) return h->fail(GFT_E_STATE, "gft_set_slab_nccl: an exchange callback is set");
+    if (h->comm) return h->fail(GFT_E_STATE, "gft_set_slab_nccl: the exchange is already set up");
+    cudaSetDevice(h->cfg.device);
+    cudaError_t e = cudaSuccess;
+    int prio_lo = 0, prio_hi = 0;  // the boundary planes' kernels ahead of the interior's CTAs
+    if (!h->comm_stream && (e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi)) == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&h->comm_stream, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess && !h->ev_bound) e = cudaEventCreateWithFlags(&h->ev_bound, cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->ev_comm) e = cudaEventCreateWithFlags(&h->ev_comm, cudaEventDisableTiming);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_set_slab_nccl");
+    std::string why;
+    SlabComm* c = nullptr;
+    const int rc = slab_comm_create(id, nranks, rank, &c, why);
+    if (rc != GFT_OK) return h->fail(rc, "gft_set_slab_nccl: " + why);
+    h->comm = c;
+    h->comm_timeout_s = timeout_s;
+    return GFT_OK;
+}
+
 int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user)
 {
     if (!h) return GFT_E_INVALID;
+    if (fn && h->comm) return h->fail(GFT_E_STATE, "gft_set_exchange: the NCCL exchange of gft_set_slab_nccl is set");
     h->exchange = fn;
     h->exchange_user = user;
     return GFT_OK;
@@ -985,7 +1133,8 @@ const char* gft_step_kernel_name(const gft_handle* h)
     if (!h) return "";
     if (h->cfg.form == GFT_FORM_REF) return "ref_step_kernel";
     const StepParams P = make_params(h, 0, false);
-    return use_tiled(h, P) ? "tiled_step_kernel" : "fast_step_kernel";
+    if (!use_tiled(h, P)) return "fast_step_kernel";
+    return use_pair(h, P) ? "tiled_pair_kernel" : "tiled_step_kernel";
 }
 
 }  // extern "C"

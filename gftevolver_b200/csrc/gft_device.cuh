@@ -79,13 +79,13 @@ struct StepParams {
     // Double_SO_N
     double m1, m2, l1, l2, l3, m12r, l4p5, l6r, l7r, m12i, l4m5, l5i, l6i, l7i;
     int break_son, break_uhalfn, apply_norm;
+    unsigned wait_limit_ns;  // limit of the tiled kernels' plane waits (0: 2 s); the drain after a
+                             // failed wait keeps the 2 s bound (placed in what was padding)
     double energy_offset;
     int store_energy;       // logging step: renormalise as the reference does and accumulate energies
     int obs_x0, obs_x1;     // planes whose sites count in observables, Gauss residuals and warnings
                             // (all planes, except on an x-slab with ghost planes)
     int fixed_axes;         // bit a: the two faces of axis a are Fixed (frozen, not evolved)
-    unsigned long long wait_limit_ns;  // limit of the tiled kernels' plane waits (0: 2 s); the drain
-                                       // after a failed wait keeps the 2 s bound
 };
 
 // The mixed form's per-site constants in float, precomputed on the host and

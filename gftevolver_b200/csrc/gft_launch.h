@@ -47,8 +47,16 @@ int tiled_blocks(const StepParams& P, int variant, int lx);
 template <class S, int MODEL>
 cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
-                              bool energy, cudaStream_t stream);
-constexpr int kTiledVariants = 4;  // 8x32, 4x32, 4x16 (TY x TZ)
+                              bool energy, cudaStream_t stream, int xa = 0, int xn = -1);
+// The SM mixed form's plain steps with two sites per thread (rows ty and ty + TY/2
+// of the tile) in paired FP32 arithmetic; same tiles, ring and tensor maps.
+cudaError_t launch_tiled_pair_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+                                   const LevelPtrs<float>& now, const LevelPtrs<float>& past, int variant, int lx,
+                                   unsigned* status, cudaStream_t stream, int xa = 0, int xn = -1);
+constexpr int kTiledVariants = 4;  // 8x32, 4x32, 4x16, 16x16 (TY x TZ)
+// Tile shapes the two-sites-per-thread kernel is built for (8 x 32 and 16 x 16:
+// 128 threads per CTA, two CTAs per SM).
+inline bool tiled_pair_tile(int variant) { return variant == 0 || variant == 3; }
 inline void tiled_tile(int variant, int& ty, int& tz)
 {
     static const int shapes[4][2] = {{8, 32}, {4, 32}, {4, 16}, {16, 16}};
@@ -56,6 +64,27 @@ inline void tiled_tile(int variant, int& ty, int& tz)
     ty = shapes[v][0];
     tz = shapes[v][1];
 }
+
+// x-slab ghost-plane exchange over NCCL (gft_slab_nccl.cu).
+constexpr int kNcclIdBytes = 128;
+constexpr int kMaxPlaneArrays = 11;  // field arrays of a level at most (2HDM with a Higgs-family SU(2))
+struct SlabComm;
+// Plane ranges of one exchange: per field array, the first and last own planes
+// (sent left and right) and the two ghost planes (received from right and left).
+struct SlabPlanes {
+    int n = 0;
+    void* send_lo[kMaxPlaneArrays];
+    void* send_hi[kMaxPlaneArrays];
+    void* recv_lo[kMaxPlaneArrays];
+    void* recv_hi[kMaxPlaneArrays];
+    size_t bytes[kMaxPlaneArrays];
+};
+int nccl_unique_id(unsigned char* out, std::string& why);
+int slab_comm_create(const unsigned char* id, int nranks, int rank, SlabComm** out, std::string& why);
+void slab_comm_destroy(SlabComm* c, bool abort);
+int slab_comm_exchange(SlabComm* c, const SlabPlanes& pl, cudaStream_t stream, std::string& why);
+int slab_comm_wait(SlabComm* c, cudaStream_t stream, double seconds, std::string& why);
+bool slab_comm_alive(const SlabComm* c);
 
 // Auxiliary kernels (gft_aux_kernels.cu).
 // The reference record has 3 x 5 link words per site, 3 x 6 with a Higgs-family

@@ -5,6 +5,7 @@
 
 #include "gft_device.cuh"
 #include "gft_launch.h"
+#include "gft_pair_body.cuh"
 #include "gft_tiled_tile.cuh"
 
 namespace gft {
@@ -19,7 +20,7 @@ template <class S, int MODEL, int TY, int TZ, bool ENERGY>
 __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(const __grid_constant__ TMaps maps,
                                                              const __grid_constant__ TMaps pmaps, StepParams P,
                                                              FConst F, LevelPtrs<S> now, LevelPtrs<S> past, int lx,
-                                                             unsigned* status, double* partials)
+                                                             int xa, int xn, unsigned* status, double* partials)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<S, TY, TZ, ND>;
@@ -42,10 +43,10 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
     for (int k = 0; k < kObsCount; k++) obs[k] = 0.0;
     unsigned warn = 0;
     RingPhase ring = {0u};
-    const int x0 = blockIdx.z * lx;
+    const int x0 = xa + blockIdx.z * lx;  // planes [xa, xa + xn) in chunks of lx
     constexpr bool STAGE = !ENERGY && HaloStage<S, TY, TZ, ND>::kUse;
     const bool ok = run_tile<S, MODEL, TY, TZ, ENERGY, LevelPtrs<S>, STAGE>(
-        maps, pmaps, P, F, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0, min(lx, P.nx - x0), smem, bars, ring,
+        maps, pmaps, P, F, now, past, blockIdx.y * TY, blockIdx.x * TZ, x0, min(lx, xa + xn - x0), smem, bars, ring,
         &s_abort, obs, warn, smem + HaloStage<S, TY, TZ, ND>::OFFSET);
     if (!ok && tid == 0) atomicOr(status, kErrTimeout);
 
@@ -54,6 +55,76 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(co
         const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         block_reduce_store<kObsCount>(obs, partials + (size_t)b * kObsCount, kObsCount);
     }
+    if (warn) atomicOr(status, warn);
+}
+
+// Both sites of a thread from a staged plane: the cell of site A (row ty) and
+// the cell TY/2 rows further (site B), as (A, B) pairs.
+template <int TY, int TZ>
+struct PairAcc {
+    using G = Geom<float, TY, TZ, 1>;
+    static constexpr int DQ = (TY / 2) * G::QP, DH = (TY / 2) * G::HP;
+    __device__ __forceinline__ static pair::Q2 ld2(const unsigned char* base, int cell)
+    {
+        const float4 a = reinterpret_cast<const float4*>(base)[cell];
+        const float4 b = reinterpret_cast<const float4*>(base)[cell + DQ];
+        return {make_float2(a.x, b.x), make_float2(a.y, b.y), make_float2(a.z, b.z), make_float2(a.w, b.w)};
+    }
+    __device__ __forceinline__ pair::Q2 q(int d, TRef r) const { return ld2(r.b + d * G::QB, r.cq); }
+    __device__ __forceinline__ pair::V th(int d, TRef r) const
+    {
+        const float* h = reinterpret_cast<const float*>(r.b + G::OFF_TH + d * G::HB);
+        return make_float2(h[r.ch], h[r.ch + DH]);
+    }
+    __device__ __forceinline__ pair::Q2 ph(TRef r) const { return ld2(r.b + G::OFF_PH, r.cq); }
+};
+
+// Plain steps of the SM mixed form with two sites per thread: the CTA's
+// TZ x TY/2 threads cover the TY x TZ tile, thread (tz, ty) rows ty and ty + TY/2,
+// with the plane ring, halo staging and bounded waits of the one-site kernel
+// (run_ring).  Two CTAs per SM: up to 255 registers per thread.
+template <int TY, int TZ>
+__global__ void __launch_bounds__(TY * TZ / 2, 2) tiled_pair_kernel(const __grid_constant__ TMaps maps,
+                                                                   const __grid_constant__ TMaps pmaps, StepParams P,
+                                                                   FConst F, LevelPtrs<float> now,
+                                                                   LevelPtrs<float> past, int lx, int xa, int xn,
+                                                                   unsigned* status)
+{
+    using G = Geom<float, TY, TZ, 1>;
+    using H = HaloStage<float, TY, TZ, 1>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::NBUF * G::BUF);
+    const int tz = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * TZ + tz;
+
+    __shared__ int s_abort;
+    if (tid == 0) {
+        s_abort = 0;
+        for (int b = 0; b < G::NBUF; b++) mbar_init(&bars[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int y0 = blockIdx.y * TY, z0 = blockIdx.x * TZ, x0 = xa + blockIdx.z * lx;
+    const int cq0 = (ty + 1) * G::QP + (tz + 1);
+    const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
+    const int y = y0 + ty, z = z0 + tz;
+    const int sb_off = (TY / 2) * P.nz;
+    pair::Carry2 carry;
+    carry.valid = false;
+    unsigned warn = 0;
+    RingPhase ring = {0u};
+    const bool ok = run_ring<float, TY, TZ, 1, LevelPtrs<float>, H::kUse>(
+        maps, pmaps, P, now, y0, z0, x0, min(lx, xa + xn - x0), smem, bars, ring, &s_abort, smem + H::OFFSET, tid,
+        [&](int i, const unsigned char* bm, const unsigned char* bc, const unsigned char* bp) {
+            const Stencil<TRef> n = plane_stencil<G::QP, G::HP>(bm, bc, bp, cq0, ch0);
+            const int x = x0 + i;
+            const int sa = (x * P.ny + y) * P.nz + z;
+            pair::site_step2(F, PairAcc<TY, TZ>{}, n, past, sa, sa + sb_off, carry, warn, counts(P, x));
+        });
+    if (!ok && tid == 0) atomicOr(status, kErrTimeout);
     if (warn) atomicOr(status, warn);
 }
 
@@ -132,28 +203,28 @@ int tiled_blocks(const StepParams& P, int variant, int lx)
 {
     int ty, tz;
     tiled_tile(variant, ty, tz);
-    return (P.nz / tz) * (P.ny / ty) * ((P.nx + lx - 1) / lx);
+    return (P.nz / tz) * (P.ny / ty) * ((P.nx + lx - 1) / lx);  // a launch over all planes
 }
 
 template <class S, int MODEL, int TY, int TZ>
 static cudaError_t launch_tiled_t(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
-                                  const LevelPtrs<S>& past, int lx, unsigned* status, double* partials, bool energy,
-                                  cudaStream_t stream)
+                                  const LevelPtrs<S>& past, int lx, int xa, int xn, unsigned* status, double* partials,
+                                  bool energy, cudaStream_t stream)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<S, TY, TZ, ND>;
     const dim3 block(TZ, TY, 1);
-    const dim3 grid(P.nz / TZ, P.ny / TY, (P.nx + lx - 1) / lx);
+    const dim3 grid(P.nz / TZ, P.ny / TY, (xn + lx - 1) / lx);
     if (energy) {
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, true>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
+        k<<<grid, block, G::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, xa, xn, status, partials);
     } else {
         using H = HaloStage<S, TY, TZ, ND>;
         constexpr int SMEM = H::kUse ? H::SMEM : G::SMEM;  // plain steps stage their wrapped halo cells
         auto k = tiled_step_kernel<S, MODEL, TY, TZ, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
-        k<<<grid, block, SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, status, partials);
+        k<<<grid, block, SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, xa, xn, status, partials);
     }
     return cudaGetLastError();
 }
@@ -161,23 +232,50 @@ static cudaError_t launch_tiled_t(const TMaps& maps, const TMaps& pmaps, const S
 template <class S, int MODEL>
 cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,
-                              bool energy, cudaStream_t stream)
+                              bool energy, cudaStream_t stream, int xa, int xn)
 {
+    if (xn < 0) xn = P.nx - xa;  // default: every plane from xa on
     switch (variant) {
-    case 0: return launch_tiled_t<S, MODEL, 8, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
-    case 1: return launch_tiled_t<S, MODEL, 4, 32>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
-    case 2: return launch_tiled_t<S, MODEL, 4, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
-    default: return launch_tiled_t<S, MODEL, 16, 16>(maps, pmaps, P, now, past, lx, status, partials, energy, stream);
+    case 0: return launch_tiled_t<S, MODEL, 8, 32>(maps, pmaps, P, now, past, lx, xa, xn, status, partials, energy, stream);
+    case 1: return launch_tiled_t<S, MODEL, 4, 32>(maps, pmaps, P, now, past, lx, xa, xn, status, partials, energy, stream);
+    case 2: return launch_tiled_t<S, MODEL, 4, 16>(maps, pmaps, P, now, past, lx, xa, xn, status, partials, energy, stream);
+    default: return launch_tiled_t<S, MODEL, 16, 16>(maps, pmaps, P, now, past, lx, xa, xn, status, partials, energy, stream);
     }
+}
+
+template <int TY, int TZ>
+static cudaError_t launch_pair_t(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+                                 const LevelPtrs<float>& now, const LevelPtrs<float>& past, int lx, int xa, int xn,
+                                 unsigned* status, cudaStream_t stream)
+{
+    using G = Geom<float, TY, TZ, 1>;
+    using H = HaloStage<float, TY, TZ, 1>;
+    constexpr int SMEM = H::kUse ? H::SMEM : G::SMEM;
+    const dim3 block(TZ, TY / 2, 1);
+    const dim3 grid(P.nz / TZ, P.ny / TY, (xn + lx - 1) / lx);
+    auto k = tiled_pair_kernel<TY, TZ>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    k<<<grid, block, SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, xa, xn, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tiled_pair_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+                                   const LevelPtrs<float>& now, const LevelPtrs<float>& past, int variant, int lx,
+                                   unsigned* status, cudaStream_t stream, int xa, int xn)
+{
+    if (xn < 0) xn = P.nx - xa;
+    // the 8 x 32 and 16 x 16 tiles (128 threads per CTA); tiled_pair_tile says which
+    if (variant == 3) return launch_pair_t<16, 16>(maps, pmaps, P, now, past, lx, xa, xn, status, stream);
+    return launch_pair_t<8, 32>(maps, pmaps, P, now, past, lx, xa, xn, status, stream);
 }
 
 template bool tiled_encode_maps<float>(const StepParams&, const LevelPtrs<float>&, int, int, int, bool, TMaps*);
 template bool tiled_encode_maps<double>(const StepParams&, const LevelPtrs<double>&, int, int, int, bool, TMaps*);
 template cudaError_t launch_tiled_step<float, kModelSM>(const TMaps&, const TMaps&, const StepParams&,
                                                         const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
-                                                        unsigned*, double*, bool, cudaStream_t);
+                                                        unsigned*, double*, bool, cudaStream_t, int, int);
 template cudaError_t launch_tiled_step<float, kModel2HDM>(const TMaps&, const TMaps&, const StepParams&,
                                                           const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
-                                                          unsigned*, double*, bool, cudaStream_t);
+                                                          unsigned*, double*, bool, cudaStream_t, int, int);
 
 }  // namespace gft

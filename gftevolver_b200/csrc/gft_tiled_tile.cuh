@@ -82,16 +82,14 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 // Wait for phase `parity` of `bar`; false after `limit_ns` (0: 2 s).  A limit
 // below 1 us is one non-blocking test (the diagnostic of gft_set_wait_limit:
 // it fails whenever the copy has not landed yet).
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
-                                                  unsigned long long limit_ns = 0)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned limit_ns = 0)
 {
-    if (limit_ns != 0 && limit_ns < 1000ull) return mbar_test_wait(bar, parity);
-    const unsigned long long lim = limit_ns ? limit_ns : kWaitLimitNs;
+    if (limit_ns - 1u < 999u) return mbar_test_wait(bar, parity);  // 1 <= limit < 1 us
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer_ns() - t0 > lim) return false;
+        if (globaltimer_ns() - t0 > (limit_ns ? (unsigned long long)limit_ns : kWaitLimitNs)) return false;
     }
 }
 
@@ -354,25 +352,25 @@ struct RingPhase {
     unsigned bits;
 };
 
-// Evolves one tile (planes x0 .. x0+nloc-1 of columns y0.., z0..) by one step.
-// smem: NBUF plane buffers followed by NBUF initialised mbarriers; s_abort: a
-// shared flag that is 0 on entry.  Returns false (on every thread) if a wait
-// gave up; the ring is then drained and must not be reused.  LV: the level
-// pointer struct (its q / th / ph members are read).
+// The plane ring of one tile (planes x0 .. x0+nloc-1 of columns y0.., z0..):
+// TMA copies, waits, wrapped-halo patches and one CTA barrier per plane.
+// body(i, bm, bc, bp) evolves the tile's sites of plane x0 + i from the staged
+// planes bm (x - 1), bc (x) and bp (x + 1).  tid: the thread's index in the CTA
+// (the halo cells and the copy issue are divided by it).  smem: NBUF plane
+// buffers followed by NBUF initialised mbarriers; s_abort: a shared flag that
+// is 0 on entry.  Returns false (on every thread) if a wait gave up; the ring
+// is then drained and must not be reused.  LV: the level pointer struct (its
+// q / th / ph members are read).
 // STAGE: the wrapped halo cells of plane i+4 are copied by cp.async into
 // `stage` (HaloStage) while plane i+1 is computed, instead of prefetched into L2
 // and loaded after the plane's wait.
-template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV, bool STAGE = false>
-__device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const FConst& F,
-                                         const LV& now, const LV& past, int y0, int z0, int x0,
-                                         int nloc, unsigned char* smem, unsigned long long* bars, RingPhase& ring,
-                                         int* s_abort, double (&obs)[kObsCount], unsigned& warn,
-                                         unsigned char* stage = nullptr)
+template <class S, int TY, int TZ, int ND, class LV, bool STAGE, class Body>
+__device__ __forceinline__ bool run_ring(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LV& now,
+                                         int y0, int z0, int x0, int nloc, unsigned char* smem,
+                                         unsigned long long* bars, RingPhase& ring, int* s_abort,
+                                         unsigned char* stage, int tid, Body&& body)
 {
-    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
     using G = Geom<S, TY, TZ, ND>;
-    const int tz = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * TZ + tz;
     const int nplanes = nloc + 2;  // planes x0-1 .. x0+nloc
     const bool wraps = (y0 == 0) || (y0 + TY == P.ny) || (z0 == 0) || (z0 + TZ == P.nz);
     auto plane_x = [&](int p) {  // global x of relative plane p (p = 0 is x0 - 1)
@@ -396,13 +394,6 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
             prefetch_wrapped_halo<S, TY, TZ, ND>(P, now, plane_x(3), y0, z0, tid);
     }
 
-    // own cells
-    const int cq0 = (ty + 1) * G::QP + (tz + 1);
-    const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
-    const int y = y0 + ty, z = z0 + tz;
-    XCarry<S, ND> carry;
-    carry.valid = false;
-
     // planes 0, 1, 2 (x0-1, x0, x0+1) resident and patched before the first site
     bool ok = true;
     for (int p = 0; p < 3; p++) {  // nplanes >= 3
@@ -420,30 +411,8 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
     // that barrier both publishes the patches and frees plane i's buffer for
     // the copy of plane i+4.
     for (int i = 0; i < nloc && !aborted; i++) {
-        const unsigned char* bm = smem + (i % G::NBUF) * G::BUF;
-        const unsigned char* bc = smem + ((i + 1) % G::NBUF) * G::BUF;
-        const unsigned char* bp = smem + ((i + 2) % G::NBUF) * G::BUF;
-        Stencil<TRef> n;
-        n.c = {bc, cq0, ch0};
-        n.m[0] = {bm, cq0, ch0};
-        n.p[0] = {bp, cq0, ch0};
-        n.m[1] = {bc, cq0 - G::QP, ch0 - G::HP};
-        n.p[1] = {bc, cq0 + G::QP, ch0 + G::HP};
-        n.m[2] = {bc, cq0 - 1, ch0 - 1};
-        n.p[2] = {bc, cq0 + 1, ch0 + 1};
-        n.d01 = {bp, cq0 - G::QP, ch0 - G::HP};
-        n.d02 = {bp, cq0 - 1, ch0 - 1};
-        n.d10 = {bm, cq0 + G::QP, ch0 + G::HP};
-        n.d12 = {bc, cq0 + G::QP - 1, ch0 + G::HP - 1};
-        n.d20 = {bm, cq0 + 1, ch0 + 1};
-        n.d21 = {bc, cq0 - G::QP + 1, ch0 - G::HP + 1};
-        const int x = x0 + i;
-        const int s = (x * P.ny + y) * P.nz + z;
-        if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
-            carry.valid = false;
-        else
-            site_step<S, MODEL, ENERGY>(P, F, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs, warn,
-                                        counts(P, x));
+        body(i, smem + (i % G::NBUF) * G::BUF, smem + ((i + 1) % G::NBUF) * G::BUF,
+             smem + ((i + 2) % G::NBUF) * G::BUF);
 
         // plane i+3 (x+2) for the next site; its copy was issued one plane ago
         bool okn = true;
@@ -488,6 +457,60 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
     for (int b = 0; b < G::NBUF; b++)
         if (b < nplanes) ring.bits ^= (((unsigned)((nplanes - b + G::NBUF - 1) / G::NBUF)) & 1u) << b;
     return true;
+}
+
+// Stencil references of the site in cell (cq0, ch0) of the staged planes bm, bc, bp.
+template <int QP, int HP>
+__device__ __forceinline__ Stencil<TRef> plane_stencil(const unsigned char* bm, const unsigned char* bc,
+                                                       const unsigned char* bp, int cq0, int ch0)
+{
+    Stencil<TRef> n;
+    n.c = {bc, cq0, ch0};
+    n.m[0] = {bm, cq0, ch0};
+    n.p[0] = {bp, cq0, ch0};
+    n.m[1] = {bc, cq0 - QP, ch0 - HP};
+    n.p[1] = {bc, cq0 + QP, ch0 + HP};
+    n.m[2] = {bc, cq0 - 1, ch0 - 1};
+    n.p[2] = {bc, cq0 + 1, ch0 + 1};
+    n.d01 = {bp, cq0 - QP, ch0 - HP};
+    n.d02 = {bp, cq0 - 1, ch0 - 1};
+    n.d10 = {bm, cq0 + QP, ch0 + HP};
+    n.d12 = {bc, cq0 + QP - 1, ch0 + HP - 1};
+    n.d20 = {bm, cq0 + 1, ch0 + 1};
+    n.d21 = {bc, cq0 - QP + 1, ch0 - HP + 1};
+    return n;
+}
+
+// Evolves one tile by one step, one site per thread (threads TZ x TY).
+template <class S, int MODEL, int TY, int TZ, bool ENERGY, class LV, bool STAGE = false>
+__device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const FConst& F,
+                                         const LV& now, const LV& past, int y0, int z0, int x0,
+                                         int nloc, unsigned char* smem, unsigned long long* bars, RingPhase& ring,
+                                         int* s_abort, double (&obs)[kObsCount], unsigned& warn,
+                                         unsigned char* stage = nullptr)
+{
+    constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
+    using G = Geom<S, TY, TZ, ND>;
+    const int tz = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * TZ + tz;
+    // own cells
+    const int cq0 = (ty + 1) * G::QP + (tz + 1);
+    const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
+    const int y = y0 + ty, z = z0 + tz;
+    XCarry<S, ND> carry;
+    carry.valid = false;
+    return run_ring<S, TY, TZ, ND, LV, STAGE>(
+        maps, pmaps, P, now, y0, z0, x0, nloc, smem, bars, ring, s_abort, stage, tid,
+        [&](int i, const unsigned char* bm, const unsigned char* bc, const unsigned char* bp) {
+            const Stencil<TRef> n = plane_stencil<G::QP, G::HP>(bm, bc, bp, cq0, ch0);
+            const int x = x0 + i;
+            const int s = (x * P.ny + y) * P.nz + z;
+            if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
+                carry.valid = false;
+            else
+                site_step<S, MODEL, ENERGY>(P, F, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs,
+                                            warn, counts(P, x));
+        });
 }
 
 }  // namespace tiled

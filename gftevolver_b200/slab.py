@@ -170,9 +170,16 @@ class SlabEvolver:
     """
 
     def __init__(self, params: LatticeParams, form: str = "mixed", device: int = 0, group=None, transport=None,
-                 rank: int | None = None, world: int | None = None, auto_exchange: bool = True):
+                 rank: int | None = None, world: int | None = None, auto_exchange: bool = True,
+                 exchange: str = "python", timeout_s: float = 300.0):
         """rank / world override the process group's (several slabs driven by one process, e.g. in
-        tests); auto_exchange=False leaves the ghost refresh to the caller (``halo``)."""
+        tests); auto_exchange=False leaves the ghost refresh to the caller (``halo``).
+
+        exchange="python": the ghost refresh runs after every step from a callback, through
+        ``transport`` (torch.distributed point-to-point operations, or a local copy on one rank).
+        exchange="library": gft_evolve posts it itself over NCCL (gft_set_slab_nccl): the boundary
+        planes go out on a second stream while the interior planes are computed, with no host
+        callback per step; its final wait gives up after ``timeout_s`` seconds."""
         import torch
         import torch.distributed as dist
         self.global_params = params
@@ -197,8 +204,29 @@ class SlabEvolver:
         self._stream = torch.cuda.ExternalStream(self.local.stream, device=f"cuda:{device}")
         self._error = None
         self._cb = _lib.EXCHANGE_FN(self._on_exchange)
-        if auto_exchange:
+        self.exchange = exchange
+        if exchange == "library":
+            self._join_nccl(timeout_s)
+        elif exchange != "python":
+            raise ValueError(f"exchange must be 'python' or 'library', not {exchange!r}")
+        elif auto_exchange:
             _lib.check(lib.gft_set_exchange(h, ctypes.cast(self._cb, ctypes.c_void_p), None), h)
+
+    def _join_nccl(self, timeout_s: float) -> None:
+        """One NCCL communicator over the ranks of the group: rank 0 makes its id, the group shares it."""
+        import torch.distributed as dist
+        lib, h = self.local.lib, self.local.h
+        id_buf = ctypes.create_string_buffer(128)
+        if self.rank == 0:
+            _lib.check(lib.gft_nccl_unique_id(id_buf))
+        if self.world > 1:
+            if not (dist.is_available() and dist.is_initialized()):
+                raise RuntimeError("exchange='library' over several ranks needs an initialised process group")
+            obj = [id_buf.raw if self.rank == 0 else None]
+            src = 0 if self.group is None else dist.get_global_rank(self.group, 0)
+            dist.broadcast_object_list(obj, src=src, group=self.group)
+            id_buf = ctypes.create_string_buffer(obj[0], 128)
+        _lib.check(lib.gft_set_slab_nccl(h, id_buf, self.world, self.rank, float(timeout_s)), h)
 
     # plane views of the library's field storage
     def _planes(self, level: int, x: int):
@@ -270,6 +298,7 @@ class SlabEvolver:
 
     def close(self) -> None:
         if getattr(self, "local", None) is not None:
-            self.local.lib.gft_set_exchange(self.local.h, None, None)
+            if self.exchange == "python":
+                self.local.lib.gft_set_exchange(self.local.h, None, None)
             self.local.close()
             self.local = None

@@ -71,8 +71,10 @@ extern "C" {
 #define GFT_FORM_REF 0    /* reference arithmetic: per-site math in FP64 in the reference's operation
                              order; storage = `storage_bytes` (4: the reference as shipped, 8: FP64 storage) */
 #define GFT_FORM_FP64 1   /* plain FP64 form: FP64 storage and math, reassociated for throughput */
-#define GFT_FORM_MIXED 2  /* FP32 storage and force math; FP64 for link momentum, updates,
-                             renormalisation and reductions */
+#define GFT_FORM_MIXED 2  /* FP32 storage and FP32 per-site math throughout (forces, link momentum,
+                             leapfrog and link update, renormalisation), rearranged so that no step
+                             subtracts nearly equal FP32 values; FP64 only for the energy, plaquette,
+                             <phi^2> and Gauss reductions (the Gauss residual itself in FP64) */
 
 typedef struct gft_config {
     int model;                     /* GFT_MODEL_* */
@@ -227,6 +229,24 @@ int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user);
  * arrays (7, 8 or 11). */
 int gft_level_planes(gft_handle* h, int level, int x, void** ptrs, size_t* bytes, int max);
 
+/* The ghost-plane exchange inside the library, over NCCL (no reference
+ * counterpart; the reference's Core/Source/Lattice.cpp:779 marks where an
+ * overlapped send / late receive would go).  gft_nccl_unique_id writes the
+ * 128-byte id of a new communicator (one rank calls it and shares the bytes
+ * with the others); gft_set_slab_nccl joins it as `rank` of `nranks` (ring
+ * neighbours rank - 1 and rank + 1 mod nranks; one rank exchanges with itself).
+ * The slab must have been set with gft_set_slab(h, ..., 1, nx - 1) and no
+ * exchange callback.  From then on gft_evolve posts the exchange itself: on
+ * plain steps of the tiled kernels it computes the two boundary planes, sends
+ * them on a second stream while the interior planes are computed, and makes
+ * the next work wait for the ghost planes; on other steps it exchanges after
+ * the whole step.  Its final wait is bounded by timeout_s seconds (and watches
+ * the communicator for errors): a rank whose peer is gone gets GFT_E_TIMEOUT or
+ * GFT_E_CUDA, and the communicator is aborted.  NCCL is loaded at run time
+ * (libnccl.so.2); GFT_E_UNSUPPORTED if it cannot be. */
+int gft_nccl_unique_id(unsigned char* id);
+int gft_set_slab_nccl(gft_handle* h, const unsigned char* id, int nranks, int rank, double timeout_s);
+
 /* Allocation-free observables (no counterpart in the reference).  For callers
  * that cannot allocate device memory where they need the numbers -- a fixed
  * memory budget, a region that must stay asynchronous (cudaMalloc/cudaFree
@@ -253,14 +273,17 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
  * kind 0 = automatic (the tiled kernel for the SM mixed form when the lattice
  * divides into a built tile, else the one-thread-per-site kernel), 1 = one
  * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
- * marching along x (mixed form).  tile = tile shape (0: 8 x 32, 1: 4 x 32,
+ * marching along x (mixed form), 3 = as 2, with two sites per thread in paired
+ * FP32 arithmetic on the plain (non-logging) steps (periodic SM model, tiles 0
+ * and 3).  tile = tile shape (0: 8 x 32, 1: 4 x 32,
  * 2: 4 x 16, 3: 16 x 16 sites in y x z); march = planes per CTA along x.  Returns
  * GFT_E_UNSUPPORTED when the lattice does not divide into the tile or carries a
  * Higgs-family field (one thread per site serves those). */
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
 /* Diagnostic with no reference counterpart: the time limit, in nanoseconds, of
- * the tiled kernel's waits for its staged planes (0 restores the default, 2 s).
+ * the tiled kernel's waits for its staged planes, at most 4e9 (0 restores the
+ * default, 2 s).
  * When a wait gives up, the tile still waits, with the 2 s bound, for its copies
  * in flight, then the step returns GFT_E_TIMEOUT and the fields are invalid
  * until the next upload.  A limit below 1 us makes each wait a single

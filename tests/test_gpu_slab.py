@@ -107,3 +107,43 @@ def test_two_slabs_on_one_gpu_equal_whole_lattice():
         assert abs(ra["energy"] + rb["energy"] - rg["energy"]) <= 1e-12 * abs(rg["energy"])
         plaq = (ra["plaq_su2"] * a.own_sites + rb["plaq_su2"] * b.own_sites) / (a.own_sites + b.own_sites)
         assert abs(plaq - rg["plaq_su2"]) <= 1e-12
+
+
+@pytest.mark.parametrize("form,kind,ftol,rtol", [
+    ("fp64", 0, 0.0, 1e-12),     # one thread per site: exchange after each whole step, bit for bit
+    ("mixed", 2, 2e-6, 1e-6),    # tiled: boundary planes, exchange overlapped with the interior planes
+    ("mixed", 3, 2e-6, 1e-6),    # tiled, two sites per thread on plain steps
+])
+def test_library_exchange_over_nccl_equals_whole_lattice(form, kind, ftol, rtol):
+    """exchange='library': gft_evolve posts the ghost-plane exchange over NCCL itself (here one rank,
+    which sends its boundary planes to itself).  The slab equals the whole lattice as with the
+    callback exchange; in the tiled kernels the x-chunks start at other planes (contraction bound)."""
+    from gftevolver_b200 import Evolver, InitialData
+    from gftevolver_b200.slab import SlabEvolver
+    p = _params(1, (12, 8, 32), every=(3, 3))
+    ic = InitialData(**IC)
+    with Evolver(p, form=form) as ev:
+        ev.init_fields(ic)
+        g_rows = ev.evolve(8)
+        g_sc, g_ve = ev.download()
+    slab = SlabEvolver(p, form=form, exchange="library")
+    try:
+        if kind:  # march 4: boundary chunks of 4 planes at each end, 4 interior planes
+            slab.local.set_kernel(kind, 0, 4)
+        slab.init_fields(ic)
+        l0 = slab.local.launch_count
+        rows = slab.evolve(8)
+        launches = slab.local.launch_count - l0
+        s_sc, s_ve = slab.download_own()
+    finally:
+        slab.close()
+    assert np.max(np.abs(s_sc - g_sc)) <= ftol and np.max(np.abs(s_ve - g_ve)) <= ftol
+    _rows_close(rows, g_rows, rtol)
+    if kind:  # the plain steps were split into boundary and interior launches
+        with Evolver(p, form=form) as ev:
+            ev.set_kernel(kind, 0, 4)
+            ev.init_fields(ic)
+            l1 = ev.launch_count
+            ev.evolve(8)
+            whole = ev.launch_count - l1
+        assert launches == whole + 2 * 5  # 5 plain steps of 8 (logging every 3), two more launches each
