@@ -1,12 +1,15 @@
 // gft_math.cuh -- elementary functions for the throughput kernels.
 //
-// Written from the Taylor series of sin, cos and asin with a two/three-term
-// Cody-Waite reduction by pi (W. J. Cody, W. Waite, "Software Manual for the
-// Elementary Functions", 1980): r = x - k*pi with k = rint(x/pi), |r| <= pi/2,
-// then sin(x) = (-1)^k sin(r), cos(x) = (-1)^k cos(r).  The series are
-// truncated where the first omitted term is below the format's rounding:
-//   float : sin to r^13, cos to r^14  (omitted term <= 7e-10 at |r| = pi/2)
-//   double: sin to r^23, cos to r^24  (omitted term <= 1e-19)
+// Written with a two/three-term Cody-Waite reduction by pi (W. J. Cody,
+// W. Waite, "Software Manual for the Elementary Functions", 1980):
+// r = x - k*pi with k = rint(x/pi), |r| <= pi/2, then sin(x) = (-1)^k sin(r),
+// cos(x) = (-1)^k cos(r).  On the reduced range:
+//   float : minimax polynomials fitted for this library by the Remez exchange
+//           (gft_math_fit.py regenerates them): sin r = r + r^3 P(r^2), degree 9,
+//           relative error <= 6.1e-9; cos r = 1 + r^2 Q(r^2), degree 10, absolute
+//           error <= 2.5e-10 -- both below float's rounding, and two multiply-adds
+//           shorter each than the Taylor series of equal accuracy (degree 13 / 14);
+//   double: Taylor series, sin to r^23, cos to r^24 (omitted term <= 1e-19).
 // The reduction uses the 1.5*2^p rounding constant (no conversion to integer):
 // it holds for |x| < 1.3e7 (float) / 1.4e15 (double); phases that large do not
 // occur in the evolution (the step kernels flag |theta| > 1e4).
@@ -44,35 +47,40 @@ namespace gft {
 #define GFT_C22 (-1.0 / 1124000727777607680000.0)
 #define GFT_C24 (1.0 / 620448401733239439360000.0)
 
+// Float minimax coefficients on |r| <= pi/2 (gft_math_fit.py): sin r = r + r^3 P(r^2), cos r = 1 + r^2 Q(r^2).
+#define GFT_FS3 (-0.16666659712791443f)
+#define GFT_FS5 (0.00833306647837162f)
+#define GFT_FS7 (-0.00019809602235909551f)
+#define GFT_FS9 (2.605780537123792e-06f)
+#define GFT_FC2 (-0.5f)
+#define GFT_FC4 (0.04166664183139801f)
+#define GFT_FC6 (-0.00138884037733078f)
+#define GFT_FC8 (2.4761886379565112e-05f)
+#define GFT_FC10 (-2.607710598567792e-07f)
+
 __device__ __forceinline__ void sincos_poly(float r, float& s, float& c)
 {
     const float r2 = r * r;
-    float ps = (float)GFT_S13;
-    ps = fmaf(ps, r2, (float)GFT_S11);
-    ps = fmaf(ps, r2, (float)GFT_S9);
-    ps = fmaf(ps, r2, (float)GFT_S7);
-    ps = fmaf(ps, r2, (float)GFT_S5);
-    ps = fmaf(ps, r2, (float)GFT_S3);
+    float ps = GFT_FS9;
+    ps = fmaf(ps, r2, GFT_FS7);
+    ps = fmaf(ps, r2, GFT_FS5);
+    ps = fmaf(ps, r2, GFT_FS3);
     s = fmaf(ps * r2, r, r);
-    float pc = (float)GFT_C14;
-    pc = fmaf(pc, r2, (float)GFT_C12);
-    pc = fmaf(pc, r2, (float)GFT_C10);
-    pc = fmaf(pc, r2, (float)GFT_C8);
-    pc = fmaf(pc, r2, (float)GFT_C6);
-    pc = fmaf(pc, r2, (float)GFT_C4);
-    pc = fmaf(pc, r2, (float)GFT_C2);
+    float pc = GFT_FC10;
+    pc = fmaf(pc, r2, GFT_FC8);
+    pc = fmaf(pc, r2, GFT_FC6);
+    pc = fmaf(pc, r2, GFT_FC4);
+    pc = fmaf(pc, r2, GFT_FC2);
     c = fmaf(pc, r2, 1.0f);
 }
 
 __device__ __forceinline__ float sin_poly(float r)
 {
     const float r2 = r * r;
-    float ps = (float)GFT_S13;
-    ps = fmaf(ps, r2, (float)GFT_S11);
-    ps = fmaf(ps, r2, (float)GFT_S9);
-    ps = fmaf(ps, r2, (float)GFT_S7);
-    ps = fmaf(ps, r2, (float)GFT_S5);
-    ps = fmaf(ps, r2, (float)GFT_S3);
+    float ps = GFT_FS9;
+    ps = fmaf(ps, r2, GFT_FS7);
+    ps = fmaf(ps, r2, GFT_FS5);
+    ps = fmaf(ps, r2, GFT_FS3);
     return fmaf(ps * r2, r, r);
 }
 

@@ -113,12 +113,10 @@ __device__ __forceinline__ V flip(V v, unsigned sx, unsigned sy)
 __device__ __forceinline__ V sin_poly(V r)
 {
     const V r2 = mul(r, r);
-    V ps = bc((float)GFT_S13);
-    ps = fma(ps, r2, bc((float)GFT_S11));
-    ps = fma(ps, r2, bc((float)GFT_S9));
-    ps = fma(ps, r2, bc((float)GFT_S7));
-    ps = fma(ps, r2, bc((float)GFT_S5));
-    ps = fma(ps, r2, bc((float)GFT_S3));
+    V ps = bc(GFT_FS9);
+    ps = fma(ps, r2, bc(GFT_FS7));
+    ps = fma(ps, r2, bc(GFT_FS5));
+    ps = fma(ps, r2, bc(GFT_FS3));
     return fma(mul(ps, r2), r, r);
 }
 
@@ -134,20 +132,16 @@ __device__ __forceinline__ void gsincos(V x, V& s, V& c)
     unsigned sx, sy;
     const V r = reduce_pi(x, sx, sy);
     const V r2 = mul(r, r);
-    V ps = bc((float)GFT_S13);
-    ps = fma(ps, r2, bc((float)GFT_S11));
-    ps = fma(ps, r2, bc((float)GFT_S9));
-    ps = fma(ps, r2, bc((float)GFT_S7));
-    ps = fma(ps, r2, bc((float)GFT_S5));
-    ps = fma(ps, r2, bc((float)GFT_S3));
+    V ps = bc(GFT_FS9);
+    ps = fma(ps, r2, bc(GFT_FS7));
+    ps = fma(ps, r2, bc(GFT_FS5));
+    ps = fma(ps, r2, bc(GFT_FS3));
     s = flip(fma(mul(ps, r2), r, r), sx, sy);
-    V pc = bc((float)GFT_C14);
-    pc = fma(pc, r2, bc((float)GFT_C12));
-    pc = fma(pc, r2, bc((float)GFT_C10));
-    pc = fma(pc, r2, bc((float)GFT_C8));
-    pc = fma(pc, r2, bc((float)GFT_C6));
-    pc = fma(pc, r2, bc((float)GFT_C4));
-    pc = fma(pc, r2, bc((float)GFT_C2));
+    V pc = bc(GFT_FC10);
+    pc = fma(pc, r2, bc(GFT_FC8));
+    pc = fma(pc, r2, bc(GFT_FC6));
+    pc = fma(pc, r2, bc(GFT_FC4));
+    pc = fma(pc, r2, bc(GFT_FC2));
     c = flip(fma(pc, r2, bc(1.0f)), sx, sy);
 }
 
