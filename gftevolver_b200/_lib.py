@@ -115,6 +115,7 @@ SIGNATURES = {
     "gft_selftest_math": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gft_set_kernel": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gft_set_wait_limit": (ctypes.c_int, [_H, ctypes.c_ulonglong]),
+    "gft_set_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
     "gft_nccl_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
     "gft_set_slab_nccl": (ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "gft_observe_static": (ctypes.c_int, [ctypes.POINTER(GftConfig), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,11 @@ void set_global_error(const std::string& s)
 // gaugeNum maximum Gauss slots (room for gaugeNum = 7).
 constexpr int kRowSlots = kRowSlotCount;
 constexpr int kMaxProfiled = 8192;
+// Single handles replay whole logging periods from a CUDA graph up to this many
+// sites (160^3 and below: a step is short enough that launching it costs), for
+// periods up to kMaxGraphPeriod steps.
+constexpr int kGraphMaxSites = 1 << 22;
+constexpr int kMaxGraphPeriod = 256;
 
 }  // namespace
 
@@ -65,7 +71,15 @@ struct gft_handle {
     bool has_data = false;
     bool profile = true;
     std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_steps;  // steps each profiled interval covers (a graph replay: its period)
     int ev_used = 0;
+    // CUDA graph of one logging period (graph_period)
+    bool use_graphs = true;
+    cudaGraphExec_t graph = nullptr;
+    int graph_period = 0, graph_rows = 0;
+    long long graph_launches = 0;
+    double* d_graph_rows = nullptr;
+    int graph_rows_cap = 0;
     long long launches = 0;  // kernels launched by gft_evolve / gft_observe
     std::string err;
     size_t dev_bytes = 0;
@@ -111,6 +125,24 @@ struct gft_handle {
 namespace {
 
 bool is_f64_storage(const gft_handle* h) { return h->sbytes == 8; }
+
+// Whether step `ti` writes an analyser row.
+bool logs_row(const gft_config& c, int ti)
+{
+    return (c.energy_every > 0 && ti % c.energy_every == 0) || (c.gauss_every > 0 && ti % c.gauss_every == 0);
+}
+
+// Forget the captured period (its launches bake in the kernel choice, tensor maps,
+// buffers and parameters that the caller is about to change).
+void drop_graph(gft_handle* h)
+{
+    if (h->graph) {
+        cudaStreamSynchronize(h->stream);
+        cudaGraphExecDestroy(h->graph);
+    }
+    h->graph = nullptr;
+    h->graph_period = 0;
+}
 
 // Parameters of one launch.  For the reference-arithmetic form with float
 // storage, the couplings and the damping factor take the values the shipped
@@ -487,6 +519,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     cudaMemcpy(h->d_scale, scale, sizeof(scale), cudaMemcpyHostToDevice);
     cudaMemset(h->d_status, 0, sizeof(unsigned));
     h->ev.resize(2 * (size_t)kMaxProfiled);
+    h->ev_steps.assign(kMaxProfiled, 1);
     for (auto& x : h->ev) {
         if ((e = cudaEventCreate(&x)) != cudaSuccess) {
             x = nullptr;
@@ -511,6 +544,8 @@ void gft_destroy(gft_handle* h)
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->comm_stream) cudaStreamSynchronize(h->comm_stream);
+    drop_graph(h);
+    cudaFree(h->d_graph_rows);
     slab_comm_destroy(h->comm, false);
     if (h->ev_bound) cudaEventDestroy(h->ev_bound);
     if (h->ev_comm) cudaEventDestroy(h->ev_comm);
@@ -718,6 +753,136 @@ cudaError_t split_slab_step(gft_handle* h, const StepParams& P, int tn, const Le
     return err;
 }
 
+// The launches of one step at time_iter `ti`: the step kernel (split for an
+// x-slab with the library's exchange), the energy row into `out`, the ghost
+// exchange, the Gauss pass and its row.  prof: record the step kernel's events.
+// Returns a CUDA error, or sets rc / why (exchange failures).
+template <class S>
+cudaError_t issue_step(gft_handle* h, const LevelPtrs<S>* lv, int ti, double* out, bool prof, int& rc,
+                       std::string& why)
+{
+    const gft_config& c = h->cfg;
+    const int tn = (ti + 1) % 2, tp = 1 - tn;
+    const bool e = c.energy_every > 0 && ti % c.energy_every == 0;  // rows
+    const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
+    // local outputs: the energy pass (and its renormalisation) also runs on their steps
+    const bool el = c.energy_local_every > 0 && ti % c.energy_local_every == 0;
+    const bool gl = c.gauss_local_every > 0 && ti % c.gauss_local_every == 0;
+    StepParams P = make_params(h, ti, e || el);
+    P.loc_energy = el ? h->d_loc_e : nullptr;
+    P.loc_gauss = gl ? h->d_loc_g : nullptr;
+    if (el) h->loc_e_step = ti;
+    if (gl) h->loc_g_step = ti;
+    if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
+    // an x-slab with the exchange in the library overlaps it with the interior on plain steps
+    const bool split = h->comm && !(e || el) && sizeof(S) == 4 && use_tiled(h, P) && h->x_begin == 1 &&
+                       h->x_end == c.nx - 1;
+    int nstep = 1;
+    cudaError_t err;
+    if (split) {
+        nstep = 0;
+        err = split_slab_step<S>(h, P, tn, lv, nstep, rc, why);
+        if (rc != GFT_OK) return cudaSuccess;
+    } else {
+        err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e || el);
+    }
+    h->launches += nstep + (e ? finalize_launches(step_blocks(h, P), true) : 0) + ((g || gl) ? 1 : 0) +
+                   (g ? finalize_launches(gauss_blocks(h, P), true) : 0);
+    if (prof) {
+        cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
+        h->ev_steps[h->ev_used] = 1;
+        h->ev_used++;
+    }
+    if (err != cudaSuccess) return err;
+    if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->d_mid,
+                                 h->stream);
+    if (h->comm && !split && err == cudaSuccess) {
+        // logging steps (and forms without the split): the exchange after the whole step
+        SlabPlanes pl;
+        rc = fill_slab_planes(h, tp, pl);
+        if (rc == GFT_OK) rc = slab_comm_exchange(h->comm, pl, h->stream, why);
+        if (rc != GFT_OK) return cudaSuccess;
+    }
+    if (h->exchange && err == cudaSuccess) {
+        // refresh the ghost planes of the level just written before anything reads them
+        const int xr = h->exchange(h, tp, h->exchange_user);
+        if (xr != 0) {
+            rc = GFT_E_STATE;
+            why = "the exchange callback failed (" + std::to_string(xr) + ")";
+            return cudaSuccess;
+        }
+    }
+    if ((g || gl) && err == cudaSuccess) {
+        err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
+        if (err == cudaSuccess && g)
+            err = launch_finalize(h->d_part_g, gauss_blocks(h, P), 2 * h->neq, h->neq, h->d_scale + kObsCount,
+                                  out + kObsCount, h->d_mid, h->stream);
+    }
+    return err;
+}
+
+// Logging period replayed from a CUDA graph (lcm of 2 and the analysers'
+// cadences), or 0 where a single handle steps launch by launch: lattices large
+// enough that launching is no cost, x-slabs (per-step exchange), local outputs.
+int graph_period(const gft_handle* h)
+{
+    const gft_config& c = h->cfg;
+    if (!h->use_graphs || h->nsite > kGraphMaxSites || h->exchange || h->comm || c.energy_local_every > 0 ||
+        c.gauss_local_every > 0)
+        return 0;
+    int p = 2;
+    if (c.energy_every > 0) p = std::lcm(p, c.energy_every);
+    if (c.gauss_every > 0) p = std::lcm(p, c.gauss_every);
+    return p <= kMaxGraphPeriod ? p : 0;
+}
+
+// Capture the period starting at ti0 (a multiple of the period; the launches
+// depend on time_iter only through its parity and the logging cadence).
+template <class S>
+int build_graph(gft_handle* h, const LevelPtrs<S>* lv, int ti0, int period)
+{
+    int nrows = 0;
+    for (int s = 0; s < period; s++) nrows += logs_row(h->cfg, ti0 + s) ? 1 : 0;
+    if (nrows > h->graph_rows_cap) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->d_graph_rows);
+        h->d_graph_rows = nullptr;
+        if (cudaMalloc(&h->d_graph_rows, (size_t)std::max(nrows, 1) * kRowSlots * sizeof(double)) != cudaSuccess)
+            return h->fail(GFT_E_NOMEM, "gft_evolve: graph rows allocation failed");
+        h->graph_rows_cap = nrows;
+    }
+    const long long l0 = h->launches;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_evolve: begin capture");
+    cudaError_t ie = cudaSuccess;
+    int rc = GFT_OK, row = 0;
+    std::string why;
+    for (int s = 0; s < period && ie == cudaSuccess && rc == GFT_OK; s++) {
+        const int ti = ti0 + s;
+        ie = issue_step<S>(h, lv, ti, h->d_graph_rows + (size_t)row * kRowSlots, false, rc, why);
+        if (logs_row(h->cfg, ti)) row++;
+    }
+    e = cudaStreamEndCapture(h->stream, &g);
+    const long long nl = h->launches - l0;
+    h->launches = l0;
+    if (ie != cudaSuccess || e != cudaSuccess || rc != GFT_OK) {
+        if (g) cudaGraphDestroy(g);
+        if (rc != GFT_OK) return h->fail(rc, "gft_evolve: " + why);
+        return h->cuda_fail(ie != cudaSuccess ? ie : e, "gft_evolve: capture");
+    }
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gft_evolve: graph instantiate");
+    drop_graph(h);
+    h->graph = x;
+    h->graph_period = period;
+    h->graph_rows = nrows;
+    h->graph_launches = nl;
+    return GFT_OK;
+}
+
 template <class S>
 int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observables* rows, int max_rows, int* n_rows)
 {
@@ -728,79 +893,62 @@ int evolve_impl(gft_handle* h, const LevelPtrs<S>* lv, int n_steps, gft_observab
     };
     std::vector<Meta> meta;
     int nlog = 0;
-    for (int s = 0; s < n_steps; s++) {
-        const int ti = h->time_iter + s;
-        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;
-        const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
-        if (e || g) nlog++;
-    }
+    for (int s = 0; s < n_steps; s++)
+        if (logs_row(c, h->time_iter + s)) nlog++;
     int rc = ensure_rows(h, std::max(nlog, 1));
     if (rc != GFT_OK) return rc;
+    const int period = graph_period(h);
     cudaError_t err = cudaSuccess;
     int row = 0;
-    for (int s = 0; s < n_steps && err == cudaSuccess; s++) {
+    for (int s = 0; s < n_steps && err == cudaSuccess;) {
         const int ti = h->time_iter;
-        const int tn = (ti + 1) % 2, tp = 1 - tn;
-        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;  // rows
-        const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
-        // local outputs: the energy pass (and its renormalisation) also runs on their steps
-        const bool el = c.energy_local_every > 0 && ti % c.energy_local_every == 0;
-        const bool gl = c.gauss_local_every > 0 && ti % c.gauss_local_every == 0;
-        StepParams P = make_params(h, ti, e || el);
-        P.loc_energy = el ? h->d_loc_e : nullptr;
-        P.loc_gauss = gl ? h->d_loc_g : nullptr;
-        if (el) h->loc_e_step = ti;
-        if (gl) h->loc_g_step = ti;
-        const bool prof = h->profile && h->ev_used < kMaxProfiled;
-        if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
-        // an x-slab with the exchange in the library overlaps it with the interior on plain steps
-        const bool split = h->comm && !(e || el) && sizeof(S) == 4 && use_tiled(h, P) && h->x_begin == 1 &&
-                           h->x_end == c.nx - 1;
-        int nstep = 1, crc = GFT_OK;
-        std::string cwhy;
-        if (split) {
-            nstep = 0;
-            err = split_slab_step<S>(h, P, tn, lv, nstep, crc, cwhy);
-            if (crc != GFT_OK) return h->fail(crc, "gft_evolve: " + cwhy);
-        } else {
-            err = launch_step<S>(h, P, tn, lv[tn], lv[tp], e || el);
-        }
-        h->launches += nstep + (e ? finalize_launches(step_blocks(h, P), true) : 0) + ((g || gl) ? 1 : 0) +
-                       (g ? finalize_launches(gauss_blocks(h, P), true) : 0);
-        if (prof) {
-            cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
-            h->ev_used++;
-        }
-        if (err != cudaSuccess) break;
-        double* out = h->d_rows + (size_t)row * kRowSlots;
-        if (e) err = launch_finalize(h->d_part_e, step_blocks(h, P), kObsCount, kObsCount, h->d_scale, out, h->d_mid,
-                                         h->stream);
-        if (h->comm && !split && err == cudaSuccess) {
-            // logging steps (and forms without the split): the exchange after the whole step
-            SlabPlanes pl;
-            int xrc = fill_slab_planes(h, tp, pl);
-            if (xrc == GFT_OK) xrc = slab_comm_exchange(h->comm, pl, h->stream, cwhy);
-            if (xrc != GFT_OK) return h->fail(xrc, "gft_evolve: " + cwhy);
-        }
-        if (h->exchange && err == cudaSuccess) {
-            // refresh the ghost planes of the level just written before anything reads them
-            const int xr = h->exchange(h, tp, h->exchange_user);
-            if (xr != 0) {
-                h->time_iter++;
-                return h->fail(GFT_E_STATE, "gft_evolve: the exchange callback failed (" + std::to_string(xr) + ")");
+        if (period > 0 && ti % period == 0 && n_steps - s >= period && ti >= c.nt_damped) {
+            // a whole logging period from the graph (no host launch per kernel)
+            if (!h->graph || h->graph_period != period) {
+                rc = build_graph<S>(h, lv, ti, period);
+                if (rc != GFT_OK) return rc;
             }
+            const bool prof = h->profile && h->ev_used < kMaxProfiled;
+            if (prof) cudaEventRecord(h->ev[2 * (size_t)h->ev_used], h->stream);
+            err = cudaGraphLaunch(h->graph, h->stream);
+            if (prof) {
+                cudaEventRecord(h->ev[2 * (size_t)h->ev_used + 1], h->stream);
+                h->ev_steps[h->ev_used] = period;
+                h->ev_used++;
+            }
+            h->launches += h->graph_launches;
+            if (err == cudaSuccess && h->graph_rows > 0)
+                err = cudaMemcpyAsync(h->d_rows + (size_t)row * kRowSlots, h->d_graph_rows,
+                                      (size_t)h->graph_rows * kRowSlots * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      h->stream);
+            for (int k = 0; k < period; k++) {
+                const int t = ti + k;
+                const bool e = c.energy_every > 0 && t % c.energy_every == 0;
+                const bool g = c.gauss_every > 0 && t % c.gauss_every == 0;
+                if (e || g) {
+                    meta.push_back({t, e, g});
+                    row++;
+                }
+            }
+            h->time_iter += period;
+            s += period;
+            continue;
         }
-        if ((g || gl) && err == cudaSuccess) {
-            err = launch_gauss<S>(h, P, lv[tn], lv[tp]);
-            if (err == cudaSuccess && g)
-                err = launch_finalize(h->d_part_g, gauss_blocks(h, P), 2 * h->neq, h->neq, h->d_scale + kObsCount,
-                                      out + kObsCount, h->d_mid, h->stream);
+        const bool e = c.energy_every > 0 && ti % c.energy_every == 0;
+        const bool g = c.gauss_every > 0 && ti % c.gauss_every == 0;
+        std::string why;
+        err = issue_step<S>(h, lv, ti, h->d_rows + (size_t)row * kRowSlots, h->profile && h->ev_used < kMaxProfiled,
+                            rc, why);
+        if (rc != GFT_OK) {
+            h->time_iter++;
+            return h->fail(rc, "gft_evolve: " + why);
         }
         if (e || g) {
             meta.push_back({ti, e, g});
             row++;
         }
         h->time_iter++;
+        s++;
     }
     if (err != cudaSuccess) return h->cuda_fail(err, "gft_evolve(launch)");
     std::vector<double> host((size_t)std::max(row, 1) * kRowSlots);
@@ -928,10 +1076,19 @@ int gft_observe(gft_handle* h, gft_observables* row)
     return GFT_OK;
 }
 
+int gft_set_graphs(gft_handle* h, int on)
+{
+    if (!h) return GFT_E_INVALID;
+    drop_graph(h);
+    h->use_graphs = on != 0;
+    return GFT_OK;
+}
+
 int gft_set_wait_limit(gft_handle* h, unsigned long long ns)
 {
     if (!h) return GFT_E_INVALID;
     if (ns > 4000000000ull) return h->fail(GFT_E_INVALID, "gft_set_wait_limit: the limit is at most 4 s");
+    drop_graph(h);
     h->wait_limit_ns = (unsigned)ns;
     return GFT_OK;
 }
@@ -944,6 +1101,7 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
         return h->fail(GFT_E_UNSUPPORTED,
                        "gft_set_kernel: two sites per thread serve the periodic SM model in 8 x 32 or 16 x 16 tiles");
     if (kind == 1) {
+        drop_graph(h);
         h->kernel_kind = 1;
         return GFT_OK;
     }
@@ -951,11 +1109,13 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel has no Higgs-family field");
     if (h->cfg.form != GFT_FORM_MIXED) {
         if (kind >= 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
+        drop_graph(h);
         h->kernel_kind = 0;
         return GFT_OK;
     }
     if (tile < 0 || tile >= kTiledVariants) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad tile index");
     cudaSetDevice(h->cfg.device);
+    drop_graph(h);
     const StepParams P = make_params(h, h->time_iter, false);
     if (!tiled_supported(P, tile))
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the lattice shape does not divide into this tile");
@@ -1002,12 +1162,13 @@ double gft_step_kernel_ms(gft_handle* h, int* launches)
     if (!h || h->ev_used == 0) return 0.0;
     cudaEventSynchronize(h->ev[2 * (size_t)h->ev_used - 1]);
     double total = 0.0;
+    int n = 0;
     for (int i = 0; i < h->ev_used; i++) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev[2 * (size_t)i], h->ev[2 * (size_t)i + 1]);
         total += ms;
+        n += h->ev_steps[i];
     }
-    const int n = h->ev_used;
     h->ev_used = 0;
     if (launches) *launches = n;
     return total / n;
@@ -1042,6 +1203,7 @@ int gft_set_slab(gft_handle* h, int x_offset, int nx_global, int x_begin, int x_
         return h->fail(GFT_E_INVALID, "gft_set_slab: need 0 <= x_begin < x_end <= nx and nx_global >= 1");
     if (h->cfg.fixed_axes & 1)
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_slab: x-slabs need a periodic x axis (Fixed x faces given)");
+    drop_graph(h);
     h->x_offset = x_offset;
     h->nx_global = nx_global;
     h->x_begin = x_begin;
@@ -1088,6 +1250,7 @@ int gft_set_slab_nccl(gft_handle* h, const unsigned char* id, int nranks, int ra
     SlabComm* c = nullptr;
     const int rc = slab_comm_create(id, nranks, rank, &c, why);
     if (rc != GFT_OK) return h->fail(rc, "gft_set_slab_nccl: " + why);
+    drop_graph(h);
     h->comm = c;
     h->comm_timeout_s = timeout_s;
     return GFT_OK;
@@ -1097,6 +1260,7 @@ int gft_set_exchange(gft_handle* h, gft_exchange_fn fn, void* user)
 {
     if (!h) return GFT_E_INVALID;
     if (fn && h->comm) return h->fail(GFT_E_STATE, "gft_set_exchange: the NCCL exchange of gft_set_slab_nccl is set");
+    drop_graph(h);
     h->exchange = fn;
     h->exchange_user = user;
     return GFT_OK;

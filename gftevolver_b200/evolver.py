@@ -278,6 +278,10 @@ class Evolver:
             self.lib.gft_evolve(self.h, int(n_steps), rows, int(max_rows), ctypes.byref(n)), self.h)
         return [_row_dict(rows[i], self.params.neq) for i in range(n.value)]
 
+    def set_graphs(self, on: bool = True) -> None:
+        """Replay whole logging periods of small lattices from a CUDA graph (default) or launch directly."""
+        _lib.check(self.lib.gft_set_graphs(self.h, int(bool(on))), self.h)
+
     def set_wait_limit(self, ns: int = 0) -> None:
         """Time limit of the tiled kernel's plane waits in ns (0: the 2 s default); see gft_set_wait_limit."""
         _lib.check(self.lib.gft_set_wait_limit(self.h, int(ns)), self.h)

@@ -281,6 +281,16 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
  * Higgs-family field (one thread per site serves those). */
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march);
 
+/* Launch mode of gft_evolve (no reference counterpart).  on != 0 (the default):
+ * lattices of up to 4,194,304 sites (160^3), without an x-slab exchange or local
+ * analyser outputs, replay each whole logging period (lcm of 2 and the analyser
+ * cadences, after the damped steps) from a CUDA graph captured once, so short
+ * steps pay no host launch each; the results are those of the launches one by
+ * one.  For such periods gft_step_kernel_ms averages the whole period's device
+ * time per step (step kernels, reductions and Gauss passes).  on = 0 launches
+ * every kernel directly. */
+int gft_set_graphs(gft_handle* h, int on);
+
 /* Diagnostic with no reference counterpart: the time limit, in nanoseconds, of
  * the tiled kernel's waits for its staged planes, at most 4e9 (0 restores the
  * default, 2 s).

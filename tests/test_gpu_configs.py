@@ -242,3 +242,39 @@ def test_thousand_step_precision_at_256():
     assert g64 <= 1e-12, g64
     assert g32 <= 1e-5, g32
     assert d_sc <= 1e-3 and d_ve <= 1e-3, (d_sc, d_ve)
+
+
+# ---------------------------------------------------------------------------
+# small lattices: whole logging periods replayed from a CUDA graph
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("form,shape,every,steps", [
+    ("fp64", (32, 32, 32), (10, 10), 47),    # configuration 1; a tail shorter than a period
+    ("mixed", (8, 8, 32), (3, 2), 20),       # tiled kernel, period lcm(2, 3, 2) = 6
+    ("ref32", (6, 5, 4), (2, 3), 13),        # reference arithmetic, odd shape
+])
+def test_graph_replay_equals_direct_launches(form, shape, every, steps):
+    from gftevolver_b200 import Evolver, InitialData, LatticeParams
+    nx, ny, nz = shape
+    p = LatticeParams(nx=nx, ny=ny, nz=nz, energy_every=every[0], gauss_every=every[1])
+    ic = InitialData(seed=5, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    out = []
+    for graphs in (True, False):
+        with Evolver(p, form=form) as ev:
+            ev.set_graphs(graphs)
+            ev.init_fields(ic)
+            l0 = ev.launch_count
+            rows = ev.evolve(5)          # starts off a period boundary, then whole periods and a tail
+            rows += ev.evolve(steps)
+            launches = ev.launch_count - l0
+            assert ev.time_iter == 5 + steps
+            out.append((ev.download(), rows, launches))
+    (a, ra, la), (b, rb, lb) = out
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert la == lb
+    assert [r["time_iter"] for r in ra] == [r["time_iter"] for r in rb]
+    for x, y in zip(ra, rb):
+        for k in ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "plaq_su2", "plaq_u1",
+                  "phi_sq"):
+            assert x[k] == y[k], k
+        assert x["gauss_max"] == y["gauss_max"] and x["gauss_int"] == y["gauss_int"]
