@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--exchange", choices=["library", "python"], default="library",
                     help="x-slabs (--slab, N > 1): ghost-plane exchange posted by the library over NCCL and "
                          "overlapped with the interior planes, or a per-step callback through torch.distributed")
+    ap.add_argument("--fp64-kernel", choices=["auto", "global", "tiled"], default="auto",
+                    help="step kernel of the FP64 form (its own line with --form fp64, or the comparison leg)")
     ap.add_argument("--kernel", choices=["auto", "global", "tiled", "pair"], default="auto",
                     help="step kernel of the throughput forms")
     ap.add_argument("--tile", type=int, default=0, help="tiled kernel: tile shape index (0: 8x32, 1: 4x32, 2: 4x16, 3: 16x16)")
@@ -511,6 +513,7 @@ def main():
     balg = B_ALG[(args.model, sbytes)]
 
     kind = {"auto": 0, "global": 1, "tiled": 2, "pair": 3}[args.kernel]
+    kind64 = {"auto": 0, "global": 1, "tiled": 2}[args.fp64_kernel]
 
     def make_runner(form_):
         """N = 1: the whole lattice.  N > 1: this rank's x-slab of an (N * n) x n x n lattice
@@ -529,6 +532,8 @@ def main():
         runner, ev = make_runner(form_)
         if form_ == "mixed" and (kind != 0 or args.tile != 0 or args.march != 32):
             ev.set_kernel(kind, args.tile, args.march)
+        if form_ == "fp64" and kind64 != 0:
+            ev.set_kernel(kind64, args.tile if kind64 == 2 else 0, args.march)
         runner.init_fields(ic)
         if warmup:
             runner.evolve(warmup)

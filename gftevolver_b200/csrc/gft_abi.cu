@@ -278,8 +278,13 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
     int ty, tz;
     tiled_tile(tile, ty, tz);
     for (int t = 0; t < 2; t++) {
-        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, true, &tm[t])) return false;
-        if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, false, &tp[t])) return false;
+        if (h->sbytes == 8) {
+            if (!tiled_encode_maps<double>(P, h->ld[t], h->nsc / 4, ty, tz, true, &tm[t])) return false;
+            if (!tiled_encode_maps<double>(P, h->ld[t], h->nsc / 4, ty, tz, false, &tp[t])) return false;
+        } else {
+            if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, true, &tm[t])) return false;
+            if (!tiled_encode_maps<float>(P, h->lf[t], h->nsc / 4, ty, tz, false, &tp[t])) return false;
+        }
     }
     return true;
 }
@@ -290,7 +295,10 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
 // need 130 KB of shared memory and leave one CTA per SM (30 % against 45 %).
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
-    if (h->cfg.form != GFT_FORM_MIXED || !h->tiled_ready || h->kernel_kind == 1 || h->hf != kHfNone) return false;
+    if (!h->tiled_ready || h->kernel_kind == 1 || h->hf != kHfNone) return false;
+    // the FP64 form: the staged SM step, on request (gft_set_kernel kind 2)
+    const bool fp64_tiled = h->cfg.form == GFT_FORM_FP64 && h->cfg.model == GFT_MODEL_SM && h->kernel_kind == 2;
+    if (h->cfg.form != GFT_FORM_MIXED && !fp64_tiled) return false;
     if (h->kernel_kind == 0 && h->cfg.model != GFT_MODEL_SM) return false;
     return tiled_supported(P, h->tile_variant);
 }
@@ -321,6 +329,11 @@ cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelP
     if (h->cfg.form == GFT_FORM_REF) {
         if (model == GFT_MODEL_SM) return launch_ref_step<S, kModelSM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
         return launch_ref_step<S, kModel2HDM>(P, now, past, h->d_status, h->d_part_e, energy, h->stream);
+    }
+    if constexpr (sizeof(S) == 8) {
+        if (model == GFT_MODEL_SM && use_tiled(h, P))
+            return launch_tiled_step<S, kModelSM>(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
+                                                  h->d_status, h->d_part_e, energy, st ? st : h->stream, xa, xn);
     }
     if constexpr (sizeof(S) == 4) {
         if (use_tiled(h, P)) {
@@ -1107,8 +1120,11 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     }
     if (kind >= 2 && h->hf != kHfNone)
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel has no Higgs-family field");
-    if (h->cfg.form != GFT_FORM_MIXED) {
-        if (kind >= 2) return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel serves the mixed form");
+    const bool fp64_sm = h->cfg.form == GFT_FORM_FP64 && h->cfg.model == GFT_MODEL_SM && kind == 2;
+    if (h->cfg.form != GFT_FORM_MIXED && !fp64_sm) {
+        if (kind >= 2)
+            return h->fail(GFT_E_UNSUPPORTED,
+                           "gft_set_kernel: the tiled kernel serves the mixed form and the FP64 form of the SM model");
         drop_graph(h);
         h->kernel_kind = 0;
         return GFT_OK;

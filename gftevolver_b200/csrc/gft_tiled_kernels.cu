@@ -14,10 +14,12 @@ namespace {
 
 using namespace tiled;
 
-// At least 512 threads per SM resident (two 8 x 32 tiles): caps registers at 128
-// per thread, which the logging-step variant would otherwise exceed.
+// Float: at least 512 threads per SM resident (two 8 x 32 tiles), which caps
+// registers at 128 per thread (the logging-step variant would otherwise exceed
+// it).  Double: the staged planes take 200-209 KB of shared memory, one CTA per
+// SM, so the registers are left uncapped (the FP64 body needs about 170).
 template <class S, int MODEL, int TY, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ)) tiled_step_kernel(const __grid_constant__ TMaps maps,
+__global__ void __launch_bounds__(TY * TZ, sizeof(S) == 4 ? 512 / (TY * TZ) : 1) tiled_step_kernel(const __grid_constant__ TMaps maps,
                                                              const __grid_constant__ TMaps pmaps, StepParams P,
                                                              FConst F, LevelPtrs<S> now, LevelPtrs<S> past, int lx,
                                                              int xa, int xn, unsigned* status, double* partials)
@@ -274,6 +276,9 @@ template bool tiled_encode_maps<double>(const StepParams&, const LevelPtrs<doubl
 template cudaError_t launch_tiled_step<float, kModelSM>(const TMaps&, const TMaps&, const StepParams&,
                                                         const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
                                                         unsigned*, double*, bool, cudaStream_t, int, int);
+template cudaError_t launch_tiled_step<double, kModelSM>(const TMaps&, const TMaps&, const StepParams&,
+                                                         const LevelPtrs<double>&, const LevelPtrs<double>&, int, int,
+                                                         unsigned*, double*, bool, cudaStream_t, int, int);
 template cudaError_t launch_tiled_step<float, kModel2HDM>(const TMaps&, const TMaps&, const StepParams&,
                                                           const LevelPtrs<float>&, const LevelPtrs<float>&, int, int,
                                                           unsigned*, double*, bool, cudaStream_t, int, int);
