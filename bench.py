@@ -66,7 +66,7 @@ def parse():
                          "overlapped with the interior planes, or a per-step callback through torch.distributed")
     ap.add_argument("--fp64-kernel", choices=["auto", "global", "tiled"], default="auto",
                     help="step kernel of the FP64 form (its own line with --form fp64, or the comparison leg)")
-    ap.add_argument("--kernel", choices=["auto", "global", "tiled", "pair"], default="auto",
+    ap.add_argument("--kernel", choices=["auto", "global", "tiled", "pair", "split"], default="auto",
                     help="step kernel of the throughput forms")
     ap.add_argument("--tile", type=int, default=0, help="tiled kernel: tile shape index (0: 8x32, 1: 4x32, 2: 4x16, 3: 16x16)")
     ap.add_argument("--march", type=int, default=32, help="tiled kernel: planes per CTA along x")
@@ -512,7 +512,7 @@ def main():
     sbytes = 8 if form in ("fp64", "ref64") else 4
     balg = B_ALG[(args.model, sbytes)]
 
-    kind = {"auto": 0, "global": 1, "tiled": 2, "pair": 3}[args.kernel]
+    kind = {"auto": 0, "global": 1, "tiled": 2, "pair": 3, "split": 4}[args.kernel]
     kind64 = {"auto": 0, "global": 1, "tiled": 2}[args.fp64_kernel]
 
     def make_runner(form_):

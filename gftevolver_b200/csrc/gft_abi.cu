@@ -85,13 +85,15 @@ struct gft_handle {
     size_t dev_bytes = 0;
     // step kernel selection for the throughput forms
     int kernel_kind = 0;    // 0 auto, 1 global-memory kernel, 2 tiled (TMA) kernel, 3 tiled with two
-                            // sites per thread on plain steps (SM)
+                            // sites per thread on plain steps (SM), 4 tiled with each site split
+                            // between two threads on plain steps (SM)
     int tile_variant = 0;   // tiled: index into the built tile shapes
     int march = 32;         // tiled: planes per CTA along x
     unsigned wait_limit_ns = 0;  // gft_set_wait_limit (0: the 2 s default)
     bool tiled_ready = false;
     TMaps tm[2];   // staged "now" planes (with halo), per level
     TMaps tp[2];   // past-level L2 prefetch boxes (no halo), per level
+    TMaps tm_split[2], tp_split[2];  // the same for the split-site kernel's tile (kernel kind 4)
     // x-slab of a larger lattice (gft_set_slab): planes [x_begin, x_end) are
     // this handle's own, the others are ghost copies of the neighbours' planes
     int x_begin = 0, x_end = 0;  // x_end = 0: all planes
@@ -311,6 +313,14 @@ bool use_pair(const gft_handle* h, const StepParams& P)
            tiled_pair_tile(h->tile_variant);
 }
 
+// Plain steps of the SM mixed form with each site split between two threads
+// (kernel kind 4): periodic lattices whose (ny, nz) divide into its tile.
+bool use_split(const gft_handle* h, const StepParams& P)
+{
+    return h->kernel_kind == 4 && h->cfg.model == GFT_MODEL_SM && P.fixed_axes == 0 && P.ny % kSplitTileY == 0 &&
+           P.nz % kSplitTileZ == 0;
+}
+
 int step_blocks(const gft_handle* h, const StepParams& P)
 {
     if (h->cfg.form == GFT_FORM_REF) return ref_launch_blocks(P);
@@ -338,6 +348,9 @@ cudaError_t launch_step(gft_handle* h, const StepParams& P, int tn, const LevelP
     if constexpr (sizeof(S) == 4) {
         if (use_tiled(h, P)) {
             cudaStream_t s = st ? st : h->stream;
+            if (!energy && use_split(h, P))
+                return launch_tiled_split_step(h->tm_split[tn], h->tp_split[1 - tn], P, now, past, h->march,
+                                               h->d_status, s, xa, xn);
             if (!energy && use_pair(h, P))
                 return launch_tiled_pair_step(h->tm[tn], h->tp[1 - tn], P, now, past, h->tile_variant, h->march,
                                               h->d_status, s, xa, xn);
@@ -1109,7 +1122,12 @@ int gft_set_wait_limit(gft_handle* h, unsigned long long ns)
 int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
 {
     if (!h) return GFT_E_INVALID;
-    if (kind < 0 || kind > 3 || march < 1) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad kind or march");
+    if (kind < 0 || kind > 4 || march < 1) return h->fail(GFT_E_INVALID, "gft_set_kernel: bad kind or march");
+    if (kind == 4 && (h->cfg.model != GFT_MODEL_SM || h->cfg.fixed_axes != 0 || h->cfg.ny % kSplitTileY != 0 ||
+                      h->cfg.nz % kSplitTileZ != 0))
+        return h->fail(GFT_E_UNSUPPORTED,
+                       "gft_set_kernel: the split-site step serves the periodic SM model with ny % 8 == 0 and "
+                       "nz % 16 == 0");
     if (kind == 3 && (h->cfg.model != GFT_MODEL_SM || h->cfg.fixed_axes != 0 || !tiled_pair_tile(tile)))
         return h->fail(GFT_E_UNSUPPORTED,
                        "gft_set_kernel: two sites per thread serve the periodic SM model in 8 x 32 or 16 x 16 tiles");
@@ -1138,6 +1156,12 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     TMaps tm[2], tp[2];
     if (!encode_tiled(h, P, tile, tm, tp))
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed");
+    if (kind == 4) {
+        for (int t = 0; t < 2; t++)
+            if (!tiled_encode_maps<float>(P, h->lf[t], 1, kSplitTileY, kSplitTileZ, true, &h->tm_split[t]) ||
+                !tiled_encode_maps<float>(P, h->lf[t], 1, kSplitTileY, kSplitTileZ, false, &h->tp_split[t]))
+                return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed (split tile)");
+    }
     const int nb = tiled_blocks(P, tile, march);
     if (nb > h->part_cap) {
         cudaStreamSynchronize(h->stream);
@@ -1314,6 +1338,7 @@ const char* gft_step_kernel_name(const gft_handle* h)
     if (h->cfg.form == GFT_FORM_REF) return "ref_step_kernel";
     const StepParams P = make_params(h, 0, false);
     if (!use_tiled(h, P)) return "fast_step_kernel";
+    if (use_split(h, P)) return "tiled_split_kernel";
     return use_pair(h, P) ? "tiled_pair_kernel" : "tiled_step_kernel";
 }
 

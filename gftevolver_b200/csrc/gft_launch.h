@@ -53,6 +53,13 @@ cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepP
 cudaError_t launch_tiled_pair_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
                                    const LevelPtrs<float>& now, const LevelPtrs<float>& past, int variant, int lx,
                                    unsigned* status, cudaStream_t stream, int xa = 0, int xn = -1);
+// The SM mixed form's plain steps with each site's update split between two
+// threads (links / scalars), kSplitTileY x kSplitTileZ tiles, 256 threads,
+// three CTAs per SM; its tensor maps are encoded for that tile.
+constexpr int kSplitTileY = 8, kSplitTileZ = 16;
+cudaError_t launch_tiled_split_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+                                    const LevelPtrs<float>& now, const LevelPtrs<float>& past, int lx,
+                                    unsigned* status, cudaStream_t stream, int xa = 0, int xn = -1);
 constexpr int kTiledVariants = 4;  // 8x32, 4x32, 4x16, 16x16 (TY x TZ)
 // Tile shapes the two-sites-per-thread kernel is built for (8 x 32 and 16 x 16:
 // 128 threads per CTA, two CTAs per SM).

@@ -6,6 +6,7 @@
 #include "gft_device.cuh"
 #include "gft_launch.h"
 #include "gft_pair_body.cuh"
+#include "gft_split_body.cuh"
 #include "gft_tiled_tile.cuh"
 
 namespace gft {
@@ -125,6 +126,93 @@ __global__ void __launch_bounds__(TY * TZ / 2, 2) tiled_pair_kernel(const __grid
             const int x = x0 + i;
             const int sa = (x * P.ny + y) * P.nz + z;
             pair::site_step2(F, PairAcc<TY, TZ>{}, n, past, sa, sa + sb_off, carry, warn, counts(P, x));
+        });
+    if (!ok && tid == 0) atomicOr(status, kErrTimeout);
+    if (warn) atomicOr(status, warn);
+}
+
+// Shared memory of the split-site kernel: the ring, its barriers, the halo
+// staging (when it fits) and the scalars-to-links handoff.
+template <int TY, int TZ>
+struct SplitLayout {
+    using G = Geom<float, TY, TZ, 1>;
+    using H = HaloStage<float, TY, TZ, 1>;
+    using HO = split::Handoff<TY * TZ>;
+    static constexpr bool kStage = H::kUse;
+    static constexpr int OFF_HO = kStage ? (H::OFFSET + H::BYTES + 15) / 16 * 16 : G::NBUF * G::BUF + 64;
+    static constexpr int SMEM = OFF_HO + HO::kBytes + 128;  // + alignment slack of the dynamic base
+};
+
+__device__ __forceinline__ void named_arrive(int id, int count)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Plain steps of the SM mixed form with each site's update divided between two
+// threads (gft_split_body.cuh): warps 0 .. NT/32 - 1 take the links of the
+// tile's sites, the next NT/32 warps the scalars of the same sites; warp w of
+// the scalars hands E and J to warp w of the links through shared memory,
+// ordered by named barrier 1 + w (bar.arrive / bar.sync over the 64 threads of
+// the pair).  The plane ring, halo staging and bounded waits are run_ring's.
+// Three CTAs per SM: up to 85 registers per thread, 24 warps.
+template <int TY, int TZ>
+__global__ void __launch_bounds__(2 * TY * TZ, 3) tiled_split_kernel(const __grid_constant__ TMaps maps,
+                                                                    const __grid_constant__ TMaps pmaps, StepParams P,
+                                                                    FConst F, LevelPtrs<float> now,
+                                                                    LevelPtrs<float> past, int lx, int xa, int xn,
+                                                                    unsigned* status)
+{
+    using G = Geom<float, TY, TZ, 1>;
+    using L = SplitLayout<TY, TZ>;
+    constexpr int NT = TY * TZ;  // sites of the tile = threads per role
+    static_assert(NT % 32 == 0, "each role is whole warps");
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::NBUF * G::BUF);
+    const int tid = threadIdx.x;
+    const bool scalars = tid >= NT;  // warp-uniform
+    const int t = scalars ? tid - NT : tid;
+    const int ty = t / TZ, tz = t % TZ;
+    const int pair_bar = 1 + t / 32;
+
+    __shared__ int s_abort;
+    if (tid == 0) {
+        s_abort = 0;
+        for (int b = 0; b < G::NBUF; b++) mbar_init(&bars[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int y0 = blockIdx.y * TY, z0 = blockIdx.x * TZ, x0 = xa + blockIdx.z * lx;
+    const int cq0 = (ty + 1) * G::QP + (tz + 1);
+    const int ch0 = (ty + 1) * G::HP + (tz + 1) + G::TP - 1;
+    const int y = y0 + ty, z = z0 + tz;
+    const split::Handoff<NT> ho{reinterpret_cast<float*>(smem + L::OFF_HO), t};
+    split::ScalarCarry carry;
+    carry.valid = false;
+    unsigned warn = 0;
+    RingPhase ring = {0u};
+    const bool ok = run_ring<float, TY, TZ, 1, LevelPtrs<float>, L::kStage>(
+        maps, pmaps, P, now, y0, z0, x0, min(lx, xa + xn - x0), smem, bars, ring, &s_abort,
+        smem + HaloStage<float, TY, TZ, 1>::OFFSET, tid,
+        [&](int i, const unsigned char* bm, const unsigned char* bc, const unsigned char* bp) {
+            const Stencil<TRef> n = plane_stencil<G::QP, G::HP>(bm, bc, bp, cq0, ch0);
+            const int x = x0 + i;
+            const int s = (x * P.ny + y) * P.nz + z;
+            const unsigned warn_in = warn;
+            if (scalars) {
+                split::site_scalars(F, TileAcc<float, TY, TZ, 1>{}, n, past, s, carry, ho, warn);
+                named_arrive(pair_bar, 64);
+            } else {
+                split::site_links(F, TileAcc<float, TY, TZ, 1>{}, n, past, s, ho,
+                                  [&] { named_sync(pair_bar, 64); }, warn);
+            }
+            if (!counts(P, x)) warn = warn_in;  // ghost planes of an x-slab
         });
     if (!ok && tid == 0) atomicOr(status, kErrTimeout);
     if (warn) atomicOr(status, warn);
@@ -269,6 +357,21 @@ cudaError_t launch_tiled_pair_step(const TMaps& maps, const TMaps& pmaps, const 
     // the 8 x 32 and 16 x 16 tiles (128 threads per CTA); tiled_pair_tile says which
     if (variant == 3) return launch_pair_t<16, 16>(maps, pmaps, P, now, past, lx, xa, xn, status, stream);
     return launch_pair_t<8, 32>(maps, pmaps, P, now, past, lx, xa, xn, status, stream);
+}
+
+cudaError_t launch_tiled_split_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P,
+                                    const LevelPtrs<float>& now, const LevelPtrs<float>& past, int lx,
+                                    unsigned* status, cudaStream_t stream, int xa, int xn)
+{
+    constexpr int TY = kSplitTileY, TZ = kSplitTileZ;
+    using L = SplitLayout<TY, TZ>;
+    if (xn < 0) xn = P.nx - xa;
+    const dim3 block(2 * TY * TZ, 1, 1);
+    const dim3 grid(P.nz / TZ, P.ny / TY, (xn + lx - 1) / lx);
+    auto k = tiled_split_kernel<TY, TZ>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+    k<<<grid, block, L::SMEM, stream>>>(maps, pmaps, P, make_fconst(P), now, past, lx, xa, xn, status);
+    return cudaGetLastError();
 }
 
 template bool tiled_encode_maps<float>(const StepParams&, const LevelPtrs<float>&, int, int, int, bool, TMaps*);
