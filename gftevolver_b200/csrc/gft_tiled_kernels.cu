@@ -15,12 +15,23 @@ namespace {
 
 using namespace tiled;
 
-// Float: at least 512 threads per SM resident (two 8 x 32 tiles), which caps
-// registers at 128 per thread (the logging-step variant would otherwise exceed
-// it).  Double: the staged planes take 200-209 KB of shared memory, one CTA per
-// SM, so the registers are left uncapped (the FP64 body needs about 170).
+// CTAs per SM the launch bounds ask for: as many as shared memory admits, at
+// most 512 threads per SM.  For the SM model in float with 8 x 32 or 16 x 16
+// tiles that is two, which caps registers at 128 per thread (the logging-step
+// variant would otherwise exceed it); where the staged planes admit one CTA
+// (FP64, the 2HDM model's two doublets) the registers are left uncapped.
+template <class S, int MODEL, int TY, int TZ>
+constexpr int tiled_min_blocks()
+{
+    using G = Geom<S, TY, TZ, (MODEL == kModelSM) ? 1 : 2>;
+    constexpr int by_smem = (228 * 1024) / (G::SMEM + 16 + 1024);
+    constexpr int by_threads = 512 / (TY * TZ);
+    constexpr int b = by_smem < by_threads ? by_smem : by_threads;
+    return b < 1 ? 1 : b;
+}
+
 template <class S, int MODEL, int TY, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(TY * TZ, sizeof(S) == 4 ? 512 / (TY * TZ) : 1) tiled_step_kernel(const __grid_constant__ TMaps maps,
+__global__ void __launch_bounds__(TY * TZ, tiled_min_blocks<S, MODEL, TY, TZ>()) tiled_step_kernel(const __grid_constant__ TMaps maps,
                                                              const __grid_constant__ TMaps pmaps, StepParams P,
                                                              FConst F, LevelPtrs<S> now, LevelPtrs<S> past, int lx,
                                                              int xa, int xn, unsigned* status, double* partials)
