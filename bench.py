@@ -673,7 +673,10 @@ def main():
                    "kernel": args.kernel, "tile": args.tile, "march": args.march},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": kernel_name,
-                     "bytes_per_site_update": balg, "avg_kernel_ms": kms, "kernel_launches_timed": nk},
+                     "bytes_per_site_update": balg, "avg_kernel_ms": kms, "kernel_launches_timed": nk,
+                     # clock-normalised step time (ms x median SM MHz under load): compares runs on
+                     # boxes whose clocks differ (a power cap lowers them for this issue-bound kernel)
+                     "kernel_ms_x_sm_mhz": (kms * clocks["sm_mhz"]) if clocks and clocks.get("sm_mhz") else None},
         "gpu_launches": launches,
         "clocks": clocks,
         "forms": {"fp64": fp64} if fp64 else None,
