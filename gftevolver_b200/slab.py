@@ -152,6 +152,21 @@ def combine_rows(rows: list[dict], own_sites: int, group=None, device=None) -> l
     return out
 
 
+def share_id(make_id, rank: int, world: int, group=None) -> bytes:
+    """Bytes made by rank 0 of the group (make_id()), the same on every rank: the id a
+    group of ranks uses to join one NCCL communicator (any torch.distributed backend)."""
+    import torch.distributed as dist
+    data = make_id() if rank == 0 else None
+    if world > 1:
+        if not (dist.is_available() and dist.is_initialized()):
+            raise RuntimeError("sharing an id over several ranks needs an initialised process group")
+        obj = [data]
+        src = 0 if group is None else dist.get_global_rank(group, 0)
+        dist.broadcast_object_list(obj, src=src, group=group)
+        data = obj[0]
+    return data
+
+
 class _DeviceBuffer:
     """A device range as a CUDA-array-interface object (zero-copy torch view)."""
 
@@ -214,18 +229,14 @@ class SlabEvolver:
 
     def _join_nccl(self, timeout_s: float) -> None:
         """One NCCL communicator over the ranks of the group: rank 0 makes its id, the group shares it."""
-        import torch.distributed as dist
         lib, h = self.local.lib, self.local.h
-        id_buf = ctypes.create_string_buffer(128)
-        if self.rank == 0:
-            _lib.check(lib.gft_nccl_unique_id(id_buf))
-        if self.world > 1:
-            if not (dist.is_available() and dist.is_initialized()):
-                raise RuntimeError("exchange='library' over several ranks needs an initialised process group")
-            obj = [id_buf.raw if self.rank == 0 else None]
-            src = 0 if self.group is None else dist.get_global_rank(self.group, 0)
-            dist.broadcast_object_list(obj, src=src, group=self.group)
-            id_buf = ctypes.create_string_buffer(obj[0], 128)
+
+        def make_id() -> bytes:
+            buf = ctypes.create_string_buffer(128)
+            _lib.check(lib.gft_nccl_unique_id(buf))
+            return buf.raw
+
+        id_buf = ctypes.create_string_buffer(share_id(make_id, self.rank, self.world, self.group), 128)
         _lib.check(lib.gft_set_slab_nccl(h, id_buf, self.world, self.rank, float(timeout_s)), h)
 
     # plane views of the library's field storage

@@ -120,3 +120,41 @@ def test_partition_covers_every_plane_once():
             assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
     with pytest.raises(ValueError):
         partition(3, 4, 0)
+
+
+def _share_worker(rank, world, port, out_dir):
+    import datetime
+    import os
+
+    import torch.distributed as dist
+
+    from gftevolver_b200.slab import share_id
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        calls = []
+
+        def make_id():
+            calls.append(1)
+            return os.urandom(128)
+
+        got = share_id(make_id, rank, world)
+        with open(os.path.join(out_dir, f"id{rank}.bin"), "wb") as f:
+            f.write(got)
+        with open(os.path.join(out_dir, f"calls{rank}.txt"), "w") as f:
+            f.write(str(len(calls)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_communicator_id_is_made_once_and_shared(tmp_path, world):
+    """The library-side slab exchange joins one NCCL communicator per group of ranks: rank 0
+    alone makes the 128-byte id, and every rank ends up with the same bytes (gloo ranks on CPU)."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_share_worker, args=(world, port, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    ids = [(tmp_path / f"id{r}.bin").read_bytes() for r in range(world)]
+    assert len(ids[0]) == 128 and all(x == ids[0] for x in ids)
+    assert [int((tmp_path / f"calls{r}.txt").read_text()) for r in range(world)] == [1] + [0] * (world - 1)
