@@ -278,3 +278,26 @@ def test_graph_replay_equals_direct_launches(form, shape, every, steps):
                   "phi_sq"):
             assert x[k] == y[k], k
         assert x["gauss_max"] == y["gauss_max"] and x["gauss_int"] == y["gauss_int"]
+
+
+def test_graph_replay_across_damping_and_a_kernel_switch():
+    """Damped steps launch one by one and the graph takes over after them; switching the
+    kernel mid-run drops the captured period and the next one is captured afresh."""
+    from gftevolver_b200 import Evolver, InitialData, LatticeParams
+    p = LatticeParams(nx=8, ny=8, nz=32, energy_every=4, gauss_every=2, damping=1.0, nt_damped=7)
+    ic = InitialData(seed=6, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    out = []
+    for graphs in (True, False):
+        with Evolver(p, form="mixed") as ev:
+            ev.set_graphs(graphs)
+            ev.init_fields(ic)
+            rows = ev.evolve(13)           # damped 0..6, then whole periods of 4
+            ev.set_kernel(1, 0, 32)         # one thread per site from here on
+            rows += ev.evolve(9)
+            out.append((ev.download(), rows))
+    (a, ra), (b, rb) = out
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert [r["time_iter"] for r in ra] == [r["time_iter"] for r in rb]
+    assert [r["energy"] for r in ra] == [r["energy"] for r in rb]
+    assert [r["gauss_max"] for r in ra] == [r["gauss_max"] for r in rb]
