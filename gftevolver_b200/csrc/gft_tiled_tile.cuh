@@ -507,6 +507,9 @@ __device__ __forceinline__ bool run_tile(const TMaps& maps, const TMaps& pmaps, 
             const int s = (x * P.ny + y) * P.nz + z;
             if (frozen(P, x, y, z))  // Fixed faces: not evolved, and the next site recomputes what it carries
                 carry.valid = false;
+            else if (carry.valid)  // every site of the march after the first (uniform without Fixed faces)
+                site_step<S, MODEL, ENERGY, kHfNone, true>(P, F, TileAcc<S, TY, TZ, ND>{}, n,
+                                                           PastSite<S, LV>{past, s}, carry, obs, warn, counts(P, x));
             else
                 site_step<S, MODEL, ENERGY>(P, F, TileAcc<S, TY, TZ, ND>{}, n, PastSite<S, LV>{past, s}, carry, obs,
                                             warn, counts(P, x));
