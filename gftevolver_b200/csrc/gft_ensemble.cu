@@ -88,10 +88,13 @@ __device__ __forceinline__ void tmap_acquire(const TMaps& m)
         asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&m.ph[k]) : "memory");
 }
 
-// One persistent launch per step: CTA b evolves tiles b, b + G, b + 2G, ...
-// items[i] = {member within the group, y0, z0, x0}; tile i's energy partials
-// go to partials row i.  UNIFORM: the members share ep.common but for their
-// geometry (the per-member fields copied below).
+// One persistent launch per step.  CTA b evolves the tiles of its list,
+// order[start[b]] .. order[start[b + 1] - 1] (balanced by the host: tile costs
+// differ with the planes of the x-chunk), when the grid has the list count
+// nlist; otherwise tiles b, b + G, b + 2G, ...  items[i] = {member within the
+// group, y0, z0, x0}; tile i's energy partials go to partials row i.  UNIFORM:
+// the members share ep.common but for their geometry (the per-member fields
+// copied below).
 // Plain steps stage the wrapped halo sites (run_tile's STAGE) where the staging
 // area leaves the resident CTAs per SM unchanged; the dynamic shared memory
 // then includes it.
@@ -110,7 +113,8 @@ constexpr int ens_smem()
 template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
 __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
     ensemble_step_kernel(const __grid_constant__ EnsParams ep, const EnsMaps* __restrict__ maps,
-                         const int4* __restrict__ items, int nitems, int lx, int tn, unsigned* status,
+                         const int4* __restrict__ items, int nitems, const int* __restrict__ order,
+                         const int* __restrict__ start, int nlist, int lx, int tn, unsigned* status,
                          double* partials)
 {
     constexpr int ND = (MODEL == kModelSM) ? 1 : 2;
@@ -131,7 +135,12 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
 
     RingPhase ring = {0u};
     unsigned warn = 0;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const bool listed = order != nullptr && (int)gridDim.x == nlist;
+    const int k0 = listed ? start[blockIdx.x] : (int)blockIdx.x;
+    const int k1 = listed ? start[blockIdx.x + 1] : nitems;
+    const int kstep = listed ? 1 : (int)gridDim.x;
+    for (int k = k0; k < k1; k += kstep) {
+        const int it = listed ? order[k] : k;
         const int4 w = items[it];
         const int m = w.x;
         const EnsMaps& mp = maps[m];
@@ -238,24 +247,33 @@ int resident_ctas()
     return per_sm;
 }
 
+// A group's tiles and their per-CTA lists (balance_tiles): CTA c of a grid of
+// nlist evolves items[order[k]] for k in [start[c], start[c + 1]).
+struct GroupTiles {
+    const int4* items;
+    int nitems;
+    const int* order;
+    const int* start;
+    int nlist;
+};
+
 template <int MODEL, int TY, int TZ, bool ENERGY, bool UNIFORM>
-cudaError_t launch_step_u(const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems, int lx, int tn,
+cudaError_t launch_step_u(const EnsParams& ep, const EnsMaps* maps, const GroupTiles& gt, int lx, int tn,
                           unsigned* status, double* partials, int nsm, cudaStream_t s)
 {
-    const int grid = std::min(nitems, nsm * resident_ctas<MODEL, TY, TZ, ENERGY, UNIFORM>());
+    const int grid = std::min(gt.nitems, nsm * resident_ctas<MODEL, TY, TZ, ENERGY, UNIFORM>());
     if (grid < 1) return cudaSuccess;
     ensemble_step_kernel<MODEL, TY, TZ, ENERGY, UNIFORM><<<grid, dim3(TZ, TY, 1), ens_smem<MODEL, TY, TZ, ENERGY>(), s>>>(
-        ep, maps, items, nitems, lx, tn, status, partials);
+        ep, maps, gt.items, gt.nitems, gt.order, gt.start, gt.nlist, lx, tn, status, partials);
     return cudaGetLastError();
 }
 
 template <int MODEL, int TY, int TZ, bool ENERGY>
-cudaError_t launch_step_t(bool uniform, const EnsParams& ep, const EnsMaps* maps, const int4* items, int nitems,
-                          int lx, int tn, unsigned* status, double* partials, int nsm, cudaStream_t s)
+cudaError_t launch_step_t(bool uniform, const EnsParams& ep, const EnsMaps* maps, const GroupTiles& gt, int lx,
+                          int tn, unsigned* status, double* partials, int nsm, cudaStream_t s)
 {
-    return uniform ? launch_step_u<MODEL, TY, TZ, ENERGY, true>(ep, maps, items, nitems, lx, tn, status, partials, nsm, s)
-                   : launch_step_u<MODEL, TY, TZ, ENERGY, false>(ep, maps, items, nitems, lx, tn, status, partials, nsm,
-                                                                 s);
+    return uniform ? launch_step_u<MODEL, TY, TZ, ENERGY, true>(ep, maps, gt, lx, tn, status, partials, nsm, s)
+                   : launch_step_u<MODEL, TY, TZ, ENERGY, false>(ep, maps, gt, lx, tn, status, partials, nsm, s);
 }
 
 template <int MODEL, int TY, int TZ>
@@ -278,6 +296,18 @@ void prime_variant(int variant)
     }
 }
 
+// Resident CTAs per SM of the plain-step (uniform) instance of a tile shape.
+template <int MODEL>
+int resident_m(int variant)
+{
+    switch (variant) {
+    case 0: return resident_ctas<MODEL, 8, 32, false, true>();
+    case 1: return resident_ctas<MODEL, 4, 32, false, true>();
+    case 2: return resident_ctas<MODEL, 4, 16, false, true>();
+    default: return resident_ctas<MODEL, 16, 16, false, true>();
+    }
+}
+
 template <int MODEL, int TY, int TZ>
 cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, int lx, int tn, double* partials,
                            cudaStream_t s)
@@ -289,14 +319,12 @@ cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, i
 
 template <int MODEL>
 cudaError_t launch_step_m(int variant, bool energy, bool uniform, const EnsParams& ep, const EnsMaps* maps,
-                          const int4* items, int nitems, int lx, int tn, unsigned* status, double* partials, int nsm,
+                          const GroupTiles& gt, int lx, int tn, unsigned* status, double* partials, int nsm,
                           cudaStream_t s)
 {
-#define GFT_ENS_STEP(TY, TZ)                                                                                         \
-    return energy ? launch_step_t<MODEL, TY, TZ, true>(uniform, ep, maps, items, nitems, lx, tn, status, partials,  \
-                                                       nsm, s)                                                       \
-                  : launch_step_t<MODEL, TY, TZ, false>(uniform, ep, maps, items, nitems, lx, tn, status, partials, \
-                                                        nsm, s)
+#define GFT_ENS_STEP(TY, TZ)                                                                                    \
+    return energy ? launch_step_t<MODEL, TY, TZ, true>(uniform, ep, maps, gt, lx, tn, status, partials, nsm, s) \
+                  : launch_step_t<MODEL, TY, TZ, false>(uniform, ep, maps, gt, lx, tn, status, partials, nsm, s)
     switch (variant) {
     case 0: GFT_ENS_STEP(8, 32);
     case 1: GFT_ENS_STEP(4, 32);
@@ -346,6 +374,9 @@ struct gft_batch {
     int lx = 32;
     int4* d_items = nullptr;
     int nitems = 0;
+    int* d_order = nullptr;       // per-CTA tile lists of each group (group-local item indices)
+    int* d_start = nullptr;       // list bounds: group g's nlist + 1 entries from group_start[g]
+    std::vector<int> group_start, group_nlist;
     std::vector<int> group_item;  // first item of each group (+ end)
     int* d_first = nullptr;       // first item of each member (+ end)
     double* d_part_e = nullptr;
@@ -447,6 +478,37 @@ bool fill_params(const gft_batch* b, int g, int ti, bool energy, EnsParams* ep)
     return uniform;
 }
 
+// Per-CTA tile lists of one group for a grid of G CTAs: the tiles by
+// decreasing cost, each to the CTA with the least work so far (cost: the planes
+// of its x-chunk plus three for filling the plane ring), then each CTA's tiles
+// in item order.  Static striding over tiles of uneven x-chunks (a 48-plane
+// member in chunks of 32 and 16) leaves the busiest CTA 13 % above the mean on
+// the 64-member benchmark; these lists bring it within 1 %.
+void balance_tiles(const std::vector<int4>& items, int i0, int ni, const std::vector<gft_config>& cfg, int m0, int lx,
+                   int G, std::vector<int>& order, std::vector<int>& start)
+{
+    std::vector<int> cost(ni), idx(ni);
+    for (int i = 0; i < ni; i++) {
+        const int4 w = items[i0 + i];
+        cost[i] = std::min(lx, cfg[m0 + w.x].nx - w.w) + 3;
+        idx[i] = i;
+    }
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    std::vector<long long> load(G, 0);
+    std::vector<std::vector<int>> lists(G);
+    for (int i : idx) {
+        const int c = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[c] += cost[i];
+        lists[c].push_back(i);
+    }
+    start.assign(1, (int)order.size());
+    for (auto& l : lists) {
+        std::sort(l.begin(), l.end());
+        order.insert(order.end(), l.begin(), l.end());
+        start.push_back((int)order.size());
+    }
+}
+
 // Tile list, tensor maps and partial buffers for a tile shape and march depth.
 int configure(gft_batch* b, int variant, int lx)
 {
@@ -500,6 +562,30 @@ int configure(gft_batch* b, int variant, int lx)
         prime_variant<kModelSM>(variant);
     else
         prime_variant<kModel2HDM>(variant);
+    // per-CTA lists for the plain-step grid (a launch with another grid strides)
+    const int per_sm = (b->model == GFT_MODEL_SM) ? resident_m<kModelSM>(variant) : resident_m<kModel2HDM>(variant);
+    std::vector<int> order, starts;
+    b->group_start.assign(b->ngroups(), 0);
+    b->group_nlist.assign(b->ngroups(), 0);
+    for (int g = 0; g < b->ngroups(); g++) {  // group g's lists fill order[group_item[g] ..]
+        const int i0 = b->group_item[g], ni = b->group_item[g + 1] - i0;
+        const int G = std::max(1, std::min(ni, b->nsm * per_sm));
+        std::vector<int> st;
+        balance_tiles(items, i0, ni, b->cfg, g * kGroup, lx, G, order, st);
+        b->group_start[g] = (int)starts.size();
+        b->group_nlist[g] = G;
+        starts.insert(starts.end(), st.begin(), st.end());
+    }
+    cudaFree(b->d_order);
+    cudaFree(b->d_start);
+    b->d_order = b->d_start = nullptr;
+    e = cudaMalloc(&b->d_order, std::max<size_t>(order.size(), 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_start, std::max<size_t>(starts.size(), 1) * sizeof(int));
+    if (e == cudaSuccess && !order.empty())
+        e = cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !starts.empty())
+        e = cudaMemcpy(b->d_start, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return b->cuda_fail(e, "gft_batch: configure");
     drop_graph(b);
     return GFT_OK;
 }
@@ -514,11 +600,12 @@ cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long 
         const bool uniform = fill_params(b, gr, ti, e, &ep);
         const int i0 = b->group_item[gr], ni = b->group_item[gr + 1] - i0;
         const EnsMaps* maps = b->d_maps + (size_t)gr * kGroup;
+        const GroupTiles gt{b->d_items + i0, ni, b->d_order, b->d_start + b->group_start[gr], b->group_nlist[gr]};
         err = (b->model == GFT_MODEL_SM)
-                  ? launch_step_m<kModelSM>(b->variant, e, uniform, ep, maps, b->d_items + i0, ni, b->lx, tn,
-                                            b->d_status, b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream)
-                  : launch_step_m<kModel2HDM>(b->variant, e, uniform, ep, maps, b->d_items + i0, ni, b->lx, tn,
-                                              b->d_status, b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream);
+                  ? launch_step_m<kModelSM>(b->variant, e, uniform, ep, maps, gt, b->lx, tn, b->d_status,
+                                            b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream)
+                  : launch_step_m<kModel2HDM>(b->variant, e, uniform, ep, maps, gt, b->lx, tn, b->d_status,
+                                              b->d_part_e + (size_t)i0 * kObsCount, b->nsm, b->stream);
         (*nlaunch)++;
     }
     if (err == cudaSuccess && e) {
@@ -747,6 +834,8 @@ void gft_batch_destroy(gft_batch* b)
     cudaFree(b->arena);
     cudaFree(b->d_maps);
     cudaFree(b->d_items);
+    cudaFree(b->d_order);
+    cudaFree(b->d_start);
     cudaFree(b->d_first);
     cudaFree(b->d_part_e);
     cudaFree(b->d_part_g);
