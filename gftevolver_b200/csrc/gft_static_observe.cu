@@ -31,6 +31,7 @@
 #include "gft.h"
 #include "gft_device.cuh"
 #include "gft_launch.h"
+#include "gft_step_body.cuh"
 
 namespace gft {
 namespace {
@@ -49,17 +50,30 @@ std::mutex g_static_mu;
 double* g_static_addr[kMaxDevices] = {};
 
 // Observables of the state at the level pair (now, past), read from the
-// reference AoS layout: scalars[2][N][nsc], vectors[2][N][15].
+// reference AoS layout: scalars[2][N][nsc], vectors[2][N][3 dw], per direction
+// dw words: theta, the SU(2) quaternion, then the 2HDM Higgs-family field --
+// none (dw = 5), its U(1) phase (6) or its SU(2) quaternion (9)
+// (WilsonLoops/Source/TwoHDM.cpp:210-242).
 struct AosView {
     const float* sc;
     const float* ve;
-    int nsc, N;
+    int nsc, N, dw, hf;
+    __device__ __forceinline__ const float* link(int lvl, int s, int d) const
+    {
+        return ve + ((size_t)lvl * N + s) * (3 * dw) + dw * d;
+    }
     __device__ __forceinline__ Q<double> q(int lvl, int s, int d) const
     {
-        const float* v = ve + ((size_t)lvl * N + s) * 15 + 5 * d;
+        const float* v = link(lvl, s, d);
         return {(double)v[1], (double)v[2], (double)v[3], (double)v[4]};
     }
-    __device__ __forceinline__ double th(int lvl, int s, int d) const { return (double)ve[((size_t)lvl * N + s) * 15 + 5 * d]; }
+    __device__ __forceinline__ double th(int lvl, int s, int d) const { return (double)link(lvl, s, d)[0]; }
+    __device__ __forceinline__ double hth(int lvl, int s, int d) const { return (double)link(lvl, s, d)[5]; }
+    __device__ __forceinline__ Q<double> hq(int lvl, int s, int d) const
+    {
+        const float* v = link(lvl, s, d);
+        return {(double)v[5], (double)v[6], (double)v[7], (double)v[8]};
+    }
     __device__ __forceinline__ Q<double> ph(int lvl, int s, int db) const
     {
         const float* f = sc + ((size_t)lvl * N + s) * nsc + 4 * db;
@@ -116,15 +130,38 @@ __global__ void __launch_bounds__(kStaticThreads) static_observe_kernel(StepPara
             obs[kObsPlaqSU2] += 1.0 - o;
             obs[kObsPlaqU1] += cos(F);
         }
+        // Higgs-family loops, coupling g'' (WilsonLoops/Source/TwoHDM.cpp:484-551)
+        if (A.hf == kHfU1) {
+            for (int pl = 0; pl < 3; pl++) {
+                const int i = (pl == 2) ? 1 : 0, j = (pl == 0) ? 1 : 2;
+                const double F = A.hth(tn, s, i) + A.hth(tn, pa[i], j) - A.hth(tn, pa[j], i) - A.hth(tn, s, j);
+                const double h = sin(0.5 * F);
+                obs[kObsMagnetic] += 4.0 * P.lap[i] * P.lap[j] * P.inv_gpp_sqr * 2.0 * h * h;
+            }
+        } else if (A.hf == kHfSU2) {
+            for (int pl = 0; pl < 3; pl++) {
+                const int i = (pl == 2) ? 1 : 0, j = (pl == 0) ? 1 : 2;
+                const Q<double> P1 = qmul(qmul(qmul(qconj(A.hq(tn, pa[i], j)), A.hq(tn, pa[j], i)), A.hq(tn, s, j)),
+                                          qconj(A.hq(tn, s, i)));
+                obs[kObsMagnetic] += 4.0 * P.lap[i] * P.lap[j] * P.inv_gpp_sqr * omt(P1);
+            }
+        }
         // electric energy: U_now U_past^dag and 1 - cos(dtheta)
         for (int d = 0; d < 3; d++) {
             const Q<double> E = qmul(U[d], qconj(A.q(tp, s, d)));
             const double h = sin(0.5 * (th[d] - A.th(tp, s, d)));
             obs[kObsElectric] += 4.0 * P.lap[d] * P.inv_sqr_dt * (P.inv_g_sqr * omt(E) + P.inv_gp_sqr * 2.0 * h * h);
+            if (A.hf == kHfU1) {  // (WilsonLoops/Source/TwoHDM.cpp:601-633)
+                const double hh = sin(0.5 * (A.hth(tn, s, d) - A.hth(tp, s, d)));
+                obs[kObsElectric] += 4.0 * P.lap[d] * P.inv_sqr_dt * P.inv_gpp_sqr * 2.0 * hh * hh;
+            } else if (A.hf == kHfSU2) {  // (WilsonLoops/Source/TwoHDM.cpp:702-745)
+                obs[kObsElectric] += 4.0 * P.lap[d] * P.inv_sqr_dt * P.inv_gpp_sqr *
+                                     omt(qmul(A.hq(tn, s, d), qconj(A.hq(tp, s, d))));
+            }
         }
-        // scalar sector: gradient, kinetic, potential, <phi^dag phi>
+        // scalar sector: kinetic, <phi^dag phi>, gradient, potential
         double fsq[2] = {0.0, 0.0}, dot = 0.0, anti = 0.0;
-        Q<double> f0 = A.ph(tn, s, 0), f1 = (nd == 2) ? A.ph(tn, s, 1) : f0;
+        const Q<double> f0 = A.ph(tn, s, 0), f1 = (nd == 2) ? A.ph(tn, s, 1) : f0;
         for (int db = 0; db < nd; db++) {
             const Q<double> f = (db == 0) ? f0 : f1;
             const Q<double> fo = A.ph(tp, s, db);
@@ -133,10 +170,21 @@ __global__ void __launch_bounds__(kStaticThreads) static_observe_kernel(StepPara
                          v3 = (f.z - fo.z) / P.dt;
             obs[kObsKinetic] += 0.5 * (v0 * v0 + v1 * v1 + v2 * v2 + v3 * v3);
             obs[kObsPhiSq] += fsq[db];
-            for (int a = 0; a < 3; a++) {
-                const Q<double> t = transport_d(U[a], cos(th[a]), sin(th[a]), f);
+        }
+        // the doublets transported along each link, then acted on by the Higgs-family
+        // field of that link (Gradients/Source/TwoHDM.cpp:118-146)
+        for (int a = 0; a < 3; a++) {
+            const double cs = cos(th[a]), sn = sin(th[a]);
+            Q<double> t[2] = {transport_d(U[a], cs, sn, f0), transport_d(U[a], cs, sn, f1)};
+            if (A.hf == kHfU1) {
+                const double ha = A.hth(tn, s, a);
+                hf_act<kHfU1>(t[0], t[1], cos(ha), sin(ha), Q<double>{1.0, 0.0, 0.0, 0.0});
+            } else if (A.hf == kHfSU2) {
+                hf_act<kHfSU2>(t[0], t[1], 1.0, 0.0, A.hq(tn, s, a));
+            }
+            for (int db = 0; db < nd; db++) {
                 const Q<double> n = A.ph(tn, pa[a], db);
-                const double e0 = n.w - t.w, e1 = n.x - t.x, e2 = n.y - t.y, e3 = n.z - t.z;
+                const double e0 = n.w - t[db].w, e1 = n.x - t[db].x, e2 = n.y - t[db].y, e3 = n.z - t[db].z;
                 obs[kObsGradient] += 0.5 * P.inv_dx[a] * P.inv_dx[a] * (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
             }
         }
@@ -224,8 +272,8 @@ extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, c
         set_last_error("gft_observe_static: periodic lattices only (fixed_axes must be 0)");
         return GFT_E_UNSUPPORTED;
     }
-    if (c->higgs_family != GFT_HF_NONE || c->generator_rep) {
-        set_last_error("gft_observe_static: quaternion links without a Higgs-family field only");
+    if (c->generator_rep) {
+        set_last_error("gft_observe_static: quaternion links only (generator_rep = 0)");
         return GFT_E_UNSUPPORTED;
     }
     const long long n = (long long)c->nx * c->ny * c->nz;
@@ -289,8 +337,12 @@ extern "C" int gft_observe_static(const gft_config* c, const float* d_scalars, c
     P.break_uhalfn = c->break_uhalfn;
     P.apply_norm = c->apply_norm;
     P.energy_offset = c->energy_offset;
+    const int hf = (c->model == GFT_MODEL_2HDM) ? c->higgs_family : GFT_HF_NONE;
+    const double gpp2 = c->gpp * c->gpp;
+    P.inv_gpp_sqr = (gpp2 > c->div_tol) ? 1.0 / gpp2 : 0.0;
     const int nsc = (c->model == GFT_MODEL_SM) ? 4 : 8;
-    const AosView A{d_scalars, d_vectors, nsc, (int)n};
+    const int dw = (hf == GFT_HF_SU2) ? 9 : (hf == GFT_HF_U1) ? 6 : 5;  // words per direction
+    const AosView A{d_scalars, d_vectors, nsc, (int)n, dw, hf};
     const int tn = (time_iter + 1) % 2;
     const int nblocks = (int)((n + kSitesPerBlock - 1) / kSitesPerBlock);
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -253,7 +253,8 @@ int gft_set_slab_nccl(gft_handle* h, const unsigned char* id, int nranks, int ra
  * synchronise the device), or fields owned by another framework's allocator.
  * Computes the energy terms, plaquette means and <phi^dag phi> of the state
  * at step `time_iter` from the caller's device buffers in the reference layout
- * (float: scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][15]) and writes
+ * (float: scalars[2][nx][ny][nz][nsc], vectors[2][nx][ny][nz][3 * w], w = 5
+ * words per direction, 6 or 9 with a 2HDM Higgs-family field) and writes
  * 9 doubles to the caller's device buffer d_out (energy, potential, gradient,
  * kinetic, magnetic, electric, plaq_su2, plaq_u1, phi_sq; the units of
  * gft_observables), asynchronously on `stream` (NULL: the default stream).
@@ -263,9 +264,9 @@ int gft_set_slab_nccl(gft_handle* h, const unsigned char* id, int nranks, int ra
  * stream capture) and keeps it for the life of the process, so a device that
  * has been reset with cudaDeviceReset must not be used with it again.  Calls
  * that overlap on the GPU share the array and race, so the caller serialises
- * them.  Only cfg's lattice, model and coupling fields
- * are read (form and storage_bytes are ignored); periodic lattices without a
- * Higgs-family field only (otherwise GFT_E_UNSUPPORTED). */
+ * them.  Only cfg's lattice, model, coupling and Higgs-family fields are read
+ * (form and storage_bytes are ignored); periodic lattices with quaternion links
+ * (generator_rep = 0) only, otherwise GFT_E_UNSUPPORTED. */
 int gft_observe_static(const gft_config* cfg, const float* d_scalars, const float* d_vectors, int time_iter,
                        double* d_out, void* stream);
 

@@ -45,7 +45,10 @@ KEYS = ("energy", "potential", "gradient", "kinetic", "magnetic", "electric", "p
 
 
 @pytest.mark.parametrize("model,shape,extra", [(1, (24, 16, 32), None), (2, (12, 10, 18), None),
-                                               (2, (10, 12, 14), COUPLED_2HDM)], ids=["sm", "2hdm", "2hdm_coupled"])
+                                               (2, (10, 12, 14), COUPLED_2HDM),
+                                               (2, (10, 12, 16), dict(higgs_family=1, gpp=0.45)),
+                                               (2, (12, 10, 14), dict(higgs_family=2, gpp=0.55))],
+                         ids=["sm", "2hdm", "2hdm_coupled", "2hdm_family_u1", "2hdm_family_su2"])
 def test_observe_static_matches_observe_twice(model, shape, extra):
     import torch
     from gftevolver_b200 import _lib
