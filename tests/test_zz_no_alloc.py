@@ -98,3 +98,44 @@ def test_observe_static_rejects_an_invalid_configuration_with_a_message():
         rc = lib.gft_observe_static(ctypes.byref(cfg), dummy, dummy, 0, dummy, None)
         assert rc == _lib.GFT_E_INVALID, bad
         assert _lib.last_error().startswith("gft_observe_static: "), _lib.last_error()
+
+
+def test_observe_static_is_captured_and_replayed_in_a_cuda_graph():
+    """The property the entry point exists for: after one call outside any capture
+    (which loads the library's module and looks up its scratch array), a call is
+    captured in a CUDA graph in global capture mode -- where any device allocation,
+    by this thread or another, fails the capture -- and its replay gives the same
+    numbers bit for bit."""
+    import torch
+    from gftevolver_b200 import _lib
+    from gftevolver_b200.evolver import make_config
+    lib = _lib.load()
+    p, ref, sc, ve, ti = _state(1, (16, 12, 32), 2)
+    cfg = make_config(p, "mixed", 0)
+    d_sc = torch.from_numpy(sc).cuda()
+    d_ve = torch.from_numpy(ve).cuda()
+    out = torch.empty(9, dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+
+    def call(stream):
+        return lib.gft_observe_static(ctypes.byref(cfg), ctypes.c_void_p(d_sc.data_ptr()),
+                                      ctypes.c_void_p(d_ve.data_ptr()), ti, ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(stream.cuda_stream))
+
+    with torch.cuda.stream(side):
+        assert call(side) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    first = out.clone()
+    out.fill_(float("nan"))
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side, capture_error_mode="global"):
+        rc = call(torch.cuda.current_stream())
+    assert rc == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    assert torch.isnan(out).all()  # capturing ran nothing
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out, first)
+    assert abs(first[0].item() - ref["energy"]) <= 1e-6 * abs(ref["energy"])
+    del graph
