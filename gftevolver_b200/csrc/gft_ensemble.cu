@@ -183,13 +183,17 @@ __global__ void __launch_bounds__(TY * TZ, 512 / (TY * TZ))
     if (warn) atomicOr(status, warn);
 }
 
-// Gauss-law residual over the same tiles (one CTA per tile, x-march over its planes).
+// Gauss-law residual over the same tiles: CTA (tile, i) takes plane i of the
+// tile's x-chunk, one thread per site (independent loads; a march of the
+// chunk's planes per thread serialises them: 0.948 against 0.866 ms on the
+// 64-member benchmark with 16 x 16 tiles, march 64), and writes partial row
+// tile * gridDim.y + i (zeros past the chunk's end).
 template <int MODEL, int TY, int TZ>
 __global__ void __launch_bounds__(TY * TZ) ensemble_gauss_kernel(const __grid_constant__ EnsParams ep,
                                                                  const int4* __restrict__ items, int lx, int tn,
                                                                  double* partials)
 {
-    const int it = blockIdx.x;
+    const int it = blockIdx.x, i = blockIdx.y;
     const int4 w = items[it];
     const int m = w.x;
     const StepParams& P = ep.P[m];
@@ -198,32 +202,25 @@ __global__ void __launch_bounds__(TY * TZ) ensemble_gauss_kernel(const __grid_co
     double v[kGaussSlots];
 #pragma unroll
     for (int k = 0; k < kGaussSlots; k++) v[k] = 0.0;
-    const int nloc = min(lx, P.nx - w.w);
-    for (int i = 0; i < nloc; i++) {
-        const int x = w.w + i, xm = (x == 0) ? P.nx - 1 : x - 1;
-        if (!counts(P, x) || frozen(P, x, y, z)) continue;
-        double g[kGaussSlots];
+    const int x = w.w + i, xm = (x == 0) ? P.nx - 1 : x - 1;
+    if (i < min(lx, P.nx - w.w) && counts(P, x) && !frozen(P, x, y, z)) {
         gauss_site<float, MODEL>(P, ep.lv[m][tn], ep.lv[m][1 - tn], (x * P.ny + y) * P.nz + z,
                                  (xm * P.ny + y) * P.nz + z, (x * P.ny + ym) * P.nz + z, (x * P.ny + y) * P.nz + zm,
-                                 g);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            v[k] += g[k];
-            v[4 + k] = fmax(v[4 + k], g[4 + k]);
-        }
+                                 v);
     }
-    block_reduce_store<kGaussSlots>(v, partials + (size_t)it * kGaussSlots, 4);
+    block_reduce_store<kGaussSlots>(v, partials + ((size_t)it * gridDim.y + i) * kGaussSlots, 4);
 }
 
-// One block per member: reduce its tiles' partial rows [first[m], first[m+1])
-// into slots [off, off + nslots) of its observables row.
+// One block per member: reduce its tiles' partial rows [first[m] * rpt,
+// first[m+1] * rpt) (rpt rows per tile) into slots [off, off + nslots) of its
+// observables row.
 __global__ void __launch_bounds__(kFinThreads) ensemble_finalize_kernel(const double* __restrict__ partials,
-                                                                        const int* __restrict__ first, int nslots,
-                                                                        int max_from, const double* scales, int off,
-                                                                        double* rows)
+                                                                        const int* __restrict__ first, int rpt,
+                                                                        int nslots, int max_from,
+                                                                        const double* scales, int off, double* rows)
 {
     const int m = blockIdx.x;
-    const double t = reduce_rows_block(partials, first[m], first[m + 1], nslots, max_from);
+    const double t = reduce_rows_block(partials, first[m] * rpt, first[m + 1] * rpt, nslots, max_from);
     if (threadIdx.x < (unsigned)nslots) {
         const size_t o = (size_t)m * kRowSlotCount + off + threadIdx.x;
         rows[o] = t * scales[o];
@@ -313,7 +310,7 @@ cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, i
                            cudaStream_t s)
 {
     if (nitems < 1) return cudaSuccess;
-    ensemble_gauss_kernel<MODEL, TY, TZ><<<nitems, dim3(TZ, TY, 1), 0, s>>>(ep, items, lx, tn, partials);
+    ensemble_gauss_kernel<MODEL, TY, TZ><<<dim3(nitems, lx, 1), dim3(TZ, TY, 1), 0, s>>>(ep, items, lx, tn, partials);
     return cudaGetLastError();
 }
 
@@ -381,7 +378,8 @@ struct gft_batch {
     int* d_first = nullptr;       // first item of each member (+ end)
     double* d_part_e = nullptr;
     double* d_part_g = nullptr;
-    int part_cap = 0;
+    int part_cap = 0;           // tiles the energy partials hold
+    long long part_cap_g = 0;   // rows the Gauss partials hold (tiles x planes per chunk)
     double* d_scale = nullptr;  // [n][kRowSlotCount]
     double* d_rows = nullptr;   // [rows_cap][n][kRowSlotCount]
     int rows_cap = 0;
@@ -546,13 +544,15 @@ int configure(gft_batch* b, int variant, int lx)
     if (e == cudaSuccess) e = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(EnsMaps), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && (int)items.size() > b->part_cap) {
+    // energy partials: a row per tile; Gauss partials: a row per tile and plane of its chunk
+    if (e == cudaSuccess && ((int)items.size() > b->part_cap || (long long)items.size() * lx > b->part_cap_g)) {
         cudaFree(b->d_part_e);
         cudaFree(b->d_part_g);
         b->d_part_e = b->d_part_g = nullptr;
         e = cudaMalloc(&b->d_part_e, items.size() * kObsCount * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&b->d_part_g, items.size() * kGaussSlots * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_part_g, items.size() * (size_t)lx * kGaussSlots * sizeof(double));
         b->part_cap = (e == cudaSuccess) ? (int)items.size() : 0;
+        b->part_cap_g = (e == cudaSuccess) ? (long long)items.size() * lx : 0;
     }
     if (e != cudaSuccess) return b->cuda_fail(e, "gft_batch: configure");
     b->nitems = (int)items.size();
@@ -609,7 +609,7 @@ cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long 
         (*nlaunch)++;
     }
     if (err == cudaSuccess && e) {
-        ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_e, b->d_first, kObsCount, kObsCount,
+        ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_e, b->d_first, 1, kObsCount, kObsCount,
                                                                       b->d_scale, 0, rows);
         err = cudaGetLastError();
         (*nlaunch)++;
@@ -620,13 +620,13 @@ cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long 
             const int i0 = b->group_item[gr], ni = b->group_item[gr + 1] - i0;
             err = (b->model == GFT_MODEL_SM)
                       ? launch_gauss_m<kModelSM>(b->variant, ep, b->d_items + i0, ni, b->lx, tn,
-                                                 b->d_part_g + (size_t)i0 * kGaussSlots, b->stream)
+                                                 b->d_part_g + (size_t)i0 * b->lx * kGaussSlots, b->stream)
                       : launch_gauss_m<kModel2HDM>(b->variant, ep, b->d_items + i0, ni, b->lx, tn,
-                                                   b->d_part_g + (size_t)i0 * kGaussSlots, b->stream);
+                                                   b->d_part_g + (size_t)i0 * b->lx * kGaussSlots, b->stream);
             (*nlaunch)++;
         }
         if (err == cudaSuccess) {
-            ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_g, b->d_first, kGaussSlots, 4,
+            ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_g, b->d_first, b->lx, kGaussSlots, 4,
                                                                           b->d_scale, kObsCount, rows);
             err = cudaGetLastError();
             (*nlaunch)++;
