@@ -81,6 +81,9 @@ def parse():
                     help="N = 1: run the x-slab path (ghost planes refreshed by the exchange callback) on one GPU")
     ap.add_argument("--ensemble-steps", type=int, default=500,
                     help="steps of the 64-member ensemble run (0: skip)")
+    ap.add_argument("--ensemble-tile", type=int, default=-1,
+                    help="ensemble: tile shape index (0: 8x32, 1: 4x32, 2: 4x16, 3: 16x16); -1: the autotuner's choice")
+    ap.add_argument("--ensemble-march", type=int, default=64, help="ensemble: planes per tile along x with --ensemble-tile")
     return ap.parse_args()
 
 
@@ -368,10 +371,11 @@ def precision_table(p, ic, steps: int, device: int) -> dict:
 # ---------------------------------------------------------------------------
 # Ensemble: 64 SM realisations of uneven sizes in one persistent launch per step
 # ---------------------------------------------------------------------------
-def ensemble_report(steps: int, device: int) -> dict:
+def ensemble_report(steps: int, device: int, tile: int = -1, march: int = 64) -> dict:
     """64 SM members, edges drawn uniformly from {32, 48, 64, 96} (seeded), distinct
     seeds, mixed form, analysers every LOG_EVERY steps; tile and march depth from
-    the autotuner; whole logging periods replayed from a CUDA graph."""
+    the autotuner (or `tile` >= 0 and `march`); whole logging periods replayed
+    from a CUDA graph."""
     import random
 
     import numpy as np
@@ -386,7 +390,10 @@ def ensemble_report(steps: int, device: int) -> dict:
            for k in range(64)]
     with Ensemble(ps, device=device) as ens:
         ens.init_fields(ics)
-        tile, march = ens.autotune(4)
+        if tile < 0:
+            tile, march = ens.autotune(4)
+        else:
+            ens.set_kernel(tile, march)
         ens.evolve(2 * LOG_EVERY)  # warm-up (builds the graph)
         l0 = ens.launch_count
         rows = ens.evolve(steps)
@@ -626,7 +633,7 @@ def main():
         ptable = precision_table(p, ic, args.precision_table, local)
     ensemble = None
     if args.ensemble_steps > 0 and world == 1:
-        ensemble = ensemble_report(args.ensemble_steps, local)
+        ensemble = ensemble_report(args.ensemble_steps, local, args.ensemble_tile, args.ensemble_march)
     configs = None
     if not args.no_configs and world == 1 and args.size == 256 and args.model == "sm":
         configs = configs_report(local)
