@@ -396,7 +396,10 @@ def ensemble_report(steps: int, device: int, tile: int = -1, march: int = 64) ->
             ens.set_kernel(tile, march)
         ens.evolve(2 * LOG_EVERY)  # warm-up (builds the graph)
         l0 = ens.launch_count
+        sampler = ClockSampler(device)
+        sampler.start()
         rows = ens.evolve(steps)
+        clocks = sampler.stop()
         ms = ens.last_ms
         launches = ens.launch_count - l0
         nsite = ens.nsite
@@ -412,6 +415,9 @@ def ensemble_report(steps: int, device: int, tile: int = -1, march: int = 64) ->
         "roofline_frac": B_ALG[("sm", 4)] * nsite * steps / (ms / 1e3) / 1e9 / measured_peaks()[0],
         "tile": ["8x32", "4x32", "4x16", "16x16"][tile], "march": march, "graphs": True,
         "kernel_launches_per_step": launches / steps, "nonfinite_rows": len(bad),
+        # SM clocks of this leg (it follows the other legs' seconds of load; a power cap lowers them)
+        "clocks": clocks,
+        "ms_x_sm_mhz": (ms / steps * clocks["sm_mhz"]) if clocks.get("sm_mhz") else None,
     }
 
 
