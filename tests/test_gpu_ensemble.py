@@ -76,6 +76,28 @@ def test_members_evolve_like_single_handles(oracle_mod, model, shapes):
         _compare_rows(rows[m], r1, p.nsite)
 
 
+def test_two_launch_groups_and_uneven_chunks_evolve_like_single_handles(oracle_mod):
+    """70 members: two launch groups (64 members' parameters per launch), each with its own
+    per-CTA tile lists; x-lengths 8, 12 and 20 at march 8 give chunks of 8 and 4 planes, so
+    the lists deal tiles of unequal cost.  Members on both sides of the group boundary evolve
+    as single handles do."""
+    from gftevolver_b200 import Ensemble, InitialData
+    shapes = [((8, 12, 20)[k % 3], 8, 16) for k in range(70)]
+    ps, ics = _members(oracle_mod, 1, shapes, every=(3, 3))
+    nt = 5
+    with Ensemble(ps) as ens:
+        ens.set_kernel(2, 8)
+        ens.init_fields([InitialData(**ic) for ic in ics])
+        rows = ens.evolve(nt)
+        out = {m: ens.download(m) for m in (0, 1, 62, 63, 64, 65, 69)}
+    assert all(np.isfinite(r["energy"]) for mr in rows for r in mr if r["has_energy"])
+    for m, (sc_e, ve_e) in out.items():
+        sc, ve, r1 = _single(ps[m], ics[m], nt, 2, 8)
+        assert np.max(np.abs(sc_e - sc)) <= 2e-6, m
+        assert np.max(np.abs(ve_e - ve)) <= 2e-6, m
+        _compare_rows(rows[m], r1, ps[m].nsite)
+
+
 def test_graph_replay_equals_direct_launches(oracle_mod):
     from gftevolver_b200 import Ensemble, InitialData
     ps, ics = _members(oracle_mod, 1, [(16, 8, 16), (32, 16, 32), (8, 4, 16)], every=(2, 2))
