@@ -52,6 +52,7 @@ struct gft_handle {
     LinkCodec codec;        // generator representation: how host links map to device records
     int neq = 4;            // gauge equations per direction = Gauss constraints (gaugeNum)
     int nsite = 0;
+    int nsm = 148;          // the device's SMs (the automatic kernel choice counts waves of tiles)
     int sbytes = 4;         // storage bytes per word (4 or 8)
     void* level_mem[2] = {nullptr, nullptr};
     LevelPtrs<float> lf[2]{};
@@ -295,14 +296,27 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
 // tiled kernel for SM (46 % of HBM against 42 % for one thread per site);
 // one thread per site for 2HDM, whose four staged plane buffers (two doublets)
 // need 130 KB of shared memory and leave one CTA per SM (30 % against 45 %).
+// The automatic choice (kernel kind 0) takes the staged step for the SM model
+// when its tiles fill enough waves of resident CTAs: fewer tiles leave SMs idle
+// while each CTA marches its planes, and one thread per site is faster there
+// (mixed form at 32^3: 14x, 64^3: 3.6x, 128^3 (256 tiles, under one wave): even;
+// 192^3 (2.9 waves): the staged step 15 % faster.  FP64, one CTA per SM: one
+// thread per site faster up to 128^3, even at 192^3 (5.8 waves), the staged
+// step 5.5 % faster at 256^3 (13.8 waves)).
+constexpr int kAutoWavesMixed = 2, kAutoWavesFP64 = 8;
+
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
     if (!h->tiled_ready || h->kernel_kind == 1 || h->hf != kHfNone) return false;
-    // the FP64 form: the staged SM step, on request (gft_set_kernel kind 2)
-    const bool fp64_tiled = h->cfg.form == GFT_FORM_FP64 && h->cfg.model == GFT_MODEL_SM && h->kernel_kind == 2;
-    if (h->cfg.form != GFT_FORM_MIXED && !fp64_tiled) return false;
-    if (h->kernel_kind == 0 && h->cfg.model != GFT_MODEL_SM) return false;
-    return tiled_supported(P, h->tile_variant);
+    const bool fp64 = h->cfg.form == GFT_FORM_FP64;
+    // the FP64 form: the staged SM step only (kinds 0 and 2)
+    if (fp64 && (h->cfg.model != GFT_MODEL_SM || h->kernel_kind > 2)) return false;
+    if (h->cfg.form != GFT_FORM_MIXED && !fp64) return false;
+    if (!tiled_supported(P, h->tile_variant)) return false;
+    if (h->kernel_kind != 0) return true;
+    if (h->cfg.model != GFT_MODEL_SM) return false;
+    const long long slots = (long long)h->nsm * tiled_ctas_per_sm(h->tile_variant, fp64);
+    return tiled_blocks(P, h->tile_variant, h->march) >= (fp64 ? kAutoWavesFP64 : kAutoWavesMixed) * slots;
 }
 
 // Plain steps of the SM mixed form with two sites per thread (kernel kind 3):
@@ -482,6 +496,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
     h->nsite = cfg->nx * cfg->ny * cfg->nz;
     h->sbytes = (cfg->form == GFT_FORM_REF) ? cfg->storage_bytes : (cfg->form == GFT_FORM_FP64 ? 8 : 4);
     cudaError_t e = cudaSetDevice(cfg->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
     if (e != cudaSuccess) {
         int r = h->cuda_fail(e, "cudaSetDevice");
         delete h;
@@ -508,7 +523,7 @@ int gft_create(const gft_config* cfg, gft_handle** out)
             carve<double>(h->level_mem[t], h->nsite, h->nsc, h->ld[t], h->hf);
     }
     const StepParams P = make_params(h, 0, false);
-    if (cfg->form == GFT_FORM_MIXED) {
+    if (cfg->form == GFT_FORM_MIXED || (cfg->form == GFT_FORM_FP64 && cfg->model == GFT_MODEL_SM)) {
         // default tile: the largest built shape the lattice divides
         h->tile_variant = 0;
         while (h->tile_variant < kTiledVariants && !tiled_supported(P, h->tile_variant)) h->tile_variant++;

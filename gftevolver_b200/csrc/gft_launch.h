@@ -44,6 +44,8 @@ template <class S>
 bool tiled_encode_maps(const StepParams& P, const LevelPtrs<S>& L, int nd, int ty, int tz, bool halo, TMaps* out);
 bool tiled_supported(const StepParams& P, int variant);
 int tiled_blocks(const StepParams& P, int variant, int lx);
+// Resident CTAs per SM the SM-model tiled step asks for (its launch bounds).
+int tiled_ctas_per_sm(int variant, bool fp64);
 template <class S, int MODEL>
 cudaError_t launch_tiled_step(const TMaps& maps, const TMaps& pmaps, const StepParams& P, const LevelPtrs<S>& now,
                               const LevelPtrs<S>& past, int variant, int lx, unsigned* status, double* partials,

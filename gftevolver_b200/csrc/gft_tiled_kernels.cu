@@ -300,6 +300,16 @@ bool tiled_supported(const StepParams& P, int variant)
     return encode_fn() != nullptr && P.nz % tz == 0 && P.ny % ty == 0 && P.nx >= 1;
 }
 
+int tiled_ctas_per_sm(int variant, bool fp64)
+{
+    switch (variant) {
+    case 0: return fp64 ? tiled_min_blocks<double, kModelSM, 8, 32>() : tiled_min_blocks<float, kModelSM, 8, 32>();
+    case 1: return fp64 ? tiled_min_blocks<double, kModelSM, 4, 32>() : tiled_min_blocks<float, kModelSM, 4, 32>();
+    case 2: return fp64 ? tiled_min_blocks<double, kModelSM, 4, 16>() : tiled_min_blocks<float, kModelSM, 4, 16>();
+    default: return fp64 ? tiled_min_blocks<double, kModelSM, 16, 16>() : tiled_min_blocks<float, kModelSM, 16, 16>();
+    }
+}
+
 int tiled_blocks(const StepParams& P, int variant, int lx)
 {
     int ty, tz;

@@ -247,12 +247,13 @@ def test_thousand_step_precision_at_256():
 # ---------------------------------------------------------------------------
 # small lattices: whole logging periods replayed from a CUDA graph
 # ---------------------------------------------------------------------------
-@pytest.mark.parametrize("form,shape,every,steps", [
-    ("fp64", (32, 32, 32), (10, 10), 47),    # configuration 1; a tail shorter than a period
-    ("mixed", (8, 8, 32), (3, 2), 20),       # tiled kernel, period lcm(2, 3, 2) = 6
-    ("ref32", (6, 5, 4), (2, 3), 13),        # reference arithmetic, odd shape
+@pytest.mark.parametrize("form,shape,every,steps,kind", [
+    ("fp64", (32, 32, 32), (10, 10), 47, 0),    # configuration 1; a tail shorter than a period
+    ("mixed", (8, 8, 32), (3, 2), 20, 2),       # tiled kernel, period lcm(2, 3, 2) = 6
+    ("mixed", (8, 8, 32), (3, 2), 20, 0),       # the automatic choice: one thread per site here
+    ("ref32", (6, 5, 4), (2, 3), 13, 0),        # reference arithmetic, odd shape
 ])
-def test_graph_replay_equals_direct_launches(form, shape, every, steps):
+def test_graph_replay_equals_direct_launches(form, shape, every, steps, kind):
     from gftevolver_b200 import Evolver, InitialData, LatticeParams
     nx, ny, nz = shape
     p = LatticeParams(nx=nx, ny=ny, nz=nz, energy_every=every[0], gauss_every=every[1])
@@ -261,6 +262,8 @@ def test_graph_replay_equals_direct_launches(form, shape, every, steps):
     for graphs in (True, False):
         with Evolver(p, form=form) as ev:
             ev.set_graphs(graphs)
+            if kind:
+                ev.set_kernel(kind, 0, 32)
             ev.init_fields(ic)
             l0 = ev.launch_count
             rows = ev.evolve(5)          # starts off a period boundary, then whole periods and a tail
@@ -290,6 +293,7 @@ def test_graph_replay_across_damping_and_a_kernel_switch():
     for graphs in (True, False):
         with Evolver(p, form="mixed") as ev:
             ev.set_graphs(graphs)
+            ev.set_kernel(2, 0, 32)         # the staged step first
             ev.init_fields(ic)
             rows = ev.evolve(13)           # damped 0..6, then whole periods of 4
             ev.set_kernel(1, 0, 32)         # one thread per site from here on

@@ -237,6 +237,8 @@ def test_generator_representation_forms_vs_oracle(oracle_mod, model, hf, shape):
     sc32, ve32 = oracle_mod.init_fields(op, ic, np.float32)
     from gftevolver_b200 import Evolver
     with Evolver(p, form="mixed") as ev:
+        if model == 1 and shape == (8, 8, 32):
+            ev.set_kernel(2, 0, 32)  # the staged step (too few tiles for the automatic choice)
         ev.upload(sc32, ve32, 0)
         rows = ev.evolve(10)
         sc, ve = ev.download()
@@ -399,13 +401,24 @@ def test_device_buffer_transfers_match_host_transfers(oracle_mod, form):
 
 
 def test_step_kernel_name_follows_form_and_shape(oracle_mod):
+    """The automatic choice takes the staged step for the SM model when its tiles fill
+    2 waves of resident CTAs (mixed form) or 8 (FP64), else one thread per site."""
     from gftevolver_b200 import Evolver
-    op = oracle_mod.Params(nx=8, ny=8, nz=32)
+    op = oracle_mod.Params(nx=8, ny=8, nz=32)  # one tile
     with Evolver(_lp(op.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
+        ev.set_kernel(2, 0, 32)
         assert ev.step_kernel_name == "tiled_step_kernel"
         ev.set_kernel(1, 0, 32)
         assert ev.step_kernel_name == "fast_step_kernel"
     with Evolver(_lp(op.__dict__), form="fp64") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
+        ev.set_kernel(2, 0, 32)
+        assert ev.step_kernel_name == "tiled_step_kernel"
+    big = oracle_mod.Params(nx=96, ny=256, nz=256)  # 8 x 32 tiles, march 32: 768 tiles = 2.6 waves of 296
+    with Evolver(_lp(big.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "tiled_step_kernel"
+    with Evolver(_lp(big.__dict__), form="fp64") as ev:  # FP64: 5.2 waves of 148, under 8
         assert ev.step_kernel_name == "fast_step_kernel"
     with Evolver(_lp(op.__dict__), form="ref32") as ev:
         assert ev.step_kernel_name == "ref_step_kernel"
