@@ -1021,8 +1021,11 @@ void gft::fill_observables(gft_observables* r, int time_iter, bool e, bool g, co
 {
     fill_row(r, time_iter, e, g, v, neq);
 }
-size_t gft::level_bytes_f32(int nsite, int nsc) { return level_words(nsite, nsc) * sizeof(float); }
-void gft::carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L) { carve<float>(mem, nsite, nsc, L); }
+size_t gft::level_bytes_f32(int nsite, int nsc, int hf) { return level_words(nsite, nsc, hf) * sizeof(float); }
+void gft::carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L, int hf)
+{
+    carve<float>(mem, nsite, nsc, L, hf);
+}
 void gft::set_error(const std::string& msg) { set_global_error(msg); }
 
 extern "C" {

@@ -358,6 +358,13 @@ struct gft_batch {
     int model = GFT_MODEL_SM;
     int device = 0;
     int nsc = 4;
+    int hf = kHfNone;  // 2HDM Higgs-family field shared by every member (then one launch per member and step)
+    int nve = 15;      // link words per site in the reference layout (15, 18 or 27)
+    int neq = 4;       // Gauss constraints per row (gaugeNum)
+    // family ensembles: per-member partial rows (reused member after member on the stream) and
+    // the two-stage reduction scratch
+    double* d_part_f = nullptr;
+    double* d_mid = nullptr;
     int nsm = 148;
     std::vector<gft_config> cfg;
     std::vector<int> nsite;
@@ -590,9 +597,43 @@ int configure(gft_batch* b, int variant, int lx)
     return GFT_OK;
 }
 
+// A Higgs-family ensemble: no tiled or persistent step carries the family
+// fields, so each member takes the launches a single handle makes -- the
+// one-thread-per-site step, its energy row, the Gauss pass and its row --
+// member after member on the ensemble's stream (one partial buffer serves them
+// in turn).
+cudaError_t issue_step_family(gft_batch* b, int ti, bool e, bool g, double* rows, long long* nlaunch)
+{
+    const int tn = (ti + 1) % 2, tp = 1 - tn;
+    cudaError_t err = cudaSuccess;
+    for (int m = 0; m < b->n && err == cudaSuccess; m++) {
+        const StepParams P = config_params(b->cfg[m], b->nsite[m], false, ti, e);
+        const double* scale = b->d_scale + (size_t)m * kRowSlotCount;
+        double* row = rows + (size_t)m * kRowSlotCount;
+        err = launch_fast_step<float, kModel2HDM>(P, b->lv[m][tn], b->lv[m][tp], b->d_status, b->d_part_f, e, 0,
+                                                  b->stream);
+        (*nlaunch)++;
+        if (err == cudaSuccess && e) {
+            const int nb = fast_launch_blocks(P, 0);
+            err = launch_finalize(b->d_part_f, nb, kObsCount, kObsCount, scale, row, b->d_mid, b->stream);
+            *nlaunch += finalize_launches(nb, true);
+        }
+        if (err == cudaSuccess && g) {
+            const int nb = fast_gauss_blocks(P);
+            err = launch_fast_gauss<float, kModel2HDM>(P, b->lv[m][tn], b->lv[m][tp], b->d_part_f, b->stream);
+            if (err == cudaSuccess)
+                err = launch_finalize(b->d_part_f, nb, 2 * b->neq, b->neq, scale + kObsCount, row + kObsCount,
+                                      b->d_mid, b->stream);
+            *nlaunch += 1 + finalize_launches(nb, true);
+        }
+    }
+    return err;
+}
+
 // Launches of one step (time_iter ti); rows go to `rows` when a row is logged.
 cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long long* nlaunch)
 {
+    if (b->hf != kHfNone) return issue_step_family(b, ti, e, g, rows, nlaunch);
     const int tn = (ti + 1) % 2;
     static thread_local EnsParams ep;
     cudaError_t err = cudaSuccess;
@@ -749,9 +790,9 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
             set_error("gft_batch_create: the ensemble evolves the mixed form only");
             return GFT_E_UNSUPPORTED;
         }
-        if (cfgs[m].higgs_family != GFT_HF_NONE) {
-            set_error("gft_batch_create: the ensemble has no Higgs-family gauge field (gaugeNum 4 only)");
-            return GFT_E_UNSUPPORTED;
+        if (cfgs[m].higgs_family != cfgs[0].higgs_family) {
+            set_error("gft_batch_create: all members must share the Higgs-family field (gaugeNum)");
+            return GFT_E_INVALID;
         }
         if (cfgs[m].generator_rep) {
             set_error("gft_batch_create: the ensemble transfers quaternion links only (generator_rep = 0)");
@@ -771,10 +812,13 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
     b->model = cfgs[0].model;
     b->device = cfgs[0].device;
     b->nsc = (b->model == GFT_MODEL_SM) ? 4 : 8;
+    b->hf = (b->model == GFT_MODEL_2HDM) ? cfgs[0].higgs_family : kHfNone;
+    b->nve = 3 * (5 + (b->hf == kHfSU2 ? 4 : (b->hf == kHfU1 ? 1 : 0)));
+    b->neq = config_neq(cfgs[0]);
     b->cfg.assign(cfgs, cfgs + n);
     for (int v = 0; v < kTiledVariants && b->variant < 0; v++)
         if (variant_fits(b, v)) b->variant = v;
-    if (b->variant < 0) {
+    if (b->variant < 0 && b->hf == kHfNone) {
         delete b;
         set_error("gft_batch_create: the members' (ny, nz) share no built tile shape (4 x 16, the smallest, needs ny % 4 == 0 and nz % 16 == 0)");
         return GFT_E_UNSUPPORTED;
@@ -793,7 +837,7 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
     for (int m = 0; m < n; m++) {
         b->nsite.push_back(cfgs[m].nx * cfgs[m].ny * cfgs[m].nz);
         b->level_off.push_back(off);
-        off += 2 * ((level_bytes_f32(b->nsite[m], b->nsc) + 255) / 256 * 256);
+        off += 2 * ((level_bytes_f32(b->nsite[m], b->nsc, b->hf) + 255) / 256 * 256);
     }
     b->arena_bytes = off;
     e = cudaMalloc(&b->arena, b->arena_bytes);
@@ -809,13 +853,30 @@ int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out)
     b->lv.resize(n);
     std::vector<double> scale((size_t)n * kRowSlotCount);
     for (int m = 0; m < n; m++) {
-        const size_t lb = (level_bytes_f32(b->nsite[m], b->nsc) + 255) / 256 * 256;
+        const size_t lb = (level_bytes_f32(b->nsite[m], b->nsc, b->hf) + 255) / 256 * 256;
         for (int t = 0; t < 2; t++)
             carve_level_f32(static_cast<unsigned char*>(b->arena) + b->level_off[m] + t * lb, b->nsite[m], b->nsc,
-                            b->lv[m][t]);
+                            b->lv[m][t], b->hf);
         row_scales(b->cfg[m], b->nsite[m], scale.data() + (size_t)m * kRowSlotCount);
     }
     cudaMemcpy(b->d_scale, scale.data(), scale.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (b->hf != kHfNone) {
+        // one thread per site, member after member: partial rows for the largest member
+        int rows = 0;
+        for (int m = 0; m < n; m++) {
+            const StepParams P = config_params(b->cfg[m], b->nsite[m], false, 0, false);
+            rows = std::max(rows, std::max(fast_launch_blocks(P, 0), fast_gauss_blocks(P)));
+        }
+        e = cudaMalloc(&b->d_part_f, (size_t)rows * kMaxSlots * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_mid, (size_t)kFinMidCapacity * sizeof(double));
+        if (e != cudaSuccess) {
+            b->fail(GFT_E_NOMEM, std::string("gft_batch_create: ") + cudaGetErrorString(e));
+            gft_batch_destroy(b);
+            return GFT_E_NOMEM;
+        }
+        *out = b;
+        return GFT_OK;
+    }
     int rc = configure(b, b->variant, 32);
     if (rc != GFT_OK) {
         gft_batch_destroy(b);
@@ -844,6 +905,8 @@ void gft_batch_destroy(gft_batch* b)
     cudaFree(b->d_status);
     cudaFree(b->d_stage);
     cudaFree(b->d_graph_rows);
+    cudaFree(b->d_part_f);
+    cudaFree(b->d_mid);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -882,7 +945,7 @@ int gft_batch_upload_f32(gft_batch* b, int member, const float* sc, const float*
 {
     if (!b || !sc || !ve || member < 0 || member >= b->n || time_iter < 0) return GFT_E_INVALID;
     cudaSetDevice(b->device);
-    const size_t nsc_w = 2 * (size_t)b->nsite[member] * b->nsc, nve_w = 2 * (size_t)b->nsite[member] * 15;
+    const size_t nsc_w = 2 * (size_t)b->nsite[member] * b->nsc, nve_w = 2 * (size_t)b->nsite[member] * b->nve;
     int rc = ensure_stage(b, (nsc_w + nve_w) * sizeof(float));
     if (rc != GFT_OK) return rc;
     float* dsc = static_cast<float*>(b->d_stage);
@@ -891,7 +954,7 @@ int gft_batch_upload_f32(gft_batch* b, int member, const float* sc, const float*
     if (e == cudaSuccess) e = cudaMemcpyAsync(dve, ve, nve_w * sizeof(float), cudaMemcpyHostToDevice, b->stream);
     for (int t = 0; t < 2 && e == cudaSuccess; t++)
         e = launch_aos_to_soa<float, float>(dsc + (size_t)t * b->nsite[member] * b->nsc,
-                                            dve + (size_t)t * b->nsite[member] * 15, b->nsite[member], b->nsc,
+                                            dve + (size_t)t * b->nsite[member] * b->nve, b->nsite[member], b->nsc,
                                             b->lv[member][t], b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return b->cuda_fail(e, "gft_batch_upload_f32");
@@ -905,7 +968,7 @@ int gft_batch_download_f32(gft_batch* b, int member, float* sc, float* ve)
     if (!b || !sc || !ve || member < 0 || member >= b->n) return GFT_E_INVALID;
     if (!b->has_data) return b->fail(GFT_E_STATE, "gft_batch_download_f32: no field data");
     cudaSetDevice(b->device);
-    const size_t nsc_w = 2 * (size_t)b->nsite[member] * b->nsc, nve_w = 2 * (size_t)b->nsite[member] * 15;
+    const size_t nsc_w = 2 * (size_t)b->nsite[member] * b->nsc, nve_w = 2 * (size_t)b->nsite[member] * b->nve;
     int rc = ensure_stage(b, (nsc_w + nve_w) * sizeof(float));
     if (rc != GFT_OK) return rc;
     float* dsc = static_cast<float*>(b->d_stage);
@@ -914,7 +977,7 @@ int gft_batch_download_f32(gft_batch* b, int member, float* sc, float* ve)
     for (int t = 0; t < 2 && e == cudaSuccess; t++)
         e = launch_soa_to_aos<float, float>(b->lv[member][t], b->nsite[member], b->nsc,
                                             dsc + (size_t)t * b->nsite[member] * b->nsc,
-                                            dve + (size_t)t * b->nsite[member] * 15, b->stream);
+                                            dve + (size_t)t * b->nsite[member] * b->nve, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(sc, dsc, nsc_w * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ve, dve, nve_w * sizeof(float), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -994,7 +1057,7 @@ int gft_batch_evolve(gft_batch* b, int n_steps, gft_observables* rows, int max_r
     for (int m = 0; m < b->n && rows; m++)
         for (int r = 0; r < nw; r++)
             fill_observables(&rows[(size_t)m * max_rows + r], meta[r].ti, meta[r].e, meta[r].g,
-                             host.data() + ((size_t)r * b->n + m) * kRowSlotCount);
+                             host.data() + ((size_t)r * b->n + m) * kRowSlotCount, b->neq);
     if (n_rows) *n_rows = nw;
     return (int)(status & (GFT_W_ASIN_DOMAIN | GFT_W_SQRT_DOMAIN | GFT_W_NONFINITE | GFT_W_RANGE));
 }
@@ -1002,6 +1065,11 @@ int gft_batch_evolve(gft_batch* b, int n_steps, gft_observables* rows, int max_r
 int gft_batch_set_kernel(gft_batch* b, int tile, int march, int use_graphs)
 {
     if (!b) return GFT_E_INVALID;
+    if (b->hf != kHfNone) {  // one thread per site: no tile shape or march; only the graph switch applies
+        b->use_graphs = use_graphs != 0;
+        if (!b->use_graphs) drop_graph(b);
+        return GFT_OK;
+    }
     if (tile < 0 || tile >= kTiledVariants || march < 1) return b->fail(GFT_E_INVALID, "gft_batch_set_kernel: bad tile or march");
     if (!variant_fits(b, tile)) return b->fail(GFT_E_UNSUPPORTED, "gft_batch_set_kernel: a member does not divide into this tile");
     cudaSetDevice(b->device);
@@ -1016,6 +1084,8 @@ int gft_batch_set_kernel(gft_batch* b, int tile, int march, int use_graphs)
 int gft_batch_autotune(gft_batch* b, int trial_steps, int* tile, int* march)
 {
     if (!b) return GFT_E_INVALID;
+    if (b->hf != kHfNone)
+        return b->fail(GFT_E_UNSUPPORTED, "gft_batch_autotune: a Higgs-family ensemble runs one thread per site (no tiles)");
     if (!b->has_data) return b->fail(GFT_E_STATE, "gft_batch_autotune: no field data");
     if (trial_steps < 1) trial_steps = 4;
     cudaSetDevice(b->device);

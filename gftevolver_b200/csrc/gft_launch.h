@@ -152,9 +152,9 @@ void row_scales(const gft_config& c, int nsite, double* scale);
 int validate_config(const gft_config* c, std::string& why);
 // neq = gaugeNum (Gauss constraints per row).
 void fill_observables(gft_observables* r, int time_iter, bool e, bool g, const double* v, int neq = 4);
-// One time level of float storage (no Higgs-family arrays): bytes, and the array pointers within it.
-size_t level_bytes_f32(int nsite, int nsc);
-void carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L);
+// One time level of float storage (with the Higgs-family arrays of hf): bytes, and the array pointers within it.
+size_t level_bytes_f32(int nsite, int nsc, int hf = kHfNone);
+void carve_level_f32(void* mem, int nsite, int nsc, LevelPtrs<float>& L, int hf = kHfNone);
 constexpr int kRowSlotCount = kObsCount + kGaussSlotsMax;
 // Gauge equations per direction (gaugeNum) of a configuration.
 inline int config_neq(const gft_config& c) { return c.model == GFT_MODEL_2HDM ? hf_neq(c.higgs_family) : 4; }

@@ -73,7 +73,7 @@ class Ensemble:
 
     def _shapes(self, m: int):
         p = self.params[m]
-        return (2, p.nx, p.ny, p.nz, p.nsc), (2, p.nx, p.ny, p.nz, 15)
+        return (2, p.nx, p.ny, p.nz, p.nsc), (2, p.nx, p.ny, p.nz, p.nve)
 
     def upload(self, m: int, scalars: np.ndarray, vectors: np.ndarray, time_iter: int = 0) -> None:
         ss, vs = self._shapes(m)
@@ -101,7 +101,8 @@ class Ensemble:
         n = ctypes.c_int(0)
         self.last_warnings = _lib.check_batch(
             self.lib.gft_batch_evolve(self.b, int(n_steps), rows, max_rows, ctypes.byref(n)), self.b)
-        return [[_row_dict(rows[m * max_rows + r]) for r in range(n.value)] for m in range(len(self))]
+        neq = self.params[0].neq  # Gauss constraints per row: gaugeNum, shared by the members
+        return [[_row_dict(rows[m * max_rows + r], neq) for r in range(n.value)] for m in range(len(self))]
 
     def set_kernel(self, tile: int, march: int, use_graphs: bool = True) -> None:
         _lib.check_batch(self.lib.gft_batch_set_kernel(self.b, int(tile), int(march), int(bool(use_graphs))), self.b)

@@ -317,11 +317,14 @@ int gft_selftest_math(int device, double* out);
  * one object, evolved together by ONE persistent kernel launch per time step
  * (no reference counterpart: the reference runs one lattice per process,
  * Core/Source/Lattice.cpp:755-876).  All members share the model, the device,
- * the analysers' cadence and the step counter; the form is GFT_FORM_MIXED, with
- * no Higgs-family field; the
- * members' (ny, nz) must share a tile shape (ny % 4 == 0 and nz % 16 == 0 at
- * least).  Each member evolves exactly as a single handle would with the same
- * tile shape and march depth (gft_set_kernel). */
+ * the analysers' cadence, the Higgs-family field and the step counter; the form
+ * is GFT_FORM_MIXED; the members' (ny, nz) must share a tile shape (ny % 4 == 0
+ * and nz % 16 == 0 at least).  Each member evolves exactly as a single handle
+ * would with the same tile shape and march depth (gft_set_kernel).  2HDM members
+ * with a Higgs-family field (gaugeNum 5 or 7) take the single handle's
+ * one-thread-per-site launches instead, member after member (any shape; no tile
+ * shape: gft_batch_set_kernel applies only its use_graphs, gft_batch_autotune
+ * returns GFT_E_UNSUPPORTED), and evolve bit for bit as single handles do. */
 typedef struct gft_batch gft_batch;
 
 int gft_batch_create(const gft_config* cfgs, int n, gft_batch** out);

@@ -110,9 +110,11 @@ def test_batch_create_validates_members_without_gpu(lib):
     cfgs = (_lib.GftConfig * 2)(make_config(a), make_config(d))
     assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
     assert lib.gft_batch_create(cfgs, 0, ctypes.byref(h)) == _lib.GFT_E_INVALID
+    # members with a Higgs-family field must share it (gaugeNum)
     e = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, model=_lib.GFT_MODEL_2HDM, higgs_family=_lib.GFT_HF_SU2)
-    cfgs = (_lib.GftConfig * 1)(make_config(e))
-    assert lib.gft_batch_create(cfgs, 1, ctypes.byref(h)) == _lib.GFT_E_UNSUPPORTED
+    e1 = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, model=_lib.GFT_MODEL_2HDM, higgs_family=_lib.GFT_HF_U1)
+    cfgs = (_lib.GftConfig * 2)(make_config(e), make_config(e1))
+    assert lib.gft_batch_create(cfgs, 2, ctypes.byref(h)) == _lib.GFT_E_INVALID
     assert b"Higgs-family" in lib.gft_last_error(None)
     f = LatticeParams(nx=8, ny=4, nz=16, energy_every=2, generator_rep=1)
     cfgs = (_lib.GftConfig * 1)(make_config(f))

@@ -218,3 +218,45 @@ def test_sharded_ensemble_halves_match_the_whole(oracle_mod):
                 sc, ve = se.local.download(k)
                 assert np.array_equal(sc, w_fields[m][0]) and np.array_equal(ve, w_fields[m][1])
     assert got_rows == w_rows
+
+
+@pytest.mark.parametrize("hf", [1, 2], ids=["family_u1", "family_su2"])
+def test_higgs_family_members_evolve_like_single_handles(oracle_mod, hf):
+    """2HDM members with a Higgs-family field (gaugeNum 5 / 7): the ensemble takes the
+    single handle's one-thread-per-site launches member after member, so every member
+    equals a single handle bit for bit, analyser rows included (gaugeNum Gauss
+    constraints), in lattices of any shape; replaying logging periods from a graph
+    changes nothing; there is no tile shape to tune."""
+    from gftevolver_b200 import Ensemble, Evolver, InitialData, LatticeParams
+    shapes = [(8, 6, 10), (5, 8, 16), (12, 4, 7)]
+    ps, ics = [], []
+    for k, (nx, ny, nz) in enumerate(shapes):
+        op = oracle_mod.Params(model=2, nx=nx, ny=ny, nz=nz, energy_every=2, gauss_every=3, higgs_family=hf,
+                               gpp=0.47)
+        ps.append(LatticeParams(**op.__dict__))
+        ics.append(dict(seed=700 + k, mean=[0.7] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1))
+    nt = 7
+    res = []
+    for graphs in (True, False):
+        with Ensemble(ps) as ens:
+            ens.set_kernel(0, 8, use_graphs=graphs)
+            ens.init_fields([InitialData(**ic) for ic in ics])
+            rows = ens.evolve(nt)
+            res.append((rows, [ens.download(m) for m in range(len(ps))]))
+            if graphs:
+                with pytest.raises(Exception):
+                    ens.autotune(2)
+    (ra, fa), (rb, fb) = res
+    assert ra == rb
+    for (a_sc, a_ve), (b_sc, b_ve) in zip(fa, fb):
+        assert np.array_equal(a_sc, b_sc) and np.array_equal(a_ve, b_ve)
+    neq = 5 if hf == 1 else 7
+    for m, (p, ic) in enumerate(zip(ps, ics)):
+        with Evolver(p, form="mixed") as ev:
+            ev.init_fields(InitialData(**ic))
+            r1 = ev.evolve(nt)
+            sc, ve = ev.download()
+        assert fa[m][1].shape[-1] == (18 if hf == 1 else 27)
+        assert np.array_equal(fa[m][0], sc) and np.array_equal(fa[m][1], ve), m
+        assert ra[m] == r1, m
+        assert all(len(r["gauss_max"]) == neq for r in r1 if r["has_gauss"])
