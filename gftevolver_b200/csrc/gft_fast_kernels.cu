@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(128, 3) fast_step_kernel<double, kModelSM, kHf
 // keeps the most loads in flight (a march along x that carries the x - 1 links
 // in registers serialises them and measured slower).
 template <class S, int MODEL, int HF>
-__global__ void __launch_bounds__(128) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
+__global__ void __launch_bounds__(256) fast_gauss_kernel(StepParams P, LevelPtrs<S> now, LevelPtrs<S> fut,
                                                          double* partials)
 {
     constexpr int NG = 2 * hf_neq(HF);
@@ -147,15 +147,15 @@ template <class S, int MODEL, int HF>
 void fast_gauss_launch(const StepParams& P, const LevelPtrs<S>& now, const LevelPtrs<S>& fut, double* partials,
                        cudaStream_t stream)
 {
-    const dim3 block(32, 4, 1);
-    const dim3 grid((P.nz + 31) / 32, (P.ny + 3) / 4, P.nx);
+    const dim3 block(32, 8, 1);  // 32 x 8: 2 % faster than 32 x 4 at 256^3 (624 against 638 us)
+    const dim3 grid((P.nz + 31) / 32, (P.ny + 7) / 8, P.nx);
     fast_gauss_kernel<S, MODEL, HF><<<grid, block, 0, stream>>>(P, now, fut, partials);
 }
 
 }  // namespace
 
 int fast_launch_blocks(const StepParams& P, int /*variant*/) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
-int fast_gauss_blocks(const StepParams& P) { return ((P.nz + 31) / 32) * ((P.ny + 3) / 4) * P.nx; }
+int fast_gauss_blocks(const StepParams& P) { return ((P.nz + 31) / 32) * ((P.ny + 7) / 8) * P.nx; }
 
 // P.hf selects the Higgs-family variant (2HDM only); the Gauss kernel writes
 // 2 * gaugeNum partial slots per block.
