@@ -306,11 +306,11 @@ int resident_m(int variant)
 }
 
 template <int MODEL, int TY, int TZ>
-cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, int lx, int tn, double* partials,
-                           cudaStream_t s)
+cudaError_t launch_gauss_t(const EnsParams& ep, const int4* items, int nitems, int lx, int rows, int tn,
+                           double* partials, cudaStream_t s)
 {
     if (nitems < 1) return cudaSuccess;
-    ensemble_gauss_kernel<MODEL, TY, TZ><<<dim3(nitems, lx, 1), dim3(TZ, TY, 1), 0, s>>>(ep, items, lx, tn, partials);
+    ensemble_gauss_kernel<MODEL, TY, TZ><<<dim3(nitems, rows, 1), dim3(TZ, TY, 1), 0, s>>>(ep, items, lx, tn, partials);
     return cudaGetLastError();
 }
 
@@ -332,14 +332,14 @@ cudaError_t launch_step_m(int variant, bool energy, bool uniform, const EnsParam
 }
 
 template <int MODEL>
-cudaError_t launch_gauss_m(int variant, const EnsParams& ep, const int4* items, int nitems, int lx, int tn,
+cudaError_t launch_gauss_m(int variant, const EnsParams& ep, const int4* items, int nitems, int lx, int rows, int tn,
                            double* partials, cudaStream_t s)
 {
     switch (variant) {
-    case 0: return launch_gauss_t<MODEL, 8, 32>(ep, items, nitems, lx, tn, partials, s);
-    case 1: return launch_gauss_t<MODEL, 4, 32>(ep, items, nitems, lx, tn, partials, s);
-    case 2: return launch_gauss_t<MODEL, 4, 16>(ep, items, nitems, lx, tn, partials, s);
-    default: return launch_gauss_t<MODEL, 16, 16>(ep, items, nitems, lx, tn, partials, s);
+    case 0: return launch_gauss_t<MODEL, 8, 32>(ep, items, nitems, lx, rows, tn, partials, s);
+    case 1: return launch_gauss_t<MODEL, 4, 32>(ep, items, nitems, lx, rows, tn, partials, s);
+    case 2: return launch_gauss_t<MODEL, 4, 16>(ep, items, nitems, lx, rows, tn, partials, s);
+    default: return launch_gauss_t<MODEL, 16, 16>(ep, items, nitems, lx, rows, tn, partials, s);
     }
 }
 
@@ -386,7 +386,8 @@ struct gft_batch {
     double* d_part_e = nullptr;
     double* d_part_g = nullptr;
     int part_cap = 0;           // tiles the energy partials hold
-    long long part_cap_g = 0;   // rows the Gauss partials hold (tiles x planes per chunk)
+    long long part_cap_g = 0;   // rows the Gauss partials hold (tiles x gauss_rows)
+    int gauss_rows = 32;        // Gauss partial rows per tile: planes of the longest chunk, min(lx, max nx)
     double* d_scale = nullptr;  // [n][kRowSlotCount]
     double* d_rows = nullptr;   // [rows_cap][n][kRowSlotCount]
     int rows_cap = 0;
@@ -552,15 +553,19 @@ int configure(gft_batch* b, int variant, int lx)
     if (e == cudaSuccess) e = cudaMemcpy(b->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(EnsMaps), cudaMemcpyHostToDevice);
     // energy partials: a row per tile; Gauss partials: a row per tile and plane of its chunk
-    if (e == cudaSuccess && ((int)items.size() > b->part_cap || (long long)items.size() * lx > b->part_cap_g)) {
+    int maxnx = 1;
+    for (const auto& c : b->cfg) maxnx = std::max(maxnx, c.nx);
+    const int grows = std::min(lx, maxnx);
+    if (e == cudaSuccess && ((int)items.size() > b->part_cap || (long long)items.size() * grows > b->part_cap_g)) {
         cudaFree(b->d_part_e);
         cudaFree(b->d_part_g);
         b->d_part_e = b->d_part_g = nullptr;
         e = cudaMalloc(&b->d_part_e, items.size() * kObsCount * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&b->d_part_g, items.size() * (size_t)lx * kGaussSlots * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_part_g, items.size() * (size_t)grows * kGaussSlots * sizeof(double));
         b->part_cap = (e == cudaSuccess) ? (int)items.size() : 0;
-        b->part_cap_g = (e == cudaSuccess) ? (long long)items.size() * lx : 0;
+        b->part_cap_g = (e == cudaSuccess) ? (long long)items.size() * grows : 0;
     }
+    b->gauss_rows = grows;
     if (e != cudaSuccess) return b->cuda_fail(e, "gft_batch: configure");
     b->nitems = (int)items.size();
     b->variant = variant;
@@ -660,14 +665,15 @@ cudaError_t issue_step(gft_batch* b, int ti, bool e, bool g, double* rows, long 
             fill_params(b, gr, ti, false, &ep);
             const int i0 = b->group_item[gr], ni = b->group_item[gr + 1] - i0;
             err = (b->model == GFT_MODEL_SM)
-                      ? launch_gauss_m<kModelSM>(b->variant, ep, b->d_items + i0, ni, b->lx, tn,
-                                                 b->d_part_g + (size_t)i0 * b->lx * kGaussSlots, b->stream)
-                      : launch_gauss_m<kModel2HDM>(b->variant, ep, b->d_items + i0, ni, b->lx, tn,
-                                                   b->d_part_g + (size_t)i0 * b->lx * kGaussSlots, b->stream);
+                      ? launch_gauss_m<kModelSM>(b->variant, ep, b->d_items + i0, ni, b->lx, b->gauss_rows, tn,
+                                                 b->d_part_g + (size_t)i0 * b->gauss_rows * kGaussSlots, b->stream)
+                      : launch_gauss_m<kModel2HDM>(b->variant, ep, b->d_items + i0, ni, b->lx, b->gauss_rows, tn,
+                                                   b->d_part_g + (size_t)i0 * b->gauss_rows * kGaussSlots,
+                                                   b->stream);
             (*nlaunch)++;
         }
         if (err == cudaSuccess) {
-            ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_g, b->d_first, b->lx, kGaussSlots, 4,
+            ensemble_finalize_kernel<<<b->n, kFinThreads, 0, b->stream>>>(b->d_part_g, b->d_first, b->gauss_rows, kGaussSlots, 4,
                                                                           b->d_scale, kObsCount, rows);
             err = cudaGetLastError();
             (*nlaunch)++;

@@ -98,6 +98,24 @@ def test_two_launch_groups_and_uneven_chunks_evolve_like_single_handles(oracle_m
         _compare_rows(rows[m], r1, ps[m].nsite)
 
 
+def test_march_longer_than_every_member(oracle_mod):
+    """A march of 64 planes over members 8 and 12 planes long: every tile is one whole
+    member chunk, and the Gauss pass keeps one partial row per plane of the longest member."""
+    from gftevolver_b200 import Ensemble, InitialData
+    ps, ics = _members(oracle_mod, 1, [(8, 8, 16), (12, 8, 32)], every=(2, 2))
+    nt = 5
+    with Ensemble(ps) as ens:
+        ens.set_kernel(2, 64)
+        ens.init_fields([InitialData(**ic) for ic in ics])
+        rows = ens.evolve(nt)
+        out = [ens.download(m) for m in range(len(ps))]
+    for m, (p, ic) in enumerate(zip(ps, ics)):
+        sc, ve, r1 = _single(p, ic, nt, 2, 64)
+        assert np.max(np.abs(out[m][0] - sc)) <= 2e-6
+        assert np.max(np.abs(out[m][1] - ve)) <= 2e-6
+        _compare_rows(rows[m], r1, p.nsite)
+
+
 def test_graph_replay_equals_direct_launches(oracle_mod):
     from gftevolver_b200 import Ensemble, InitialData
     ps, ics = _members(oracle_mod, 1, [(16, 8, 16), (32, 16, 32), (8, 4, 16)], every=(2, 2))
