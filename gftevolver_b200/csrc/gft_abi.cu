@@ -1156,7 +1156,8 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     }
     if (kind >= 2 && h->hf != kHfNone)
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the tiled kernel has no Higgs-family field");
-    const bool fp64_sm = h->cfg.form == GFT_FORM_FP64 && h->cfg.model == GFT_MODEL_SM && kind == 2;
+    // the FP64 form of the SM model takes tiles too (kind 2, and kind 0's automatic choice)
+    const bool fp64_sm = h->cfg.form == GFT_FORM_FP64 && h->cfg.model == GFT_MODEL_SM && (kind == 2 || kind == 0);
     if (h->cfg.form != GFT_FORM_MIXED && !fp64_sm) {
         if (kind >= 2)
             return h->fail(GFT_E_UNSUPPORTED,
@@ -1169,8 +1170,13 @@ int gft_set_kernel(gft_handle* h, int kind, int tile, int march)
     cudaSetDevice(h->cfg.device);
     drop_graph(h);
     const StepParams P = make_params(h, h->time_iter, false);
-    if (!tiled_supported(P, tile))
+    if (!tiled_supported(P, tile)) {
+        if (kind == 0) {  // automatic: the tile shape chosen at creation, or one thread per site
+            h->kernel_kind = 0;
+            return GFT_OK;
+        }
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: the lattice shape does not divide into this tile");
+    }
     TMaps tm[2], tp[2];
     if (!encode_tiled(h, P, tile, tm, tp))
         return h->fail(GFT_E_UNSUPPORTED, "gft_set_kernel: tensor map encoding failed");

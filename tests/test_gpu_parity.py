@@ -420,10 +420,14 @@ def test_step_kernel_name_follows_form_and_shape(oracle_mod):
         assert ev.step_kernel_name == "tiled_step_kernel"
     with Evolver(_lp(big.__dict__), form="fp64") as ev:  # FP64: 5.2 waves of 148, under 8
         assert ev.step_kernel_name == "fast_step_kernel"
+        ev.set_kernel(0, 3, 16)  # automatic with 16 x 16 tiles, march 16: 1536 tiles = 10.4 waves
+        assert ev.step_kernel_name == "tiled_step_kernel"
     with Evolver(_lp(op.__dict__), form="ref32") as ev:
         assert ev.step_kernel_name == "ref_step_kernel"
     odd = oracle_mod.Params(nx=5, ny=3, nz=7)
     with Evolver(_lp(odd.__dict__), form="mixed") as ev:
+        assert ev.step_kernel_name == "fast_step_kernel"
+        ev.set_kernel(0, 0, 32)  # automatic, with a tile the lattice does not divide into
         assert ev.step_kernel_name == "fast_step_kernel"
     two = oracle_mod.Params(model=2, nx=8, ny=8, nz=32)  # 2HDM: one thread per site unless asked
     with Evolver(_lp(two.__dict__), form="mixed") as ev:
