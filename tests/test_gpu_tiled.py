@@ -85,17 +85,20 @@ def test_tiled_rejects_indivisible_lattice(oracle_mod):
         ev.evolve(2)  # automatic choice falls back to the one-thread-per-site kernel
 
 
-@pytest.mark.parametrize("shape,tile,march", [
-    ((8, 8, 32), 0, 32),      # every halo wraps
-    ((10, 24, 96), 0, 4),     # an interior 8 x 32 tile; march does not divide nx
-    ((6, 48, 48), 3, 32),     # an interior 16 x 16 tile
+@pytest.mark.parametrize("shape,tile,march,fixed", [
+    ((8, 8, 32), 0, 32, 0),      # every halo wraps
+    ((10, 24, 96), 0, 4, 0),     # an interior 8 x 32 tile; march does not divide nx
+    ((6, 48, 48), 3, 32, 0),     # an interior 16 x 16 tile
+    ((10, 24, 96), 0, 4, 5),     # Fixed faces on x and z (frozen sites inside x-marches)
+    ((8, 8, 32), 0, 32, 7),      # Fixed faces on every axis
 ])
-def test_fp64_tiled_matches_oracle(oracle_mod, shape, tile, march):
-    """The FP64 form through the staged tiled step (gft_set_kernel kind 2): the FP64 bar,
-    1e-12 relative to the FP64 oracle after 10 steps; energy terms within 1e-12 of the total."""
+def test_fp64_tiled_matches_oracle(oracle_mod, shape, tile, march, fixed):
+    """The FP64 form through the staged tiled step (gft_set_kernel kind 2; the automatic FP64
+    SM kernel on large lattices): the FP64 bar, 1e-12 relative to the FP64 oracle after 10
+    steps; energy terms within 1e-12 of the total."""
     from gftevolver_b200 import Evolver, LatticeParams
     nx, ny, nz = shape
-    op = oracle_mod.Params(model=1, nx=nx, ny=ny, nz=nz, energy_every=3, gauss_every=4)
+    op = oracle_mod.Params(model=1, nx=nx, ny=ny, nz=nz, energy_every=3, gauss_every=4, fixed_axes=fixed)
     ic = oracle_mod.ICSpec(seed=33, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
     sc, ve = oracle_mod.init_fields(op, ic, np.float64)
     with Evolver(LatticeParams(**op.__dict__), form="fp64") as ev:
@@ -115,4 +118,6 @@ def test_fp64_tiled_matches_oracle(oracle_mod, shape, tile, march):
             assert abs(a["plaq_su2"] - b["plaq_su2"]) <= 1e-13
             assert abs(a["phi_sq"] - b["phi_sq"]) <= 1e-12
         if b["has_gauss"]:
-            assert max(a["gauss_max"]) <= 1e-12
+            # rounding level on periodic lattices; next to frozen sites the residual is the
+            # oracle's (the Fixed faces break the constraint there, as in the reference)
+            np.testing.assert_allclose(a["gauss_max"], b["gauss_max"], rtol=1e-8, atol=1e-12)
