@@ -156,11 +156,15 @@ class ClockSampler:
 
 
 def measured_peaks():
+    """HBM copy bandwidth (GB/s) measured on this pool's B200s, else the recipe's fallback."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            with open(path) as f:
+                d = json.load(f)
+            return float(d["hbm_gbs"]), "measured"
+        except (OSError, ValueError, KeyError, TypeError):
+            pass  # an unreadable file: the fallback, named as such in the line
     return 6650.0, "fallback"
 
 
