@@ -299,11 +299,11 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
 // The automatic choice (kernel kind 0) takes the staged step for the SM model
 // when its tiles fill enough waves of resident CTAs: fewer tiles leave SMs idle
 // while each CTA marches its planes, and one thread per site is faster there
-// (mixed form at 32^3: 14x, 64^3: 3.6x, 128^3 (256 tiles, under one wave): even;
-// 192^3 (2.9 waves): the staged step 15 % faster.  FP64, one CTA per SM: one
+// (mixed form at 32^3: 14x, 64^3 (0.11 waves): 3.6x; 128^3 (0.86 waves): the
+// staged step 2 % faster, 192^3 (2.9 waves): 15 %.  FP64, one CTA per SM: one
 // thread per site faster up to 128^3, even at 192^3 (5.8 waves), the staged
 // step 5.5 % faster at 256^3 (13.8 waves)).
-constexpr int kAutoWavesMixed = 2, kAutoWavesFP64 = 8;
+constexpr double kAutoWavesMixed = 0.8, kAutoWavesFP64 = 8.0;
 
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {
@@ -316,7 +316,7 @@ bool use_tiled(const gft_handle* h, const StepParams& P)
     if (h->kernel_kind != 0) return true;
     if (h->cfg.model != GFT_MODEL_SM) return false;
     const long long slots = (long long)h->nsm * tiled_ctas_per_sm(h->tile_variant, fp64);
-    return tiled_blocks(P, h->tile_variant, h->march) >= (fp64 ? kAutoWavesFP64 : kAutoWavesMixed) * slots;
+    return tiled_blocks(P, h->tile_variant, h->march) >= (fp64 ? kAutoWavesFP64 : kAutoWavesMixed) * (double)slots;
 }
 
 // Plain steps of the SM mixed form with two sites per thread (kernel kind 3):

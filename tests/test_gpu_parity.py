@@ -402,7 +402,7 @@ def test_device_buffer_transfers_match_host_transfers(oracle_mod, form):
 
 def test_step_kernel_name_follows_form_and_shape(oracle_mod):
     """The automatic choice takes the staged step for the SM model when its tiles fill
-    2 waves of resident CTAs (mixed form) or 8 (FP64), else one thread per site."""
+    0.8 of a wave of resident CTAs (mixed form) or 8 waves (FP64), else one thread per site."""
     from gftevolver_b200 import Evolver
     op = oracle_mod.Params(nx=8, ny=8, nz=32)  # one tile
     with Evolver(_lp(op.__dict__), form="mixed") as ev:
