@@ -15,14 +15,19 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_plane_wait_gives_up_and_the_handle_recovers(oracle_mod):
+@pytest.mark.parametrize("form,shape", [
+    ("mixed", (16, 16, 64)),  # every tile wraps: one CTA barrier per plane
+    ("fp64", (8, 24, 96)),    # an interior 8 x 32 tile: the FP64 march without per-plane barriers
+])
+def test_plane_wait_gives_up_and_the_handle_recovers(oracle_mod, form, shape):
     from gftevolver_b200 import Evolver, GftError, LatticeParams
     from gftevolver_b200 import _lib
-    op = oracle_mod.Params(model=oracle_mod.MODEL_SM, nx=16, ny=16, nz=64, energy_every=2, gauss_every=2)
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=oracle_mod.MODEL_SM, nx=nx, ny=ny, nz=nz, energy_every=2, gauss_every=2)
     p = LatticeParams(**op.__dict__)
     ic = oracle_mod.ICSpec(seed=77, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
-    sc, ve = oracle_mod.init_fields(op, ic, np.float32)
-    with Evolver(p, form="mixed") as ev:
+    sc, ve = oracle_mod.init_fields(op, ic, np.float64 if form == "fp64" else np.float32)
+    with Evolver(p, form=form) as ev:
         ev.set_kernel(2, 0, 8)
         ev.set_wait_limit(1)
         ev.upload(sc, ve, 0)
@@ -35,7 +40,7 @@ def test_plane_wait_gives_up_and_the_handle_recovers(oracle_mod):
         rows = ev.evolve(5)
         assert ev.last_warnings == 0
         a_sc, a_ve = ev.download()
-    with Evolver(p, form="mixed") as ev:
+    with Evolver(p, form=form) as ev:
         ev.set_kernel(2, 0, 8)
         ev.upload(sc, ve, 0)
         rows_ref = ev.evolve(5)
