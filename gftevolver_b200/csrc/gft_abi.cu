@@ -301,9 +301,10 @@ bool encode_tiled(const gft_handle* h, const StepParams& P, int tile, TMaps* tm,
 // while each CTA marches its planes, and one thread per site is faster there
 // (mixed form at 32^3: 14x, 64^3 (0.11 waves): 3.6x; 128^3 (0.86 waves): the
 // staged step 2 % faster, 192^3 (2.9 waves): 15 %.  FP64, one CTA per SM: one
-// thread per site faster up to 128^3, even at 192^3 (5.8 waves), the staged
-// step 5.5 % faster at 256^3 (13.8 waves)).
-constexpr double kAutoWavesMixed = 0.8, kAutoWavesFP64 = 8.0;
+// thread per site 11 % faster at 128^3 (1.7 waves) and 7.5 % at 160^3 (3.4
+// waves); the staged step 1.6 % faster at 192^3 (5.8 waves) and 7 % at 256^3
+// (13.8 waves)).
+constexpr double kAutoWavesMixed = 0.8, kAutoWavesFP64 = 5.0;
 
 bool use_tiled(const gft_handle* h, const StepParams& P)
 {

@@ -273,7 +273,7 @@ int gft_observe_static(const gft_config* cfg, const float* d_scalars, const floa
 /* Step-kernel selection for the throughput forms (no reference counterpart):
  * kind 0 = automatic (for the SM model, the tiled kernel when the lattice
  * divides into a built tile and the tiles fill at least 0.8 of a wave of
- * resident CTAs -- 8 waves in the FP64 form --, else the one-thread-per-site
+ * resident CTAs -- 5 waves in the FP64 form --, else the one-thread-per-site
  * kernel), 1 = one
  * thread per site with neighbours read through L1/L2, 2 = TMA-staged tiles
  * marching along x (mixed form; FP64 form of the SM model), 3 = as 2, with two sites per thread in paired

@@ -402,7 +402,7 @@ def test_device_buffer_transfers_match_host_transfers(oracle_mod, form):
 
 def test_step_kernel_name_follows_form_and_shape(oracle_mod):
     """The automatic choice takes the staged step for the SM model when its tiles fill
-    0.8 of a wave of resident CTAs (mixed form) or 8 waves (FP64), else one thread per site."""
+    0.8 of a wave of resident CTAs (mixed form) or 5 waves (FP64), else one thread per site."""
     from gftevolver_b200 import Evolver
     op = oracle_mod.Params(nx=8, ny=8, nz=32)  # one tile
     with Evolver(_lp(op.__dict__), form="mixed") as ev:
@@ -415,12 +415,12 @@ def test_step_kernel_name_follows_form_and_shape(oracle_mod):
         assert ev.step_kernel_name == "fast_step_kernel"
         ev.set_kernel(2, 0, 32)
         assert ev.step_kernel_name == "tiled_step_kernel"
-    big = oracle_mod.Params(nx=96, ny=256, nz=256)  # 8 x 32 tiles, march 32: 768 tiles = 2.6 waves of 296
+    big = oracle_mod.Params(nx=64, ny=256, nz=256)  # 8 x 32 tiles, march 32: 512 tiles = 1.7 waves of 296
     with Evolver(_lp(big.__dict__), form="mixed") as ev:
         assert ev.step_kernel_name == "tiled_step_kernel"
-    with Evolver(_lp(big.__dict__), form="fp64") as ev:  # FP64: 5.2 waves of 148, under 8
+    with Evolver(_lp(big.__dict__), form="fp64") as ev:  # FP64: 3.5 waves of 148, under 5
         assert ev.step_kernel_name == "fast_step_kernel"
-        ev.set_kernel(0, 3, 16)  # automatic with 16 x 16 tiles, march 16: 1536 tiles = 10.4 waves
+        ev.set_kernel(0, 3, 16)  # automatic with 16 x 16 tiles, march 16: 1024 tiles = 6.9 waves
         assert ev.step_kernel_name == "tiled_step_kernel"
     with Evolver(_lp(op.__dict__), form="ref32") as ev:
         assert ev.step_kernel_name == "ref_step_kernel"
