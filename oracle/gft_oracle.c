@@ -791,6 +791,46 @@ static double damping_step(const ctx_t* m, int time_iter)
 }
 
 /*
+ * Gauss-law residual of the levels (now, fut) in the reference's site order
+ * (GaugeCondition.cpp:117-165 with Model.cpp:323-337): per constraint the sum
+ * of |violation| in the storage type (ref_int) and in double (gint), and its
+ * maximum (gmax); loc_g (may be NULL) [nsite][gaugeNum] receives the signed
+ * violations rounded to float.
+ */
+static void gauss_pass(ctx_t* m, const long long* order, const S* sc_now, const S* sc_fut, const S* ve_now,
+                       const S* ve_fut, double* loc_g, double* gint, double* gmax, S* ref_int)
+{
+    const long long N = m->nsite;
+    const int nsc = m->nsc, NV = m->nv, neq = m->neq;
+    for (long long oi = 0; oi < N; oi++) {
+        long long idx = order[oi];
+        long long x = idx / (m->ny * m->nz), y = (idx / m->nz) % m->ny, z = idx % m->nz;
+        if (frozen(m, x, y, z)) continue;
+        long long p[3] = {x, y, z}, n[3] = {m->nx, m->ny, m->nz};
+        const S* xm_now[3];
+        const S* xm_fut[3];
+        for (int d = 0; d < 3; d++) {
+            long long q[3] = {p[0], p[1], p[2]};
+            q[d] = wrap(q[d] - 1, n[d]);
+            long long j = site_index(m, q[0], q[1], q[2]);
+            xm_now[d] = ve_now + j * NV;
+            xm_fut[d] = ve_fut + j * NV;
+        }
+        S el[ORC_MAX_EQ], gr[ORC_MAX_EQ];
+        loop_constraint(m, ve_now + idx * NV, ve_fut + idx * NV, xm_now, xm_fut, el);
+        gradient_constraint(m, sc_fut + idx * nsc, sc_now + idx * nsc, gr);
+        for (int k = 0; k < neq; k++) {
+            S viol = el[k] - (S)m->gsq_coupling[k] * gr[k];
+            if (loc_g) loc_g[idx * neq + k] = (double)(float)viol;
+            S v = viol < (S)0 ? -viol : viol;
+            ref_int[k] = ref_int[k] + v;
+            gint[k] += (double)v;
+            if ((double)v > gmax[k]) gmax[k] = (double)v;
+        }
+    }
+}
+
+/*
  * Evolve nsteps steps starting at time step time_iter0, in place on the
  * two-level arrays.  Energy / Gauss rows are written on steps where
  * time_iter % every == 0 (the analysers' counters, Energy.cpp:212-219,
@@ -909,32 +949,7 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
             /* post-evolve: the past slot now holds t + dt (Lattice.cpp:441-541) */
             S ref_int[ORC_MAX_EQ] = {0};
             double gint[ORC_MAX_EQ] = {0}, gmax[ORC_MAX_EQ] = {0};
-            for (long long oi = 0; oi < N; oi++) {
-                long long idx = order[oi];
-                long long x = idx / (m.ny * m.nz), y = (idx / m.nz) % m.ny, z = idx % m.nz;
-                if (frozen(&m, x, y, z)) continue;
-                long long p[3] = {x, y, z}, n[3] = {m.nx, m.ny, m.nz};
-                const S* xm_now[3];
-                const S* xm_fut[3];
-                for (int d = 0; d < 3; d++) {
-                    long long q[3] = {p[0], p[1], p[2]};
-                    q[d] = wrap(q[d] - 1, n[d]);
-                    long long j = site_index(&m, q[0], q[1], q[2]);
-                    xm_now[d] = ve_now + j * NV;
-                    xm_fut[d] = ve_past + j * NV;
-                }
-                S el[ORC_MAX_EQ], gr[ORC_MAX_EQ];
-                loop_constraint(&m, ve_now + idx * NV, ve_past + idx * NV, xm_now, xm_fut, el);
-                gradient_constraint(&m, sc_past + idx * nsc, sc_now + idx * nsc, gr);
-                for (int k = 0; k < neq; k++) {
-                    S viol = el[k] - (S)m.gsq_coupling[k] * gr[k];
-                    if (local_g && loc_g) loc_g[idx * neq + k] = (double)(float)viol;
-                    S v = viol < (S)0 ? -viol : viol;
-                    ref_int[k] = ref_int[k] + v;
-                    gint[k] += (double)v;
-                    if ((double)v > gmax[k]) gmax[k] = (double)v;
-                }
-            }
+            gauss_pass(&m, order, sc_now, sc_past, ve_now, ve_past, local_g ? loc_g : NULL, gint, gmax, ref_int);
             double dv = cfg->dx * cfg->dy * cfg->dz;
             row.has_gauss = do_gauss;
             for (int k = 0; k < neq && do_gauss; k++) {
@@ -950,6 +965,36 @@ int FN(evolve)(const orc_config* cfg, S* scalars, S* vectors, int time_iter0, in
     free(order);
     if (warn) *warn = w;
     return nrows;
+}
+
+/*
+ * The Gauss row of the two levels as they stand after step time_iter (the
+ * past slot of that step holding t + dt), computed as the post-evolve analyser
+ * of FN(evolve) computes it, without stepping: gauss_int[k] (times the cell
+ * volume) and gauss_max[k] for the gaugeNum constraints; loc_g as in FN(evolve)
+ * (may be NULL).  Returns 0, or < 0 on error.
+ */
+int FN(gauss)(const orc_config* cfg, const S* scalars, const S* vectors, int time_iter, double* gauss_int,
+              double* gauss_max, double* loc_g)
+{
+    ctx_t m;
+    if (ctx_init(&m, cfg) != 0) return -1;
+    long long* order = reference_site_order(&m);
+    if (!order) return -2;
+    const long long N = m.nsite;
+    const int t_now = (time_iter + 1) % 2, t_past = 1 - t_now;
+    S ref_int[ORC_MAX_EQ] = {0};
+    double gint[ORC_MAX_EQ] = {0}, gmax[ORC_MAX_EQ] = {0};
+    gauss_pass(&m, order, scalars + (long long)t_now * N * m.nsc, scalars + (long long)t_past * N * m.nsc,
+               vectors + (long long)t_now * N * m.nv, vectors + (long long)t_past * N * m.nv, loc_g, gint, gmax,
+               ref_int);
+    const double dv = cfg->dx * cfg->dy * cfg->dz;
+    for (int k = 0; k < m.neq; k++) {
+        gauss_int[k] = gint[k] * dv;
+        gauss_max[k] = gmax[k];
+    }
+    free(order);
+    return 0;
 }
 
 /* ----------------------------------------------------------------------------

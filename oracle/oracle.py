@@ -187,6 +187,10 @@ def _load():
                 f.argtypes = [ctypes.POINTER(OrcConfig), fp, fp, ctypes.c_int, ctypes.c_int,
                               ctypes.POINTER(OrcRow), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+                f = getattr(lib, p + "gauss")
+                f.restype = ctypes.c_int
+                f.argtypes = [ctypes.POINTER(OrcConfig), fp, fp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
                 f = getattr(lib, p + "init_fields")
                 f.restype = None
                 f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -276,3 +280,25 @@ def evolve(p: Params, scalars: np.ndarray, vectors: np.ndarray, nsteps: int, tim
     if local:
         return out, warn.value, loc_e, loc_g
     return out, warn.value
+
+
+def gauss(p: Params, scalars: np.ndarray, vectors: np.ndarray, time_iter: int):
+    """The Gauss row of two levels as they stand after step time_iter (the post-evolve
+    analyser of evolve, without stepping): (gauss_int[neq], gauss_max[neq], loc_g[nsite, neq])
+    with loc_g the signed violations rounded to float."""
+    lib = _load()
+    assert scalars.flags.c_contiguous and vectors.flags.c_contiguous
+    assert scalars.dtype == vectors.dtype
+    assert scalars.shape == (2, p.nx, p.ny, p.nz, p.nsc), scalars.shape
+    assert vectors.shape == (2, p.nx, p.ny, p.nz, p.nve), vectors.shape
+    gi = np.zeros(MAX_EQ, np.float64)
+    gm = np.zeros(MAX_EQ, np.float64)
+    loc_g = np.zeros((p.nsite, p.neq), np.float64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    cfg = p.to_c()
+    n = getattr(lib, _prefix(scalars.dtype) + "gauss")(
+        ctypes.byref(cfg), _ptr(scalars), _ptr(vectors), int(time_iter), gi.ctypes.data_as(dp), gm.ctypes.data_as(dp),
+        loc_g.ctypes.data_as(dp))
+    if n < 0:
+        raise ValueError(f"oracle rejected the configuration (code {n})")
+    return gi[: p.neq].copy(), gm[: p.neq].copy(), loc_g

@@ -121,3 +121,55 @@ def test_fp64_tiled_matches_oracle(oracle_mod, shape, tile, march, fixed):
             # rounding level on periodic lattices; next to frozen sites the residual is the
             # oracle's (the Fixed faces break the constraint there, as in the reference)
             np.testing.assert_allclose(a["gauss_max"], b["gauss_max"], rtol=1e-8, atol=1e-12)
+
+
+@pytest.mark.parametrize("kind,shape,tile,march,fixed", [
+    (1, (10, 24, 96), 0, 4, 0),   # after the one-thread-per-site step
+    (2, (10, 24, 96), 0, 4, 0),   # after the tiled step: an interior 8 x 32 tile; march does not divide nx
+    (2, (8, 8, 32), 0, 32, 0),    # every halo wraps
+    (2, (6, 48, 48), 3, 32, 0),   # 16 x 16 tiles with interior tiles
+    (2, (9, 12, 48), 2, 1, 0),    # 4 x 16 tiles, march 1
+    (2, (7, 8, 32), 1, 3, 0),     # 4 x 32 tiles
+    (2, (10, 24, 96), 0, 4, 5),   # Fixed faces on x and z
+    (2, (8, 8, 32), 0, 32, 7),    # Fixed faces on every axis
+])
+def test_gauss_pass_matches_oracle_on_the_same_fields(oracle_mod, kind, shape, tile, march, fixed):
+    """The mixed form's Gauss pass (fast_gauss_kernel, FP64 from the stored floats) against
+    the oracle's FP64 Gauss pass over the very fields the GPU's last step left, downloaded and
+    widened exactly to double: both evaluate the residual in FP64 from the same inputs, so
+    the maximum and the integral agree to 1e-12 relative, and every local violation (rounded
+    to float) to one float ulp plus 1e-16: the kernel may contract multiply-adds where the
+    oracle rounds twice, a difference of order 1e-17 on terms of order 0.1, which the float
+    rounding of the smallest violations (down to 1e-13) can show."""
+    nx, ny, nz = shape
+    op = oracle_mod.Params(model=1, nx=nx, ny=ny, nz=nz, gauss_every=1, gauss_local_every=1, fixed_axes=fixed)
+    _check_gauss_on_same_fields(oracle_mod, op, kind, tile, march, mean=1.0)
+
+
+@pytest.mark.parametrize("hf", [0, 1, 2], ids=["2hdm", "2hdm_hf_u1", "2hdm_hf_su2"])
+def test_gauss_pass_2hdm_matches_oracle_on_the_same_fields(oracle_mod, hf):
+    """As above for the 2HDM model: both doublets, and the Higgs-family constraints of gaugeNum
+    5 and 7 (one thread per site; the kernel the automatic choice takes for 2HDM)."""
+    op = oracle_mod.Params(model=2, nx=6, ny=8, nz=32, gauss_every=1, gauss_local_every=1, higgs_family=hf)
+    _check_gauss_on_same_fields(oracle_mod, op, 1, 0, 32, mean=0.7)
+
+
+def _check_gauss_on_same_fields(oracle_mod, op, kind, tile, march, mean):
+    from gftevolver_b200 import Evolver, LatticeParams
+    ic = oracle_mod.ICSpec(seed=41, mean=[mean] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(op, ic, np.float32)
+    with Evolver(LatticeParams(**op.__dict__), form="mixed") as ev:
+        ev.set_kernel(kind, tile, march)
+        assert ev.step_kernel_name == ("tiled_step_kernel" if kind == 2 else "fast_step_kernel")
+        ev.upload(sc, ve, 0)
+        rows = ev.evolve(3)
+        g_sc, g_ve = ev.download()
+        _, _, lg, gstep = ev.local_fields()
+    assert rows[-1]["time_iter"] == 2 and rows[-1]["has_gauss"] and gstep == 2
+    gi, gm, o_lg = oracle_mod.gauss(op, g_sc.astype(np.float64), g_ve.astype(np.float64), 2)
+    np.testing.assert_allclose(rows[-1]["gauss_max"], gm, rtol=1e-12, atol=1e-18)
+    np.testing.assert_allclose(rows[-1]["gauss_int"], gi, rtol=1e-12, atol=1e-18)
+    assert max(gm) > 0.0
+    tol = np.spacing(np.abs(o_lg).astype(np.float32)).astype(np.float64) + 1e-16
+    excess = np.abs(lg.astype(np.float64) - o_lg) - tol
+    assert excess.max() <= 0.0, (excess.max(), o_lg.flat[np.argmax(excess)])

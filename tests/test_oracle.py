@@ -69,6 +69,21 @@ def test_oracle_free_field_limit(oracle_mod):
     np.testing.assert_allclose(sc[0], expect, rtol=0, atol=1e-15)
 
 
+@pytest.mark.parametrize("model,dtype,time_iter", [
+    (1, np.float64, 0), (1, np.float32, 3), (2, np.float64, 1), (2, np.float32, 0)])
+def test_oracle_gauss_matches_its_post_evolve_row(oracle_mod, model, dtype, time_iter):
+    """gauss() on the levels after a step reproduces that step's own Gauss row and local
+    violations exactly (the same pass over the same fields, no step)."""
+    p = oracle_mod.Params(model=model, nx=5, ny=4, nz=6, gauss_every=1, gauss_local_every=1)
+    ic = oracle_mod.ICSpec(seed=9, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
+    sc, ve = oracle_mod.init_fields(p, ic, dtype)
+    rows, _, _, loc_g = oracle_mod.evolve(p, sc, ve, 1, time_iter0=time_iter, local=True)
+    gi, gm, lg = oracle_mod.gauss(p, sc, ve, time_iter)
+    assert list(gi) == rows[0]["gauss_int"] and list(gm) == rows[0]["gauss_max"]
+    assert np.array_equal(lg, loc_g)
+    assert max(gm) > 0.0
+
+
 def test_oracle_rejects_bad_config(oracle_mod):
     p = oracle_mod.Params(model=7, nx=2, ny=2, nz=2)
     sc = np.zeros((2, 2, 2, 2, p.nsc), np.float32)
