@@ -88,6 +88,7 @@ def test_tiled_rejects_indivisible_lattice(oracle_mod):
 @pytest.mark.parametrize("shape,tile,march,fixed", [
     ((8, 8, 32), 0, 32, 0),      # every halo wraps
     ((10, 24, 96), 0, 4, 0),     # an interior 8 x 32 tile; march does not divide nx
+    ((9, 48, 128), 0, 4, 0),     # 8 of 24 tiles per chunk interior: the march without per-plane barriers
     ((6, 48, 48), 3, 32, 0),     # an interior 16 x 16 tile
     ((10, 24, 96), 0, 4, 5),     # Fixed faces on x and z (frozen sites inside x-marches)
     ((8, 8, 32), 0, 32, 7),      # Fixed faces on every axis
