@@ -388,9 +388,11 @@ __device__ __forceinline__ bool run_ring(const TMaps& maps, const TMaps& pmaps, 
     };
     auto parity = [&](int p) { return ((ring.bits >> (p % G::NBUF)) ^ (unsigned)(p / G::NBUF)) & 1u; };
     // Tiles without wrapped halo cells in the FP64 form march without a CTA
-    // barrier per plane (below).  Measured at 256^3: the FP64 step (one CTA of 8
-    // warps per SM) 2 % faster; the FP32 steps 3 % slower (two CTAs per SM,
-    // whose barrier gaps the other CTA fills), so they keep the barrier.
+    // barrier per plane (below): its warps wait on long FP64 latencies, and the
+    // FP64 step (one CTA of 8 warps per SM) measured 2 % faster at 256^3.  The
+    // FP32 steps keep the barrier: without it the SM step (two CTAs per SM) was
+    // 3 % slower at 256^3 and the 2HDM step (one CTA per SM) 4 % slower at
+    // 192^3, their warps waiting on copies and past-level loads instead.
     constexpr bool kFree = sizeof(S) == 8;
     // After the barriers: per buffer, the warps that have computed the plane in
     // it (tiles without wrapped halo); then the number of planes issued.
