@@ -69,12 +69,15 @@ def test_oracle_free_field_limit(oracle_mod):
     np.testing.assert_allclose(sc[0], expect, rtol=0, atol=1e-15)
 
 
-@pytest.mark.parametrize("model,dtype,time_iter", [
-    (1, np.float64, 0), (1, np.float32, 3), (2, np.float64, 1), (2, np.float32, 0)])
-def test_oracle_gauss_matches_its_post_evolve_row(oracle_mod, model, dtype, time_iter):
+@pytest.mark.parametrize("model,hf,fixed,dtype,time_iter", [
+    (1, 0, 0, np.float64, 0), (1, 0, 0, np.float32, 3), (1, 0, 5, np.float64, 2), (2, 0, 0, np.float64, 1),
+    (2, 0, 0, np.float32, 0), (2, 1, 0, np.float64, 1), (2, 2, 0, np.float32, 2), (2, 2, 3, np.float64, 0)])
+def test_oracle_gauss_matches_its_post_evolve_row(oracle_mod, model, hf, fixed, dtype, time_iter):
     """gauss() on the levels after a step reproduces that step's own Gauss row and local
-    violations exactly (the same pass over the same fields, no step)."""
-    p = oracle_mod.Params(model=model, nx=5, ny=4, nz=6, gauss_every=1, gauss_local_every=1)
+    violations exactly (the same pass over the same fields, no step), with the Higgs-family
+    constraints of gaugeNum 5 and 7 and Fixed faces."""
+    p = oracle_mod.Params(model=model, nx=5, ny=4, nz=6, gauss_every=1, gauss_local_every=1, higgs_family=hf,
+                          fixed_axes=fixed)
     ic = oracle_mod.ICSpec(seed=9, mean=[1.0] * 8, sigma=[0.1] * 8, theta_sigma=0.1, eps_sigma=0.1)
     sc, ve = oracle_mod.init_fields(p, ic, dtype)
     rows, _, _, loc_g = oracle_mod.evolve(p, sc, ve, 1, time_iter0=time_iter, local=True)
